@@ -1,0 +1,327 @@
+"""Benchmark: filtered ANN QPS of the HDGrid query path on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--config config2] [--impl hdgrid|reference]
+
+A step is one hdg_query over the whole query batch of the workload (index resident in HBM,
+queries and labels already on the device for ``value``).  ``e2e`` repeats the step through
+the public API with pinned host buffers: H2D of queries + labels, query, D2H of the results.
+The path does not shard (queries are independent, each GPU holds a full replica), so
+``--gpus N`` runs N replicas, one process per GPU, with the barrier + max-over-ranks timing.
+
+``--impl reference`` times the CPU port of the same query schedule (oracle/, all host
+threads) on a bounded sample of the workload; the reference's own CUDA build does not
+compile offline (it fetches RAFT/RMM at configure time).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(MEASURED_PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def workload(name: str, scale: float):
+    from hdgrid_b200 import datasets
+    if name == "config1":
+        return datasets.config1(scale=scale, break_down=1)
+    if name == "config2":
+        return datasets.config2(scale=scale, n_queries=max(1000, int(10_000 * min(1.0, scale * 4))), break_down=1)
+    if name == "config4":
+        return datasets.config4(scale=scale, n_queries=max(2000, int(100_000 * scale)), break_down=1)
+    raise SystemExit(f"unknown config {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    import torch
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline_bruteforce(ws, n_sample: int):
+    """FP64 filtered brute force (the reference's host verifier, generalised) on a sample."""
+    import oracle
+    import hdgrid_b200 as hg
+    spec = hg.parse_filter(ws["filter_conf"])
+    fd = int(hg.parse_config(ws["hdgrid_conf"])["filter_dim"])
+    qs = ws["queries"][:n_sample]
+    ranges = oracle.recover_filters(spec, ws["query_labels"][:n_sample], filter_dim=fd)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    oracle.bruteforce_f64(ws["base"], ws["labels"], qs, ranges, ws["k"], threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n_sample / dt, "unit": "queries/s", "cores": cores, "kind": "port",
+            "sample": f"FP64 filtered brute force (ground_truth.cuh:165-232 generalised) over the full base set "
+                      f"for {n_sample} of the workload's queries"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU port of the HDGrid query schedule on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    import hdgrid_b200 as hg
+    import oracle
+    from tests.helpers import build_gpu
+    ws = workload(args.config, args.scale)
+    idx, base, _ = build_gpu(ws, "cuda:0")
+    d = tempfile.mkdtemp(prefix="hdg_ref_")
+    path = os.path.join(d, "index.hdg")
+    idx.save(path)
+    ora = oracle.OracleIndex(path)
+    n_sample = args.ref_sample
+    cores = os.cpu_count() or 1
+    qs, ql = ws["queries"][:n_sample], ws["query_labels"][:n_sample]
+    for _ in range(max(0, min(args.warmup, 1))):
+        ora.query(qs, ql, ws["base"], ws["k"], threads=cores, trace=False)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ora.query(qs, ql, ws["base"], ws["k"], threads=cores, trace=False)
+        times.append(time.perf_counter() - t0)
+    value = n_sample * len(times) / sum(times)
+    sample = f"{n_sample} of the {ws['name']} queries per step through the CPU port of the super-grid query"
+    line = {"impl": "reference", "metric": metric_name(ws), "value": value, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(ws, args),
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def metric_name(ws):
+    return "filtered QPS @recall@100>=0.95, 1 B200 (plain HDGrid path); ADC scan HBM GB/s"
+
+
+def workload_config(ws, args):
+    import hdgrid_b200 as hg
+    p = hg.parse_config(ws["hdgrid_conf"])
+    return {"workload": f"{ws['name']}: {ws['base'].shape[0]}x{ws['base'].shape[1]} base, "
+                        f"{ws['labels'].shape[1]} label dims, {ws['queries'].shape[0]} queries, k={ws['k']}",
+            "n_lists": int(p["clusters"] * p["sub_clusters"]), "clusters": int(p["clusters"]),
+            "n_list": int(p["n_list"]), "sub_lists": int(p["sub_lists"]), "pq_dim": int(p["pq_dim"]),
+            "exps0": int(p["exps0"]), "max_grids": int(p["max_grids"]), "lut": "fp16" if p["lut_fp16"] else "f32",
+            "l2_flush": "256 MiB buffer written between timed steps", "parallelism": f"replicas{args.gpus}"}
+
+
+def run_hdgrid(args):
+    import torch
+    import hdgrid_b200 as hg
+    rank, world, local = dist_setup(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ws = workload(args.config, args.scale)
+    k = ws["k"]
+    idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
+    base = torch.from_numpy(ws["base"]).to(dev)
+    labels = torch.from_numpy(ws["labels"]).to(dev)
+    t_build = time.perf_counter()
+    idx.build(hg.build_input_t(base, labels))
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
+    q = torch.from_numpy(ws["queries"]).to(dev)
+    ql = torch.from_numpy(ws["query_labels"]).to(dev)
+    nq = q.shape[0]
+    idx.reserve(nq)
+    dist = torch.empty((nq, k), device=dev)
+    ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    qin, qout = hg.query_input_t(base, q, ql), hg.query_output_t(dist, ids)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    # recall against the exact filtered kNN (GPU brute force, FP32)
+    spec = hg.filter_spec(ws["filter_conf"])
+    ranges = torch.empty((nq, 2 * ws["labels"].shape[1]), device=dev)
+    hg.recover_filters(ws["filter_conf"], ql, ranges)
+    gt_d = torch.empty((nq, k), device=dev)
+    gt_i = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    hg.bruteforce_knn(base, labels, q, ranges, k, gt_d, gt_i)
+
+    for _ in range(args.warmup):
+        idx.query(qin, qout)
+    torch.cuda.synchronize()
+    from hdgrid_b200 import datasets
+    rec = datasets.recall(ids.cpu().numpy().view(np.uint64), gt_i.cpu().numpy().view(np.uint64))
+    cand = int(np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64).sum())
+
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    scan_ms = []
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.fill_(float(s))
+            ev[s][0].record(stream)
+            idx.query(qin, qout)
+            ev[s][1].record(stream)
+            st = idx.stage_times()
+            scan_ms.append(st.get("scan", float("nan")))
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms), world)
+    barrier(world)
+
+    # end to end through the public API with host buffers
+    q_h = torch.from_numpy(ws["queries"]).pin_memory()
+    ql_h = torch.from_numpy(ws["query_labels"]).pin_memory()
+    d_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    i_h = torch.empty((nq, k), dtype=torch.int64).pin_memory()
+    e2e_ms = []
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q.copy_(q_h, non_blocking=True)
+        ql.copy_(ql_h, non_blocking=True)
+        idx.query(qin, qout)
+        d_h.copy_(dist, non_blocking=True)
+        i_h.copy_(ids, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+
+    value = world * nq * args.steps / (total_ms / 1e3)
+    peak, peak_kind = hbm_peak()
+    info = idx.info()
+    p = hg.parse_config(ws["hdgrid_conf"])
+    lbl = ws["labels"].shape[1]
+    per_cand = info["M"] + (4 * lbl if p["exps0"] <= 1 else 0)
+    scan_avg = float(np.nanmean(scan_ms))
+    achieved = cand * per_cand / (scan_avg / 1e3) / 1e9
+    if rank != 0:
+        return
+    line = {
+        "metric": metric_name(ws), "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture, configs of the benchmark)",
+        "config": workload_config(ws, args) | {"recall_at_k": rec, "build_s": round(t_build, 2),
+                                               "candidates_per_step": cand},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_scan", "peak_kind": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg},
+        "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
+                "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4),
+                "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},
+        "gpu_launches": args.steps * (5 if p["exps0"] > 1 and lbl > 1 else 4 if p["exps0"] > 1 else 3),
+        "clocks": clk.summary(),
+        "stage_ms": idx.stage_times(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_bruteforce(ws, args.cpu_sample)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hdgrid", choices=["hdgrid", "reference"])
+    ap.add_argument("--config", default="config2")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-sample", type=int, default=100)
+    ap.add_argument("--ref-sample", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_hdgrid(args)
+    try:
+        import torch
+        if torch.distributed.is_initialized():
+            torch.distributed.destroy_process_group()
+    except Exception:
+        pass
+
+
+if __name__ == "__main__":
+    main()

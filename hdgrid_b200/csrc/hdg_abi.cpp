@@ -1,0 +1,311 @@
+// extern "C" boundary of libhdgrid.  Every entry point catches hdg::Error (and any other
+// exception) and turns it into an hdg_status plus hdg_last_error() text; nothing here
+// exits the process (the reference calls exit() on CUDA errors,
+// src/utils/debugging_utils.cuh:11-20).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "hdg_internal.h"
+
+namespace hdg {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void DeviceBuffer::reset() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void DeviceBuffer::ensure(size_t b) {
+    if (ptr && bytes >= b) return;
+    reset();
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, b ? b : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? HDG_ERR_OOM : HDG_ERR_CUDA,
+             std::string("cudaMalloc of ") + std::to_string(b) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    ptr = p;
+    bytes = b;
+}
+
+template <typename F>
+static hdg_status guarded(F&& f) {
+    try {
+        f();
+        return HDG_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return HDG_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return HDG_ERR_INVALID_ARG;
+    }
+}
+
+static void check_algorithm(const char* algorithm) {
+    HDG_REQUIRE(algorithm, HDG_ERR_INVALID_ARG, "null algorithm");
+    const std::string a = upper(algorithm);
+    if (a == "SUPER-GRID") return;
+    static const char* known[] = {"PQ", "PREFILTER", "SORTING", "PARAFILTER", "IVF-IVF_PQ",
+                                  "GRID-IVF_PQ", "CAGRA-POST", "IVFPQ-POST"};
+    for (const char* k : known)
+        if (a == k)
+            fail(HDG_ERR_UNSUPPORTED, std::string("algorithm '") + algorithm +
+                                          "' is not part of this build (only super-grid)");
+    fail(HDG_ERR_INVALID_ARG, std::string("Unknown index type: ") + algorithm);
+}
+
+static hdg_index* make_index(const std::string& conf, const std::string& filt) {
+    std::unique_ptr<hdg_index> idx(new hdg_index());
+    default_params(&idx->params);
+    parse_hdgrid_conf(conf, &idx->params);
+    parse_filter_conf(filt, &idx->filter);
+    HDG_REQUIRE(idx->params.filter_dim == 1 || idx->params.filter_dim == 2, HDG_ERR_INVALID_ARG,
+                "filter_dim must be 1 or 2");
+    CK(cudaGetDevice(&idx->device));
+    upload_filter(idx.get());
+    return idx.release();
+}
+
+}  // namespace hdg
+
+using namespace hdg;
+
+extern "C" {
+
+const char* hdg_last_error(void) { return g_last_error.c_str(); }
+const char* hdg_version(void) { return "hdgrid-b200 0.1.0 (sm_100a)"; }
+
+hdg_status hdg_create(const char* algorithm, const char* hdgrid_conf_path, const char* filter_conf_path,
+                      hdg_index** out) {
+    return guarded([&] {
+        HDG_REQUIRE(out && hdgrid_conf_path, HDG_ERR_INVALID_ARG, "null argument");
+        check_algorithm(algorithm);
+        const std::string conf = read_text_file(hdgrid_conf_path);
+        std::string fpath = filter_conf_path ? filter_conf_path : "";
+        if (fpath.empty()) {  // default <path>/filter.conf (search-engine-auto-batch.cu:134-140)
+            hdg_params p;
+            default_params(&p);
+            parse_hdgrid_conf(conf, &p);
+            fpath = std::string(p.path) + "filter.conf";
+        }
+        *out = make_index(conf, read_text_file(fpath));
+    });
+}
+
+hdg_status hdg_create_from_text(const char* algorithm, const char* conf, const char* filt, hdg_index** out) {
+    return guarded([&] {
+        HDG_REQUIRE(out && conf && filt, HDG_ERR_INVALID_ARG, "null argument");
+        check_algorithm(algorithm);
+        *out = make_index(conf, filt);
+    });
+}
+
+hdg_status hdg_destroy(hdg_index* index) {
+    return guarded([&] { delete index; });
+}
+
+hdg_status hdg_parse_config(const char* text, hdg_params* out) {
+    return guarded([&] {
+        HDG_REQUIRE(text && out, HDG_ERR_INVALID_ARG, "null argument");
+        default_params(out);
+        parse_hdgrid_conf(text, out);
+    });
+}
+
+hdg_status hdg_parse_filter(const char* text, hdg_filter_spec* out) {
+    static thread_local FilterSpec keep;
+    return guarded([&] {
+        HDG_REQUIRE(text && out, HDG_ERR_INVALID_ARG, "null argument");
+        parse_filter_conf(text, &keep);
+        std::memset(out, 0, sizeof(*out));
+        out->l = keep.l;
+        for (int i = 0; i < HDG_MAX_LABEL_DIMS; i++) {
+            out->type[i] = keep.type[i];
+            out->div_value[i] = keep.div_value[i];
+            out->shift_val[2 * i] = keep.shift_val[2 * i];
+            out->shift_val[2 * i + 1] = keep.shift_val[2 * i + 1];
+        }
+        out->n_map = (int32_t)keep.interval_map.size();
+        out->interval_map = keep.interval_map.data();
+    });
+}
+
+hdg_status hdg_get_params(const hdg_index* index, hdg_params* out) {
+    return guarded([&] {
+        HDG_REQUIRE(index && out, HDG_ERR_INVALID_ARG, "null argument");
+        *out = index->params;
+    });
+}
+
+hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t d, const float* d_labels,
+                     uint32_t l, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        build_index(index, d_data, n, d, d_labels, l, static_cast<cudaStream_t>(stream));
+    });
+}
+
+hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        reserve_workspace(index, max_queries, index->params.exps0 <= 1 ? 1 : 8192 - 256);
+    });
+}
+
+hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q, const float* d_query_labels,
+                     uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+                     void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        run_query(index, d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids,
+                  static_cast<cudaStream_t>(stream));
+    });
+}
+
+int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, int cap) {
+    if (!index) return 0;
+    const int n = std::min<int>(cap, (int)index->stage_ms.size());
+    for (int i = 0; i < n; i++) {
+        if (ms) ms[i] = index->stage_ms[i];
+        if (names) names[i] = index->stage_names[i].c_str();
+    }
+    return n;
+}
+
+hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst, size_t bytes,
+                           size_t* bytes_needed) {
+    return guarded([&] {
+        HDG_REQUIRE(index && name, HDG_ERR_INVALID_ARG, "null argument");
+        auto it = index->work_layout.find(name);
+        HDG_REQUIRE(it != index->work_layout.end(), HDG_ERR_INVALID_ARG,
+                    std::string("no workspace buffer named ") + name);
+        const size_t off = it->second.first, sz = it->second.second;
+        if (bytes_needed) *bytes_needed = sz;
+        if (!host_dst) return;
+        HDG_REQUIRE(bytes >= sz, HDG_ERR_INVALID_ARG, "destination too small");
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(host_dst, static_cast<const char*>(index->work.ptr) + off, sz, cudaMemcpyDeviceToHost));
+    });
+}
+
+hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out) {
+    return guarded([&] {
+        HDG_REQUIRE(index && out, HDG_ERR_INVALID_ARG, "null argument");
+        HDG_REQUIRE(index->built, HDG_ERR_STATE, "index not built");
+        std::memset(out, 0, sizeof(*out));
+        const HostIndex& H = index->host;
+        out->n = H.n;
+        out->d = H.d;
+        out->l = H.l;
+        out->M = H.M;
+        out->M_pad = H.M_pad;
+        out->n_lists = H.n_lists;
+        out->clusters = H.C;
+        out->tot_cells = H.grid.tot_cells;
+        for (int i = 0; i < HDG_MAX_LABEL_DIMS; i++) {
+            out->grid_dims[i] = H.grid.grid_dims[i];
+            out->shuffle[i] = H.grid.shuffle[i];
+            out->label_left[i] = H.grid.left[i];
+            out->label_span[i] = H.grid.span[i];
+        }
+        out->morton_dims = H.grid.morton_dims;
+        out->morton_max_bits = H.grid.morton_max_bits;
+        out->morton_valid_map = H.grid.morton_valid_map;
+        out->diff_dim = H.grid.diff_dim;
+        out->device_bytes = index->arena.bytes;
+    });
+}
+
+hdg_status hdg_save(const hdg_index* index, const char* path) {
+    return guarded([&] {
+        HDG_REQUIRE(index && path, HDG_ERR_INVALID_ARG, "null argument");
+        save_index(index, path);
+    });
+}
+
+hdg_status hdg_load(const char* path, hdg_index** out) {
+    return guarded([&] {
+        HDG_REQUIRE(path && out, HDG_ERR_INVALID_ARG, "null argument");
+        *out = load_index(path);
+    });
+}
+
+hdg_status hdg_pq_lut(const float* d_centers, const float* d_queries, uint64_t n_queries, uint32_t n_dim,
+                      uint32_t pq_dim, uint32_t pq_len, uint32_t n_codes, float* d_lut, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_centers && d_queries && d_lut, HDG_ERR_INVALID_ARG, "null pointer");
+        pq_lut(d_centers, d_queries, n_queries, n_dim, pq_dim, pq_len, n_codes, d_lut,
+               static_cast<cudaStream_t>(stream));
+    });
+}
+
+hdg_status hdg_pq_adc(const uint8_t* d_codebook, uint64_t tot_data, const float* d_lut, uint64_t n_queries,
+                      uint32_t pq_dim, uint32_t n_codes, const uint64_t* d_indices, uint64_t n_cand,
+                      float* d_dist, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_codebook && d_lut && d_dist, HDG_ERR_INVALID_ARG, "null pointer");
+        pq_adc(d_codebook, tot_data, d_lut, n_queries, pq_dim, n_codes, d_indices, n_cand, d_dist,
+               static_cast<cudaStream_t>(stream));
+    });
+}
+
+hdg_status hdg_label_mask(const float* d_ranges, const float* d_labels, uint32_t l, uint64_t n_data,
+                          uint64_t n_queries, const uint64_t* d_indices, uint64_t n_cand, int32_t* d_mask,
+                          void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_ranges && d_labels && d_mask, HDG_ERR_INVALID_ARG, "null pointer");
+        label_mask(d_ranges, d_labels, l, n_data, n_queries, d_indices, n_cand, d_mask,
+                   static_cast<cudaStream_t>(stream));
+    });
+}
+
+hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query_labels, uint64_t n_queries,
+                               float* d_ranges, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(spec && d_query_labels && d_ranges, HDG_ERR_INVALID_ARG, "null pointer");
+        HDG_REQUIRE(spec->l >= 1 && spec->l <= HDG_MAX_LABEL_DIMS, HDG_ERR_INVALID_ARG, "bad l");
+        DeviceBuffer map;
+        map.ensure(std::max<size_t>(16, (size_t)spec->n_map * 4));
+        if (spec->n_map)
+            CK(cudaMemcpy(map.ptr, spec->interval_map, (size_t)spec->n_map * 4, cudaMemcpyHostToDevice));
+        FilterDev f{};
+        f.l = spec->l;
+        bool range = false;
+        for (int i = 0; i < HDG_MAX_LABEL_DIMS; i++) {
+            f.type[i] = spec->type[i];
+            f.div_value[i] = spec->div_value[i] ? spec->div_value[i] : 1;
+            f.shift_val[2 * i] = spec->shift_val[2 * i];
+            f.shift_val[2 * i + 1] = spec->shift_val[2 * i + 1];
+            if (i < spec->l && spec->type[i] == 3) range = true;
+        }
+        f.filter_dim = range ? 2 : 1;
+        f.n_map = spec->n_map;
+        f.map = static_cast<const float*>(map.ptr);
+        recover_filters(f, d_query_labels, n_queries, d_ranges, static_cast<cudaStream_t>(stream));
+        CK(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    });
+}
+
+hdg_status hdg_bruteforce_knn(const float* d_data, uint64_t n, uint32_t d, const float* d_labels, uint32_t l,
+                              const float* d_queries, uint64_t q, const float* d_ranges, uint32_t k,
+                              float* d_dist, uint64_t* d_ids, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_data && d_labels && d_queries && d_ranges && d_dist && d_ids, HDG_ERR_INVALID_ARG,
+                    "null pointer");
+        bruteforce_knn(d_data, n, d, d_labels, l, d_queries, q, d_ranges, k, d_dist, d_ids,
+                       static_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Device-side building blocks shared by the build and query kernels.
+//
+// The integer stages (filter box, cell ids, Morton codes) follow the reference's float
+// semantics exactly so that cell boxes, Morton codes and counts are bit-identical:
+//   - filter recovery: denormalize_labels_kernel (src/core/preprocessing.cu:3-32)
+//   - cell id: get_grid_id_device (src/index/2-level_index/Super-Grid-IVF_PQ.cu:24-26)
+//   - cell box: get_filter_grid_ranges_kernel (Super-Grid-IVF_PQ.cu:930-961)
+//   - Morton: morton_encode (src/core/zorder.cu:3-15)
+// A C-style float->uint64 cast on the GPU is cvt.rzi.u64.f32, which saturates
+// (NaN and negatives -> 0, >= 2^64 -> UINT64_MAX); the kernels rely on that, exactly as
+// the reference does.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+#include "hdg_index.h"
+
+namespace hdg {
+
+// ---- filter recovery (preprocessing.cu:13-30) --------------------------------------
+// x points at the query's label row; returns [lo, hi] for label dim i.
+__device__ __forceinline__ void recover_dim(const FilterDev& f, const float* row, int i, float* lo,
+                                            float* hi) {
+    const int t = f.type[i];
+    if (t == 0) {
+        // max(float, double) promotes to double; the result is rounded back to f32.
+        const float x = row[i];
+        const double sl = fmax((double)f.shift_val[2 * i], 1e-7);
+        const double sr = fmax((double)f.shift_val[2 * i + 1], 1e-7);
+        *lo = (float)((double)x - sl);
+        *hi = (float)((double)x + sr);
+    } else if (t == 1) {
+        const int v = (int)(row[i] - 1.0f);
+        if (v >= 0 && 2 * v + 1 < f.n_map) {
+            *lo = f.map[2 * v];
+            *hi = f.map[2 * v + 1];
+        } else {  // out-of-table label: the reference reads out of bounds; empty box here
+            *lo = FLT_MAX;
+            *hi = -FLT_MAX;
+        }
+    } else if (t == 2) {
+        const int v = (int)row[i];
+        *lo = (float)(v / f.div_value[i]);
+        *hi = FLT_MAX;
+    } else {
+        // type 3 reads a [lo, hi] pair from a filter_dim = 2 label row (preprocessing.cu:27-28)
+        *lo = row[2 * i];
+        *hi = row[2 * i + 1];
+    }
+}
+
+// ---- grid cells (Super-Grid-IVF_PQ.cu:24-26) ----------------------------------------
+// ((uint64_t)((x - l) * M)) / len, returned as int (truncating), float arithmetic.
+__device__ __forceinline__ int grid_id(float x, uint64_t left, uint64_t len, int M) {
+    const float t = __fmul_rn(__fsub_rn(x, (float)left), (float)M);
+    const uint64_t u = (uint64_t)t;  // saturating cvt.rzi.u64.f32
+    return (int)(u / len);
+}
+
+// Cell box of one shuffled dim (Super-Grid-IVF_PQ.cu:947-960).
+__device__ __forceinline__ void cell_range(float box_lo, float box_hi, uint64_t left, uint64_t span,
+                                           int M, int* out_lo, int* out_hi) {
+    const uint64_t blo = (uint64_t)box_lo;  // saturating
+    const uint64_t bhi = (uint64_t)box_hi;
+    const float l = (float)(blo > left ? blo : left);
+    const uint64_t rr = left + span;
+    const float r = (float)(bhi < rr ? bhi : rr);
+    const int gl = grid_id(l, left, span, M);
+    const int gr = grid_id(r, left, span, M);
+    int hi = gr < M - 1 ? gr : M - 1;
+    int lo = hi < gl ? hi : gl;
+    // The int truncation can only go negative when the uint64 cell value reaches 2^31,
+    // where the reference indexes out of bounds; clamp to a valid cell instead.
+    if (hi < 0) hi = 0;
+    if (lo < 0) lo = 0;
+    *out_hi = hi;
+    *out_lo = lo;
+}
+
+// ---- Morton (zorder.cu:3-15): MSB-first bit interleave over valid dims -------------
+__device__ __forceinline__ uint64_t morton_encode(const int* coords, int dims, int max_bits,
+                                                  int valid_map) {
+    uint64_t code = 0;
+    for (int b = 0; b < max_bits; ++b) {
+        for (int i = 0; i < dims; ++i) {
+            if (!((valid_map >> i) & 1)) continue;
+            const int bit = (coords[i] >> (max_bits - 1 - b)) & 1;
+            code = (code << 1) | (uint64_t)bit;
+        }
+    }
+    return code;
+}
+
+// ---- distances --------------------------------------------------------------------
+// Exact f32 L2 in the reference's order (refine.cu:71-88 with d <= 512): each squared
+// difference rounded to f32, then summed sequentially in dimension order.
+__device__ __forceinline__ float seq_l2(const float* __restrict__ a, const float* __restrict__ b,
+                                        int d) {
+    float s = 0.f;
+    for (int i = 0; i < d; ++i) {
+        const float t = __fsub_rn(a[i], b[i]);
+        s = __fadd_rn(s, __fmul_rn(t, t));
+    }
+    return s;
+}
+
+// Monotone map float -> u32 (ascending order preserved, +inf largest finite key).
+__device__ __forceinline__ uint32_t float_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+    const uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+// In-place ascending bitonic sort of n (power of two) u64 keys in shared memory.
+// Must be called by all threads of the block.
+__device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < (n >> 1); i += blockDim.x) {
+                const int lo = 2 * i - (i & (j - 1));
+                const int hi = lo + j;
+                const bool up = ((lo & k) == 0);
+                const uint64_t a = keys[lo], b = keys[hi];
+                if ((a > b) == up) {
+                    keys[lo] = b;
+                    keys[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace hdg

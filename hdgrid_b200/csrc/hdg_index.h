@@ -1,0 +1,115 @@
+// Device-resident layout of a built HDGrid index and the host object that owns it.
+//
+// HBM layout (one arena per index, 256-byte aligned sub-buffers):
+//   centers      f32 [C x d]            coarse centroids (src/index/2-level_index/Super-Grid-IVF_PQ.cuh:77)
+//   sub_centers  f32 [L x d]            one centroid per inverted list, grouped by cluster (:72)
+//   centers_bf16 / sub_centers_bf16     BF16 copies for the tensor-core coarse GEMM
+//   cnorm        f32 [C + L]            squared norms of the centroids (GEMM epilogue)
+//   cluster_off  u32 [C + 1]            list range of each cluster (sub_cluster_offsets/counts, :78-79)
+//   list_off     u32 [L + 1]            pool range of each list (zorder_array_offsets/lengthes, :70-71)
+//   zcodes       u64 [N]                Morton code of every point, sorted inside each list (:69)
+//   ids          u32 [N]                original point id in pool order (zorder_node_arrays, :68)
+//   codes        u8  [N x M_pad]        PQ codes in pool order, one 16-byte-aligned row per point
+//   labels       f32 [N x l]            labels in pool order (read by the fused predicate)
+//   pq_centers   f32 [M x 256 x pq_len] PQ codebooks (pq::index_data_t::centers, product-quantization.cuh:9)
+//   prefix       u32 [cells x L]        inclusive multi-dim prefix counts per list, cell-major,
+//                                       list fastest (dense form of compressed_sums, :67)
+// L = C*S inverted lists; N points; M PQ subspaces; M_pad = M rounded up to 16.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "hdg_common.h"
+
+namespace hdg {
+
+constexpr int kMaxDims = HDG_MAX_LABEL_DIMS;
+constexpr int kCodes = 256;
+
+// Label grid + Morton configuration (calc_grid_shape, Super-Grid-IVF_PQ.cu:305-412).
+// Dims are stored in "shuffled" order (label dims sorted by span, ascending).
+struct GridMeta {
+    int l = 0;
+    int grid_dims[kMaxDims] = {0};
+    int shuffle[kMaxDims] = {0};          // shuffled position -> original label dim
+    uint64_t left[kMaxDims] = {0};        // floor(min label)
+    uint64_t span[kMaxDims] = {0};        // ceil(max) - floor(min)
+    uint64_t cell_stride[kMaxDims] = {0}; // row-major strides, last dim fastest
+    uint64_t tot_cells = 0;
+    int morton_dims = 0, morton_max_bits = 0, morton_valid_map = 0;
+    int diff_dim = 0;
+};
+
+// filter.conf on the device (passed by value; the map table lives in the arena).
+struct FilterDev {
+    int l;
+    int filter_dim;
+    int type[kMaxDims];
+    float shift_val[2 * kMaxDims];
+    int div_value[kMaxDims];
+    int n_map;
+    const float* map;
+};
+
+struct IndexDev {
+    uint32_t n, d, l, M, M_pad, pq_len, n_lists, C, S_max;
+    const float* centers;
+    const float* sub_centers;
+    const uint16_t* centers_bf16;
+    const uint16_t* sub_centers_bf16;
+    const float* cnorm;
+    const uint32_t* cluster_off;
+    const uint32_t* list_off;
+    const uint64_t* zcodes;
+    const uint32_t* ids;
+    const uint8_t* codes;
+    const float* labels;
+    const float* pq_centers;
+    const uint32_t* prefix;
+};
+
+// Host-side copy of every index array (build output, save/load payload).
+struct HostIndex {
+    uint64_t n = 0, d = 0, l = 0, M = 0, M_pad = 0, pq_len = 0, n_lists = 0, C = 0;
+    GridMeta grid;
+    std::vector<float> centers, sub_centers, pq_centers;
+    std::vector<uint32_t> cluster_off, list_off, ids, prefix;
+    std::vector<uint64_t> zcodes;
+    std::vector<uint8_t> codes;
+    std::vector<float> labels;
+};
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reset();
+    void ensure(size_t b);  // grow-only cudaMalloc
+    ~DeviceBuffer() { reset(); }
+};
+
+}  // namespace hdg
+
+struct hdg_index {
+    hdg_params params{};
+    hdg::FilterSpec filter;
+    bool built = false;
+    hdg::HostIndex host;           // kept for save() and the debug/oracle handoff
+    hdg::GridMeta grid;
+    hdg::IndexDev dev{};
+    hdg::DeviceBuffer arena;       // all index arrays
+    hdg::DeviceBuffer map_buf;     // filter interval map
+    hdg::DeviceBuffer work;        // per-query workspace
+    uint64_t work_queries = 0;
+    std::map<std::string, std::pair<size_t, size_t>> work_layout;  // name -> (offset, bytes)
+    int device = 0;
+    // stage timing (break_down=1)
+    std::vector<std::string> stage_names;
+    std::vector<float> stage_ms;
+    // last-query scalars (host copy)
+    uint64_t last_q = 0, last_ncand = 0;
+    float last_beta = 0.f;
+};

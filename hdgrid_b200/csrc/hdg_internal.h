@@ -1,0 +1,62 @@
+// Internal declarations shared by the translation units of libhdgrid.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "hdg_index.h"
+
+namespace hdg {
+
+inline void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        const hdg_status s = (e == cudaErrorMemoryAllocation) ? HDG_ERR_OOM : HDG_ERR_CUDA;
+        throw Error(s, std::string(what) + " failed: " + cudaGetErrorString(e) + " (" + file + ":" +
+                           std::to_string(line) + ")");
+    }
+}
+#define CK(x) ::hdg::check_cuda((x), #x, __FILE__, __LINE__)
+#define CK_LAUNCH() ::hdg::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+// RAII device allocation used by the build (never on the query path).
+template <typename T>
+struct DevMem {
+    T* p = nullptr;
+    explicit DevMem(uint64_t count) {
+        if (count) CK(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count));
+    }
+    ~DevMem() {
+        if (p) cudaFree(p);
+    }
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+};
+
+GridMeta compute_grid_shape(const std::vector<float>& mins, const std::vector<float>& maxs, int l,
+                            uint64_t max_grids, uint64_t label_mask_bits);
+void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, const float* d_labels,
+                 uint32_t l, cudaStream_t st);
+void upload_index(hdg_index* idx, cudaStream_t st);
+void upload_filter(hdg_index* idx);
+FilterDev filter_dev(const hdg_index* idx);
+void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand);
+void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+               uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+               cudaStream_t st);
+void save_index(const hdg_index* idx, const std::string& path);
+hdg_index* load_index(const std::string& path);
+
+// kernel-level entry points (hdg_kernels_ref.cu)
+void pq_lut(const float* centers, const float* queries, uint64_t nq, uint32_t n_dim, uint32_t pq_dim,
+            uint32_t pq_len, uint32_t n_codes, float* lut, cudaStream_t st);
+void pq_adc(const uint8_t* codebook, uint64_t tot_data, const float* lut, uint64_t nq, uint32_t pq_dim,
+            uint32_t n_codes, const uint64_t* indices, uint64_t n_cand, float* dist, cudaStream_t st);
+void label_mask(const float* ranges, const float* labels, uint32_t l, uint64_t n_data, uint64_t nq,
+                const uint64_t* indices, uint64_t n_cand, int32_t* mask, cudaStream_t st);
+void recover_filters(const FilterDev& f, const float* qlabels, uint64_t nq, float* ranges,
+                     cudaStream_t st);
+void bruteforce_knn(const float* data, uint64_t n, uint32_t d, const float* labels, uint32_t l,
+                    const float* queries, uint64_t q, const float* ranges, uint32_t k, float* dist,
+                    uint64_t* ids, cudaStream_t st);
+
+}  // namespace hdg

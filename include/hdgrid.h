@@ -1,0 +1,188 @@
+/*
+ * hdgrid.h -- C ABI of the B200-native HDGrid ("super-grid") filtered ANN index.
+ *
+ * Every entry point is plain C: opaque handles, raw pointers, sizes and a status code.
+ * Pointers named d_* are DEVICE pointers owned by the caller (the index never frees
+ * them).  Streams are passed as `void*` holding a cudaStream_t (NULL = legacy stream).
+ *
+ * Reference interfaces replaced (paths inside the HDGrid project):
+ *   hdg_create*      config_factory::create + index_factory::create
+ *                    (src/index/index-factory.cuh:10-87), HDGrid.conf reader
+ *                    (src/utils/config_utils.h:33-88), filter.conf reader (:121-172)
+ *   hdg_build        super_grid::index::build (src/index/2-level_index/Super-Grid-IVF_PQ.cu:420-646)
+ *                    through index_base_t::build (src/core/interfaces.cuh:30)
+ *   hdg_query        super_grid::index::query (Super-Grid-IVF_PQ.cu:985-1249)
+ *                    through index_base_t::query (src/core/interfaces.cuh:31)
+ *   hdg_pq_lut       build_pq_lut_kernel (src/index/product-quantization.cu:4-35)
+ *   hdg_pq_adc       compute_batched_L2_distance_kernel (product-quantization.cu:37-77)
+ *   hdg_label_mask   label_matrix_by_filter_indices_kernel (src/core/filter.cu:30-64)
+ *   hdg_recover_filters  recovery_filters / denormalize_labels_kernel (src/core/preprocessing.cu:3-32,206-230)
+ *   hdg_bruteforce_knn   brute_forece_vector_search (src/verification/ground_truth.cuh:165-232),
+ *                    generalised to the filter.conf predicate
+ *   hdg_save/hdg_load    no counterpart: the reference rebuilds the index every run
+ *                    (src/search-engine/search-engine-auto-batch.cu:266-274)
+ */
+#ifndef HDGRID_H_
+#define HDGRID_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference exits the process on any CUDA error
+ * (src/utils/debugging_utils.cuh:11-20); every entry point here returns instead. */
+typedef enum hdg_status {
+    HDG_OK = 0,
+    HDG_ERR_INVALID_ARG = 1,
+    HDG_ERR_IO = 2,
+    HDG_ERR_CUDA = 3,
+    HDG_ERR_OOM = 4,
+    HDG_ERR_TIMEOUT = 5,
+    HDG_ERR_UNSUPPORTED = 6,
+    HDG_ERR_STATE = 7
+} hdg_status;
+
+typedef struct hdg_index hdg_index;
+
+#define HDG_MAX_LABEL_DIMS 8
+
+/* Index and search parameters: the union of the HDGrid.conf keys read by
+ * common_config (config_utils.h:97-108), pq::config_t (product-quantization.cuh:33-35)
+ * and super_grid::config_t (Super-Grid-IVF_PQ.cuh:47-54), plus the B200 precision switches. */
+typedef struct hdg_params {
+    uint64_t topk;          /* TOPK */
+    uint64_t filter_dim;    /* FILTER_DIM: label columns per label dim in the query labels (1 or 2) */
+    uint64_t pq_dim;        /* PQ_DIM: number of PQ subspaces M */
+    uint64_t n_clusters;    /* N_CLUSTERS: PQ codebook size (only 256 is supported) */
+    uint64_t exps0;         /* EXPS0: refine ratio; <=1 selects the pre-filter schedule */
+    uint64_t clusters;      /* CLUSTERS: coarse clusters C */
+    uint64_t sub_clusters;  /* SUB_CLUSTERS: inverted lists per cluster S (C*S lists in total) */
+    uint64_t max_grids;     /* MAX_GRIDS: label-grid cell budget */
+    uint64_t n_list;        /* N_LIST: coarse clusters probed per query */
+    uint64_t sub_lists;     /* SUB_LISTS: inverted lists probed per query */
+    uint64_t n_split;       /* N_SPLIT: Morton sub-ranges per probed list when is_split=1 */
+    uint64_t label_mask;    /* LABEL_MASK: bit i set = label dim i left out of the grid */
+    uint64_t is_split;      /* IS_SPLIT */
+    uint64_t break_down;    /* BREAK_DOWN: per-stage timing log */
+    uint64_t enable_multi_gpu, mem_bound, is_calc_mem_predictor_coeff, lowest_query_batch;
+    uint64_t data_width, index_width;  /* accepted and ignored, as in the reference */
+    char path[512];         /* PATH: dataset directory */
+    /* B200 precision / schedule switches (not HDGrid.conf keys of the reference; the
+     * conf reader accepts them under the same names in upper case). */
+    uint64_t lut_fp16;      /* LUT_FP16: store the PQ LUT in FP16 (FP32 accumulation) */
+    uint64_t coarse_bf16;   /* COARSE_BF16: coarse assignment as a BF16 tensor-core GEMM */
+    uint64_t kmeans_iters;  /* KMEANS_ITERS: Lloyd iterations of the index build (default 20) */
+    uint64_t seed;          /* SEED: build RNG seed (default 1234) */
+} hdg_params;
+
+/* filter.conf contents (config_utils.h:112-172).  interval_map is the flat
+ * concatenation of every map filter's table, exactly as the reference uploads it
+ * (preprocessing.cu:145-150). */
+typedef struct hdg_filter_spec {
+    int32_t l;
+    int32_t type[HDG_MAX_LABEL_DIMS];
+    float shift_val[2 * HDG_MAX_LABEL_DIMS];
+    int32_t div_value[HDG_MAX_LABEL_DIMS];
+    int32_t n_map;
+    const float* interval_map; /* host pointer, n_map floats; copied by the callee */
+} hdg_filter_spec;
+
+/* ---- lifetime ---------------------------------------------------------------- */
+
+/* algorithm: "super-grid" (case-insensitive, so the README's "Super-Grid" works too).
+ * Other algorithm names of the reference return HDG_ERR_UNSUPPORTED. */
+hdg_status hdg_create(const char* algorithm, const char* hdgrid_conf_path,
+                      const char* filter_conf_path, hdg_index** out);
+/* Same, with the two files' contents passed as strings. */
+hdg_status hdg_create_from_text(const char* algorithm, const char* hdgrid_conf_text,
+                                const char* filter_conf_text, hdg_index** out);
+hdg_status hdg_destroy(hdg_index* index);
+
+/* Parse an HDGrid.conf / filter.conf text without creating an index. */
+hdg_status hdg_parse_config(const char* hdgrid_conf_text, hdg_params* out);
+/* interval_map of *out points into storage owned by the library until the next call. */
+hdg_status hdg_parse_filter(const char* filter_conf_text, hdg_filter_spec* out);
+hdg_status hdg_get_params(const hdg_index* index, hdg_params* out);
+
+/* ---- build / query --------------------------------------------------------------- */
+
+/* d_data [n x d] f32 row-major, d_labels [n x l] f32 row-major (l = filter.conf's l). */
+hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t d,
+                     const float* d_labels, uint32_t l, void* stream);
+
+/* Pre-size the query workspace for batches of up to max_queries, so that later
+ * hdg_query calls on such batches allocate nothing. */
+hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries);
+
+/* d_queries [q x d] f32; d_query_labels [q x label_cols] f32 with label_cols = l*filter_dim;
+ * d_data is the base set [n x d] (used by the exact re-rank, as query_input_t::dataset).
+ * Outputs d_dist [q x k] f32 (ascending) and d_ids [q x k] u64.  Slots without a
+ * result hold id UINT64_MAX and distance +inf. */
+hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q,
+                     const float* d_query_labels, uint32_t label_cols, const float* d_data,
+                     uint32_t k, float* d_dist, uint64_t* d_ids, void* stream);
+
+/* Per-stage device timings (ms) of the last hdg_query when break_down=1; returns the
+ * number of stages written (<= cap) and their names via names (may be NULL). */
+int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, int cap);
+
+/* Copy a named intermediate buffer of the last query to host memory (parity tests).
+ * Names: "box", "cells", "zrange", "list_counts", "cluster_counts", "probe_clusters",
+ * "probe_lists", "range_start", "range_len", "cand_pool", "cand_count", "scalars". */
+hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,
+                           size_t bytes, size_t* bytes_needed);
+
+/* Index geometry: n_lists, C, M, l, grid dims, Morton bits, ... (host copy). */
+typedef struct hdg_index_info {
+    uint64_t n, d, l, M, M_pad, n_lists, clusters;
+    uint64_t tot_cells;
+    int32_t grid_dims[HDG_MAX_LABEL_DIMS];
+    int32_t shuffle[HDG_MAX_LABEL_DIMS];
+    uint64_t label_left[HDG_MAX_LABEL_DIMS];
+    uint64_t label_span[HDG_MAX_LABEL_DIMS];
+    int32_t morton_dims, morton_max_bits, morton_valid_map, diff_dim;
+    uint64_t device_bytes;
+} hdg_index_info;
+hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out);
+
+/* ---- persistence ------------------------------------------------------------------ */
+
+hdg_status hdg_save(const hdg_index* index, const char* path);
+hdg_status hdg_load(const char* path, hdg_index** out);
+
+/* ---- kernel-level entry points (the reference's kernels, same data layouts) -------- */
+
+/* LUT[q][m][c] = sum_t (centers[m][c][t] - queries[q][m*pq_len+t])^2 ; f32. */
+hdg_status hdg_pq_lut(const float* d_centers, const float* d_queries, uint64_t n_queries,
+                      uint32_t n_dim, uint32_t pq_dim, uint32_t pq_len, uint32_t n_codes,
+                      float* d_lut, void* stream);
+/* dist[q][j] = sum_m lut[q][m][codebook[m*tot_data + idx]], idx = indices[q*n_cand+j]
+ * (or j when d_indices is NULL); idx >= tot_data gives FLT_MAX.  Column-major codes. */
+hdg_status hdg_pq_adc(const uint8_t* d_codebook, uint64_t tot_data, const float* d_lut,
+                      uint64_t n_queries, uint32_t pq_dim, uint32_t n_codes,
+                      const uint64_t* d_indices, uint64_t n_cand, float* d_dist, void* stream);
+/* mask[q][j] = AND_i (ranges[q][2i] <= labels[idx][i] <= ranges[q][2i+1]); idx >= n_data gives 0. */
+hdg_status hdg_label_mask(const float* d_ranges, const float* d_labels, uint32_t l,
+                          uint64_t n_data, uint64_t n_queries, const uint64_t* d_indices,
+                          uint64_t n_cand, int32_t* d_mask, void* stream);
+/* filters [q x 2l] f32 from the query labels and a filter spec. */
+hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query_labels,
+                               uint64_t n_queries, float* d_ranges, void* stream);
+/* Exact filtered kNN in FP32: distances of every base vector whose labels pass the
+ * per-query box d_ranges [q x 2l]; k smallest, ascending, ties by lower id. */
+hdg_status hdg_bruteforce_knn(const float* d_data, uint64_t n, uint32_t d,
+                              const float* d_labels, uint32_t l, const float* d_queries,
+                              uint64_t q, const float* d_ranges, uint32_t k,
+                              float* d_dist, uint64_t* d_ids, void* stream);
+
+/* Thread-local message of the last failing call. */
+const char* hdg_last_error(void);
+const char* hdg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HDGRID_H_ */

@@ -1,0 +1,219 @@
+"""GPU path (libhdgrid through the C ABI) against the CPU oracle on the same index.
+
+Integer stages -- filter boxes, cell boxes, Morton codes, per-list counts, probe lists,
+Morton candidate ranges, pool layout -- must be bit-identical.  Final results: distances
+within 1e-4 relative of FP64, recall within 0.002 of the oracle's own search.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from hdgrid_b200 import datasets
+from tests.helpers import build_gpu, exact_l2_f64, fetch_trace, query_gpu, save_and_open_oracle
+
+KATS = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
+pytestmark = pytest.mark.gpu
+INV = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _t(a, dev, dtype=None):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.to(dev) if dtype is None else t.to(dev, dtype)
+
+
+# ---- the reference's known-answer vectors through the GPU kernels ------------------------
+
+def test_gpu_pq_lut_kat(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    k = KATS["pq_lut"]
+    c = _t(np.array(k["centers"], np.float32), cuda)
+    q = _t(np.array(k["queries"], np.float32).reshape(k["n_queries"], -1), cuda)
+    out = torch.empty(k["n_queries"] * k["pq_dim"] * k["n_codes"], device=cuda)
+    hg.pq_lut(c, q, k["pq_dim"], k["pq_len"], k["n_codes"], out)
+    np.testing.assert_allclose(out.cpu().numpy(), k["expected"], atol=k["tolerance"], rtol=0)
+
+
+def test_gpu_pq_adc_kat(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    k = KATS["pq_adc"]
+    cb = _t(np.array(k["codebook_colmajor"], np.uint8), cuda)
+    lut = _t(np.array(k["lut"], np.float32), cuda)
+    out = torch.empty(k["n_queries"] * k["n_data"], device=cuda)
+    hg.pq_adc(cb, k["n_data"], lut, k["n_queries"], k["pq_dim"], k["n_codes"], None, k["n_data"], out)
+    np.testing.assert_allclose(out.cpu().numpy(), k["expected"], atol=k["tolerance"], rtol=0)
+
+
+def test_gpu_label_predicate_kat(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    k = KATS["label_predicate"]
+    nq, nc, l = k["n_queries"], k["n_candi"], k["l"]
+    rng = _t(np.array(k["constraints"], np.float32), cuda)
+    lab = _t(np.array(k["candidate_labels"], np.float32), cuda)
+    idx = _t(np.arange(nq * nc, dtype=np.int64), cuda)
+    out = torch.empty(nq * nc, dtype=torch.int32, device=cuda)
+    hg.label_mask(rng, lab, l, nq * nc, nq, idx, nc, out)
+    assert out.cpu().tolist() == k["expected_kept"]
+
+
+def test_gpu_recover_filters_bit_exact(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    import oracle
+    ws = datasets.config2(scale=0.005, n_queries=300)
+    ql = _t(ws["query_labels"], cuda)
+    out = torch.empty((300, 6), device=cuda)
+    hg.recover_filters(ws["filter_conf"], ql, out)
+    spec = hg.parse_filter(ws["filter_conf"])
+    ref = oracle.recover_filters(spec, ws["query_labels"])
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_gpu_bruteforce_matches_fp64_oracle(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    import oracle
+    ws = datasets.config1(scale=0.05, n_queries=64)
+    spec = hg.parse_filter(ws["filter_conf"])
+    ranges = oracle.recover_filters(spec, ws["query_labels"])
+    d64, i64 = oracle.bruteforce_f64(ws["base"], ws["labels"], ws["queries"], ranges, 50)
+    dist = torch.empty((64, 50), device=cuda)
+    ids = torch.empty((64, 50), dtype=torch.int64, device=cuda)
+    hg.bruteforce_knn(_t(ws["base"], cuda), _t(ws["labels"], cuda), _t(ws["queries"], cuda), _t(ranges, cuda), 50,
+                      dist, ids)
+    gi = ids.cpu().numpy().view(np.uint64)
+    assert datasets.recall(gi, i64) >= 0.999
+    ok = np.isfinite(d64)
+    np.testing.assert_allclose(dist.cpu().numpy()[ok], d64[ok], rtol=1e-4, atol=1e-5)
+
+
+# ---- end-to-end parity on the GPU-built index --------------------------------------------
+
+def _parity(ws, cuda, min_recall=None, exact_ids=False):
+    import hdgrid_b200 as hg
+    import oracle
+    k = ws["k"]
+    idx, base, labels = build_gpu(ws, cuda)
+    g_dist, g_ids = query_gpu(idx, base, ws, k, cuda)
+    nq = ws["queries"].shape[0]
+    tr = fetch_trace(idx, nq)
+    ora, path = save_and_open_oracle(idx)
+    assert ora.check_layout() == 0, "pool layout / Morton codes / prefix counts differ from the labels"
+    o_dist, o_ids, otr = ora.query(ws["queries"], ws["query_labels"], ws["base"], k)
+    for name in ("box", "cells", "zrange", "list_counts", "probe_clusters", "probe_lists", "range_start",
+                 "range_len"):
+        a, b = tr[name], otr[name]
+        assert a.shape == b.shape, name
+        if a.dtype == np.float32:
+            a, b = a.view(np.uint32), b.view(np.uint32)
+        mism = np.argwhere(a != b)
+        assert mism.size == 0, f"{name} differs at {mism[:5].tolist()}"
+    # ground truth: FP64 filtered brute force with the f32 predicate
+    spec = hg.parse_filter(ws["filter_conf"])
+    fd = int(hg.parse_config(ws["hdgrid_conf"])["filter_dim"])
+    ranges = oracle.recover_filters(spec, ws["query_labels"], filter_dim=fd)
+    _, gt = oracle.bruteforce_f64(ws["base"], ws["labels"], ws["queries"], ranges, k)
+    r_gpu, r_ora = datasets.recall(g_ids, gt), datasets.recall(o_ids, gt)
+    assert abs(r_gpu - r_ora) <= 0.002, (r_gpu, r_ora)
+    if min_recall is not None:
+        assert r_gpu >= min_recall, r_gpu
+    same = np.mean([set(a.tolist()) == set(b.tolist()) for a, b in zip(g_ids, o_ids)])
+    assert same >= (1.0 if exact_ids else 0.98), same
+    # final distances within 1e-4 relative of FP64 for every returned id
+    ex = exact_l2_f64(ws["base"], ws["queries"], g_ids)
+    valid = g_ids != INV
+    if hg.parse_config(ws["hdgrid_conf"])["exps0"] > 1:
+        rel = np.abs(g_dist[valid] - ex[valid]) / np.maximum(ex[valid], 1e-12)
+        assert rel.max() <= 1e-4, rel.max()
+    assert np.all(np.isinf(g_dist[~valid]))
+    return idx, dict(r_gpu=r_gpu, r_ora=r_ora, g_ids=g_ids, g_dist=g_dist, o_ids=o_ids, o_dist=o_dist, path=path)
+
+
+def test_parity_config1_small(cuda):
+    ws = datasets.config1(scale=0.05, n_queries=200, max_grids=100_000)
+    _parity(ws, cuda)
+
+
+def test_parity_config1_full(cuda):
+    ws = datasets.config1()
+    _, r = _parity(ws, cuda, min_recall=0.9)
+
+
+def test_parity_config2_small_postfilter(cuda):
+    ws = datasets.config2(scale=0.01, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000)
+    _parity(ws, cuda)
+
+
+def test_parity_config4_small_range_filters(cuda):
+    ws = datasets.config4(scale=0.002, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=4096)
+    _parity(ws, cuda)
+
+
+def test_parity_prefilter_exact(cuda):
+    # exps0 <= 1: predicate before ADC, ADC distances are the output; the ADC sums run in
+    # the reference's subspace order on both sides, so ids and distances match exactly
+    ws = datasets.config2(scale=0.01, n_queries=200, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000, exps0=1)
+    _, r = _parity(ws, cuda)
+    valid = r["g_ids"] != INV
+    assert np.array_equal(r["g_ids"], r["o_ids"])
+    assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+
+
+def test_parity_masked_label_dim(cuda):
+    ws = datasets.config2(scale=0.01, n_queries=150, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000, label_mask=0b010)
+    _parity(ws, cuda)
+
+
+def test_save_load_roundtrip_identical(cuda):
+    import hdgrid_b200 as hg
+    ws = datasets.config1(scale=0.03, n_queries=64, max_grids=50_000)
+    idx, base, _ = build_gpu(ws, cuda)
+    d1, i1 = query_gpu(idx, base, ws, ws["k"], cuda)
+    ora, path = save_and_open_oracle(idx)
+    idx2 = hg.SuperGridIndex.load(path)
+    d2, i2 = query_gpu(idx2, base, ws, ws["k"], cuda)
+    assert np.array_equal(i1, i2) and np.array_equal(d1.view(np.uint32), d2.view(np.uint32))
+    assert idx2.info()["tot_cells"] == idx.info()["tot_cells"]
+
+
+# ---- edge cases ------------------------------------------------------------------------
+
+def test_empty_filter_and_short_results(cuda):
+    ws = datasets.config1(scale=0.03, n_queries=8, max_grids=50_000)
+    # query 0: label far outside the data -> box matches nothing in the predicate
+    ws["query_labels"][0, 0] = 5e7
+    # query 1: a zero-width window (shift is raised to 1e-7 both sides) -> at most a few
+    idx, base, _ = build_gpu(ws, cuda)
+    ws2 = dict(ws)
+    ws2["filter_conf"] = "l = 1\nfilter0:\n\ttype = 0\n\tshift_val = [0, 0]\n"
+    idx2, base2, _ = build_gpu(ws2, cuda)
+    d, i = query_gpu(idx2, base2, ws2, ws2["k"], cuda)
+    assert np.all((i[:, -1] == INV)), "a point-window filter cannot return 100 results"
+    assert np.all(np.isinf(d[i == INV]))
+
+
+def test_query_errors_are_status_codes(cuda):
+    import torch
+    import hdgrid_b200 as hg
+    ws = datasets.config1(scale=0.03, n_queries=4, max_grids=50_000)
+    idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
+    q = torch.zeros((4, 128), device=cuda)
+    ql = torch.zeros((4, 1), device=cuda)
+    out_d = torch.empty((4, 10), device=cuda)
+    out_i = torch.empty((4, 10), dtype=torch.int64, device=cuda)
+    with pytest.raises(hg.HDGError) as e:  # not built yet
+        idx.query(hg.query_input_t(q, q, ql), hg.query_output_t(out_d, out_i))
+    assert e.value.status == 7
+    base = torch.from_numpy(ws["base"]).to(cuda)
+    with pytest.raises(hg.HDGError) as e:  # labels with the wrong number of dims
+        idx.build(hg.build_input_t(base, torch.zeros((base.shape[0], 2), device=cuda)))
+    assert e.value.status == 1
