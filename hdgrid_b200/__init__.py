@@ -62,7 +62,7 @@ class HDGError(RuntimeError):
 
 def _load() -> C.CDLL:
     if not _LIB_PATH.exists():
-        raise ImportError(f"{_LIB_PATH} is missing: run `python -m hdgrid_b200.build_native` "
+        raise ImportError(f"{_LIB_PATH} is missing: run `python hdgrid_b200/build_native.py` "
                           "(the package has no CPU fallback)")
     lib = C.CDLL(str(_LIB_PATH))
     vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int32
@@ -73,6 +73,7 @@ def _load() -> C.CDLL:
         "hdg_parse_config": [C.c_char_p, C.POINTER(hdg_params)],
         "hdg_parse_filter": [C.c_char_p, C.POINTER(hdg_filter_spec)],
         "hdg_get_params": [vp, C.POINTER(hdg_params)],
+        "hdg_set_param": [vp, C.c_char_p, u64],
         "hdg_build": [vp, vp, u64, u32, vp, u32, vp],
         "hdg_reserve": [vp, u64],
         "hdg_query": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp],
@@ -94,6 +95,8 @@ def _load() -> C.CDLL:
     lib.hdg_version.restype = C.c_char_p
     lib.hdg_last_stage_times.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.c_int]
     lib.hdg_last_stage_times.restype = C.c_int
+    lib.hdg_last_query_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.c_int]
+    lib.hdg_last_query_stats.restype = C.c_int
     return lib
 
 
@@ -212,8 +215,9 @@ class SuperGridIndex:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            LIB.hdg_destroy(h)
+        lib = globals().get("LIB")
+        if h is not None and h.value and lib is not None:  # LIB is gone at interpreter exit
+            lib.hdg_destroy(h)
             self._h = C.c_void_p()
 
     @property
@@ -227,6 +231,9 @@ class SuperGridIndex:
         out = {f: getattr(p, f) for f, _ in hdg_params._fields_ if f != "path"}
         out["path"] = p.path.decode()
         return out
+
+    def set_param(self, key: str, value: int) -> None:
+        _check(LIB.hdg_set_param(self._h, key.encode(), int(value)))
 
     @property
     def topk(self) -> int:
@@ -271,6 +278,14 @@ class SuperGridIndex:
         buf = np.empty(need.value, dtype=np.uint8)
         _check(LIB.hdg_debug_fetch(self._h, name.encode(), buf.ctypes.data, buf.nbytes, None))
         return buf
+
+    def last_query_stats(self) -> dict:
+        import struct
+        v = (C.c_uint64 * 8)()
+        LIB.hdg_last_query_stats(self._h, v, 8)
+        return {"queries": v[0], "n_cand_ref": v[1], "n_cand_used": v[2], "coarse_total": v[3], "exact_total": v[4],
+                "max_row": v[5], "beta": struct.unpack("f", struct.pack("I", v[6] & 0xFFFFFFFF))[0],
+                "schedule": ["pre-filter", "post-filter", "single-dim"][v[7]]}
 
     def stage_times(self) -> dict:
         ms = (C.c_float * 16)()

@@ -1,7 +1,7 @@
 """Build recipe for libhdgrid.so (sm_100a) and the search-engine binary.
 
 Compiles every source under hdgrid_b200/csrc with nvcc into an in-tree shared library,
-so the built artefact travels with the source tree.  Usage: python -m hdgrid_b200.build_native
+so the built artefact travels with the source tree.  Usage: python hdgrid_b200/build_native.py
 """
 from __future__ import annotations
 

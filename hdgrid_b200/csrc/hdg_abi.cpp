@@ -148,6 +148,26 @@ hdg_status hdg_get_params(const hdg_index* index, hdg_params* out) {
     });
 }
 
+hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value) {
+    return guarded([&] {
+        HDG_REQUIRE(index && key, HDG_ERR_INVALID_ARG, "null argument");
+        const std::string k = upper(key);
+        hdg_params& p = index->params;
+        uint64_t* f = nullptr;
+        if (k == "N_LIST") f = &p.n_list;
+        else if (k == "SUB_LISTS") f = &p.sub_lists;
+        else if (k == "EXPS0") f = &p.exps0;
+        else if (k == "TOPK") f = &p.topk;
+        else if (k == "BREAK_DOWN") f = &p.break_down;
+        else if (k == "IS_SPLIT") f = &p.is_split;
+        else if (k == "N_SPLIT") f = &p.n_split;
+        else if (k == "LUT_FP16") f = &p.lut_fp16;
+        else if (k == "COARSE_BF16") f = &p.coarse_bf16;
+        HDG_REQUIRE(f, HDG_ERR_INVALID_ARG, "not a search-time key: " + k);
+        *f = value;
+    });
+}
+
 hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t d, const float* d_labels,
                      uint32_t l, void* stream) {
     return guarded([&] {
@@ -159,7 +179,7 @@ hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t
 hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries) {
     return guarded([&] {
         HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
-        reserve_workspace(index, max_queries, index->params.exps0 <= 1 ? 1 : 8192 - 256);
+        reserve_workspace(index, max_queries, 0);
     });
 }
 
@@ -171,6 +191,13 @@ hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q, const
         run_query(index, d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids,
                   static_cast<cudaStream_t>(stream));
     });
+}
+
+int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap) {
+    if (!index || !out) return 0;
+    const int n = std::min(cap, 8);
+    for (int i = 0; i < n; i++) out[i] = index->last_stats[i];
+    return n;
 }
 
 int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, int cap) {

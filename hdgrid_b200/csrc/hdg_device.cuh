@@ -134,6 +134,10 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
     }
 }
 
+__device__ __forceinline__ uint32_t next_pow2_dev(uint32_t x) {
+    return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -103,6 +103,7 @@ struct hdg_index {
     hdg::DeviceBuffer arena;       // all index arrays
     hdg::DeviceBuffer map_buf;     // filter interval map
     hdg::DeviceBuffer work;        // per-query workspace
+    hdg::DeviceBuffer dist_buf;    // one f32 ADC distance per scanned candidate
     uint64_t work_queries = 0;
     std::map<std::string, std::pair<size_t, size_t>> work_layout;  // name -> (offset, bytes)
     int device = 0;
@@ -111,5 +112,6 @@ struct hdg_index {
     std::vector<float> stage_ms;
     // last-query scalars (host copy)
     uint64_t last_q = 0, last_ncand = 0;
+    uint64_t last_stats[8] = {0};
     float last_beta = 0.f;
 };

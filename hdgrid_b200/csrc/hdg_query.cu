@@ -1,5 +1,5 @@
 // The filtered query path: super_grid::index::query
-// (src/index/2-level_index/Super-Grid-IVF_PQ.cu:985-1249) as five B200 kernels.
+// (src/index/2-level_index/Super-Grid-IVF_PQ.cu:985-1249) as B200 kernels.
 //
 //   k_prologue   per query: filter recovery (preprocessing.cu:3-32) -> f32 box, cell box
 //                (:930-961), Morton corners (:903-928, zorder.cu:3-15), per-list filtered
@@ -9,18 +9,23 @@
 //                (::refine, :1034-1042); their non-empty lists, exact L2 to the list
 //                centroids, top sub_lists (select_sub_clusters, :849-901); Morton interval
 //                [lower_bound(zlo), lower_bound(zhi+1)) inside every probed list (zorder.cu:656-685).
-//   k_batch      batch sums for the post-filter candidate budget beta (:1198-1222).
-//   k_scan       per query: LUT in shared memory (product-quantization.cu:4-35), ADC over the
-//                contiguous Z-ordered candidate ranges (:37-77), optional fused label predicate
-//                (filter.cu:30-64), block top-K (RAFT select_k in the reference).
+//   k_batch      candidate offsets, work items and the batch sums of the post-filter budget
+//                beta (:1198-1222).
+//   k_lut        per query PQ lookup table (build_pq_lut_kernel, product-quantization.cu:4-35).
+//   k_scan       persistent streaming ADC over the contiguous Z-ordered candidate ranges
+//                (compute_batched_L2_distance_kernel, :37-77) with the LUT in shared memory,
+//                optional fused label predicate (filter.cu:30-64); one f32 per candidate.
+//   k_select     per query: the K smallest (distance, position) pairs (RAFT select_k in the
+//                reference) by a two-pass histogram select.
 //   k_refine     per query: label predicate on the ADC top-n_cand (post-filter, :1227-1236),
 //                exact f32 re-rank and top-k (refine.cu:36-120).
-// There is no dense [q x max_row_len] candidate table and no host round trip except the
-// one scalar read for the batch-wide candidate budget.
+// There is no dense [q x max_row_len] candidate table and one host round trip per batch
+// (the candidate total and the batch-wide budget).
 #include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "hdg_device.cuh"
 #include "hdg_internal.h"
@@ -29,7 +34,10 @@ namespace hdg {
 
 constexpr int kThreads = 256;
 constexpr uint32_t kInvalid = 0xffffffffu;
-constexpr int kMaxCand = 8192 - kThreads;  // largest ADC top-K kept in shared memory
+constexpr int kMaxCand = 16384;     // largest candidate budget n_cand
+constexpr uint32_t kChunk = 32768;  // candidates per scan work item
+constexpr int kBins = 4096;         // select histogram
+constexpr int kBCap = 4096;         // boundary-bin buffer of the select
 
 struct Workspace {
     float* box;              // [q x 2l]
@@ -42,11 +50,52 @@ struct Workspace {
     uint32_t* range_start;   // [q x Ps]
     uint32_t* range_len;     // [q x Ps]
     uint32_t* qstat;         // [q x 4]: cand_total, exact_total, n_lists, n_clusters
-    uint64_t* scal;          // [8]
+    uint64_t* scal;          // [8]: cand sum, exact sum, max cand, items
+    uint64_t* qoff;          // [q + 1] candidate offsets into dist
+    uint32_t* item_off;      // [q + 1] work-item offsets
+    uint32_t* mm;            // [q x 2] min / max finite distance key
+    uint32_t* nfin;          // [q] finite distances (predicate passed)
+    uint32_t* counter;       // [4] work counter
+    float* lut;              // [q x G x 256 x 32]
     uint32_t* cand_pool;     // [q x kcand]
     uint32_t* cand_count;    // [q]
     uint64_t kcand;
+    float* dist;             // [sum of candidates]
 };
+
+// Exclusive block-wide scan of n u32 values in shared memory (in place).  All threads.
+__device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_t* s_warp) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b = t * per, e = min(n, b + per);
+    uint32_t local = 0;
+    for (int i = b; i < e; i++) local += v[i];
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t y = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        if (lane < nw) s_warp[lane] = y;
+    }
+    __syncthreads();
+    uint32_t run = x - local + (warp ? s_warp[warp - 1] : 0);
+    for (int i = b; i < e; i++) {
+        const uint32_t vi = v[i];
+        v[i] = run;
+        run += vi;
+    }
+    __syncthreads();
+}
 
 // ------------------------------------------------------------------------------------
 // k_prologue
@@ -227,6 +276,11 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     __syncthreads();
     block_bitonic_sort(s_keys, sort_n2);
     const int nps = min(Ps, s_nvalid);
+    // the probed lists in list-id (= pool) order, so candidate positions follow pool order
+    const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
+    for (int i = t; i < sort_n3; i += blockDim.x) s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
+    __syncthreads();
+    block_bitonic_sort(s_keys, sort_n3);
     const uint64_t zlo = w.zrange[qi * 2], zhi = w.zrange[qi * 2 + 1];
     uint32_t my_cand = 0, my_exact = 0;
     for (int i = t; i < Ps; i += blockDim.x) {
@@ -256,209 +310,604 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     }
 }
 
-// Batch sums: scal[0] = sum of candidate-range sizes, scal[1] = sum of exact filtered
-// counts of the probed lists, scal[2] = max candidates of one query.
-__global__ void k_batch(const uint32_t* __restrict__ qstat, uint64_t q, uint64_t* __restrict__ scal) {
-    __shared__ unsigned long long s[3];
-    if (threadIdx.x == 0) s[0] = s[1] = s[2] = 0;
+
+// ------------------------------------------------------------------------------------
+// k_batch: per-query candidate offsets and work items, batch sums (one block)
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
+    __shared__ unsigned long long s_tot[32], s_items[32];
+    __shared__ unsigned long long s_red[3];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) s_red[0] = s_red[1] = s_red[2] = 0;
     __syncthreads();
-    unsigned long long a = 0, b = 0, m = 0;
-    for (uint64_t i = threadIdx.x; i < q; i += blockDim.x) {
-        a += qstat[i * 4];
-        b += qstat[i * 4 + 1];
-        m = max(m, (unsigned long long)qstat[i * 4]);
+    const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = t * per, e = min(q, b + per);
+    unsigned long long cand = 0, items = 0, exact = 0, mx = 0;
+    for (uint64_t i = b; i < e; i++) {
+        const uint32_t c = w.qstat[i * 4];
+        cand += c;
+        items += (c + kChunk - 1) / kChunk;
+        exact += w.qstat[i * 4 + 1];
+        mx = max(mx, (unsigned long long)c);
     }
-    atomicAdd(&s[0], a);
-    atomicAdd(&s[1], b);
-    atomicMax(&s[2], m);
+    // inclusive scans of (cand, items) across the block
+    unsigned long long xc = cand, xi = items;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long yc = __shfl_up_sync(0xffffffffu, xc, o);
+        const unsigned long long yi = __shfl_up_sync(0xffffffffu, xi, o);
+        if (lane >= o) {
+            xc += yc;
+            xi += yi;
+        }
+    }
+    if (lane == 31) {
+        s_tot[warp] = xc;
+        s_items[warp] = xi;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        scal[0] = s[0];
-        scal[1] = s[1];
-        scal[2] = s[2];
+    if (warp == 0) {
+        unsigned long long yc = lane < (int)(blockDim.x >> 5) ? s_tot[lane] : 0;
+        unsigned long long yi = lane < (int)(blockDim.x >> 5) ? s_items[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long zc = __shfl_up_sync(0xffffffffu, yc, o);
+            const unsigned long long zi = __shfl_up_sync(0xffffffffu, yi, o);
+            if (lane >= o) {
+                yc += zc;
+                yi += zi;
+            }
+        }
+        s_tot[lane] = yc;
+        s_items[lane] = yi;
+    }
+    __syncthreads();
+    unsigned long long rc = xc - cand + (warp ? s_tot[warp - 1] : 0);
+    unsigned long long ri = xi - items + (warp ? s_items[warp - 1] : 0);
+    for (uint64_t i = b; i < e; i++) {
+        const uint32_t c = w.qstat[i * 4];
+        w.qoff[i] = rc;
+        w.item_off[i] = (uint32_t)ri;
+        rc += c;
+        ri += (c + kChunk - 1) / kChunk;
+        w.mm[2 * i] = 0xffffffffu;
+        w.mm[2 * i + 1] = 0u;
+        w.nfin[i] = 0;
+        w.cand_count[i] = 0;
+    }
+    if (e == q && b < e) {
+        w.qoff[q] = rc;
+        w.item_off[q] = (uint32_t)ri;
+    }
+    atomicAdd(&s_red[0], cand);
+    atomicAdd(&s_red[1], exact);
+    atomicMax(&s_red[2], mx);
+    __syncthreads();
+    if (t == 0) {
+        w.scal[0] = s_red[0];
+        w.scal[1] = s_red[1];
+        w.scal[2] = s_red[2];
+        w.scal[3] = s_items[(blockDim.x >> 5) - 1];
+        w.counter[0] = 0;
     }
 }
 
 // ------------------------------------------------------------------------------------
-// block top-K over u64 keys (distance key << 32 | payload) in shared memory
+// k_lut: LUT[q][g][c][j] = sum_t (C[m][c][t] - x[q][m*pq_len + t])^2, m = 32g + j
+// (build_pq_lut_kernel, product-quantization.cu:4-35; the reference's `ans += (c-q)*(c-q)`
+// is an FMA under nvcc's default contraction), zero for m >= M.
 // ------------------------------------------------------------------------------------
-struct TopK {
-    uint64_t* buf;
-    int cap;   // power of two, >= K + blockDim
-    int K;
-    int* cnt;
-    uint64_t* thresh;
+__global__ void __launch_bounds__(256) k_lut(IndexDev D, const float* __restrict__ queries, int G,
+                                             float* __restrict__ lut) {
+    extern __shared__ float s_q[];
+    const uint64_t qi = blockIdx.x;
+    const int g = blockIdx.y;
+    const int d = D.d, pq_len = D.pq_len;
+    for (int i = threadIdx.x; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
+    __syncthreads();
+    float* out = lut + ((uint64_t)qi * G + g) * (kCodes * 32);
+    for (int e = threadIdx.x; e < kCodes * 32; e += blockDim.x) {
+        const int c = e >> 5, j = e & 31, m = g * 32 + j;
+        float s = 0.f;
+        if (m < (int)D.M) {
+            const float* cw = D.pq_centers + ((uint64_t)m * kCodes + c) * pq_len;
+            for (int tt = 0; tt < pq_len; tt++) {
+                const float df = __fsub_rn(cw[tt], s_q[m * pq_len + tt]);
+                s = fmaf(df, df, s);
+            }
+        }
+        out[e] = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_scan: persistent ADC stream
+// ------------------------------------------------------------------------------------
+// Shared-memory LUT layout (fast path): for each group g of 32 subspaces a [256][64] f32
+// table whose columns 32..63 repeat 0..31.  Lane r rotates its candidate's 32 code bytes of
+// the group left by r, so at step s it looks up subspace (r + s) mod 32 at column r + s:
+// the 32 lanes of a warp read 32 different banks, the column offset 4*s is an immediate,
+// and no wrap-around arithmetic is needed.
+
+// rotate 8 words left by R words (out[i] = in[(i + R) & 7]) with selects only
+__device__ __forceinline__ void rotate_words(uint32_t (&w)[8], uint32_t R) {
+    uint32_t t[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = (R & 1) ? w[(i + 1) & 7] : w[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = (R & 2) ? t[(i + 2) & 7] : t[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = (R & 4) ? w[(i + 4) & 7] : w[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = t[i];
+}
+
+struct ScanShared {
+    int item, query;
 };
 
-// Called by all threads after a chunk has been appended and the block synchronised.
-__device__ __forceinline__ void topk_maybe_compact(TopK& tk, bool force) {
-    const int c = *tk.cnt;
-    __syncthreads();  // every thread has read the count before anyone appends again
-    if (!force && c <= tk.cap - (int)blockDim.x) return;  // uniform decision
-    for (int i = c + threadIdx.x; i < tk.cap; i += blockDim.x) tk.buf[i] = ~0ull;
-    __syncthreads();
-    block_bitonic_sort(tk.buf, tk.cap);
-    if (threadIdx.x == 0) {
-        const int nc = min(c, tk.K);
-        *tk.cnt = nc;
-        if (nc == tk.K) *tk.thresh = tk.buf[tk.K - 1];
+__device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int qq, uint32_t* s_pre,
+                                                uint32_t* s_start, uint32_t* s_warp) {
+    for (int i = threadIdx.x; i < Ps; i += blockDim.x) {
+        s_pre[i] = w.range_len[(uint64_t)qq * Ps + i];
+        s_start[i] = w.range_start[(uint64_t)qq * Ps + i];
     }
+    if (threadIdx.x == 0) s_pre[Ps] = 0;
     __syncthreads();
+    block_exclusive_scan(s_pre, Ps + 1, s_warp);
 }
 
-__device__ __forceinline__ void topk_push(TopK& tk, uint64_t key) {
-    if (key < *tk.thresh) {
-        const int pos = atomicAdd(tk.cnt, 1);
-        tk.buf[pos] = key;
-    }
-}
-
-// ------------------------------------------------------------------------------------
-// k_scan: LUT + ADC (+ predicate) + top-K over the Morton candidate ranges
-// ------------------------------------------------------------------------------------
-enum ScanMode { kPre = 0, kPost = 1, kL1 = 2 };
-
-template <bool kFp16>
-__global__ void __launch_bounds__(kThreads) k_scan(IndexDev D, const float* __restrict__ queries,
-                                                   int Ps, int mode, int K, int cap, int lbl,
-                                                   Workspace w, float* __restrict__ out_dist,
-                                                   uint64_t* __restrict__ out_ids, int k_out) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int M = D.M, pq_len = D.pq_len, d = D.d;
-    uint64_t* s_buf = reinterpret_cast<uint64_t*>(smem);                  // [cap]
-    float* s_q = reinterpret_cast<float*>(s_buf + cap);                   // [d]
-    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_q + d);               // [Ps + 1]
-    uint32_t* s_start = s_pre + (Ps + 1);                                 // [Ps]
-    float* s_lut = reinterpret_cast<float*>(s_start + Ps + ((Ps + 1) & 1) + 2);  // [M x 256]
-    __half* s_lut16 = reinterpret_cast<__half*>(s_lut);
-    __shared__ int s_cnt;
-    __shared__ uint64_t s_thresh;
+template <int G, int NT>
+__global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre, int lbl, uint64_t q,
+                                                     Workspace w) {
+    extern __shared__ __align__(16) float s_lut[];  // [G][256][64]
+    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 64);  // [Ps + 1]
+    uint32_t* s_start = s_pre + Ps + 1;                                       // [Ps]
+    __shared__ ScanShared s;
+    __shared__ uint32_t s_warp[32];
     __shared__ float s_box[2 * kMaxDims];
-    const uint64_t qi = blockIdx.x;
-    const int t = threadIdx.x;
-    for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
-    if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
-    if (t == 0) {
-        s_cnt = 0;
-        s_thresh = ~0ull;
-        uint32_t acc = 0;
-        for (int i = 0; i < Ps; i++) {
-            s_pre[i] = acc;
-            acc += w.range_len[qi * Ps + i];
-            s_start[i] = w.range_start[qi * Ps + i];
-        }
-        s_pre[Ps] = acc;
-    }
-    __syncthreads();
-    // LUT[m][c] = sum_t (C[m][c][t] - q[m*pq_len+t])^2, sequential FMA accumulation
-    for (int e = t; e < M * kCodes; e += blockDim.x) {
-        const int m = e / kCodes;
-        const float* cw = D.pq_centers + (uint64_t)e * pq_len;
-        float s = 0.f;
-        for (int tt = 0; tt < pq_len; tt++) {
-            const float df = __fsub_rn(cw[tt], s_q[m * pq_len + tt]);
-            s = fmaf(df, df, s);
-        }
-        if (kFp16)
-            s_lut16[e] = __float2half_rn(s);
-        else
-            s_lut[e] = s;
-    }
-    __syncthreads();
-    TopK tk{s_buf, cap, K, &s_cnt, &s_thresh};
-    const uint32_t total = s_pre[Ps];
-    const int Mv = D.M_pad / 16;
-    for (uint32_t base = 0; base < total; base += blockDim.x) {
-        const uint32_t e = base + t;
-        if (e < total) {
-            // range r with s_pre[r] <= e < s_pre[r+1]
-            int lo = 0, hi = Ps - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_pre[mid] <= e)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            const uint32_t pool = s_start[lo] + (e - s_pre[lo]);
-            bool pass = true;
-            if (mode == kPre) {
-                const float* lab = D.labels + (uint64_t)pool * lbl;
-                for (int i = 0; i < lbl; i++) {
-                    const float v = lab[i];
-                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) {
-                        pass = false;
-                        break;
-                    }
+    const int t = threadIdx.x, lane = t & 31;
+    const uint32_t R = lane >> 2, sh = 8u * (lane & 3);
+    const uint32_t n_items = w.item_off[q];
+    int cur = -1;
+    for (;;) {
+        if (t == 0) {
+            const int item = (int)atomicAdd(w.counter, 1u);
+            s.item = item;
+            if (item < (int)n_items) {  // largest query with item_off <= item
+                int lo = 0, hi = (int)q - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (w.item_off[mid] <= (uint32_t)item) lo = mid;
+                    else hi = mid - 1;
                 }
-            }
-            if (pass) {
-                const uint4* cp = reinterpret_cast<const uint4*>(D.codes + (uint64_t)pool * D.M_pad);
-                float sum = 0.f;
-                for (int v = 0; v < Mv; v++) {
-                    const uint4 cv = __ldg(cp + v);
-                    const uint32_t wv[4] = {cv.x, cv.y, cv.z, cv.w};
-#pragma unroll
-                    for (int b = 0; b < 16; b++) {
-                        const int m = v * 16 + b;
-                        if (m < M) {
-                            const uint32_t code = (wv[b >> 2] >> (8 * (b & 3))) & 0xffu;
-                            sum += kFp16 ? __half2float(s_lut16[m * kCodes + code]) : s_lut[m * kCodes + code];
-                        }
-                    }
-                }
-                topk_push(tk, ((uint64_t)float_key(sum) << 32) | pool);
+                s.query = lo;
             }
         }
         __syncthreads();
-        topk_maybe_compact(tk, false);
+        const int item = s.item;
+        if (item >= (int)n_items) break;
+        const int qq = s.query;
+        if (qq != cur) {
+            const float4* src = reinterpret_cast<const float4*>(w.lut + (uint64_t)qq * G * kCodes * 32);
+            for (int e = t; e < G * kCodes * 8; e += NT) {
+                const float4 v = src[e];
+                const int row = e >> 3, col = (e & 7) * 4;  // row = g*256 + c
+                float4* dst = reinterpret_cast<float4*>(s_lut + row * 64 + col);
+                dst[0] = v;
+                dst[8] = v;  // columns 32..63 repeat 0..31
+            }
+            if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
+            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
+            cur = qq;
+        }
+        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
+        const uint32_t e1 = min(total, e0 + kChunk);
+        float* dst = w.dist + w.qoff[qq];
+        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
+        int r = 0;
+        {
+            const uint32_t e = e0 + t;
+            int lo = 0, hi = Ps - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_pre[mid] <= e) lo = mid;
+                else hi = mid - 1;
+            }
+            r = lo;
+        }
+        for (uint32_t e = e0 + t; e < e1; e += NT) {
+            while (s_pre[r + 1] <= e) r++;
+            const uint32_t pool = s_start[r] + (e - s_pre[r]);
+            bool pass = true;
+            if (pre) {
+                const float* lab = D.labels + (uint64_t)pool * lbl;
+                for (int i = 0; i < lbl; i++) {
+                    const float v = lab[i];
+                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
+                }
+            }
+            float sum = INFINITY;
+            if (pass) {
+                sum = 0.f;
+                const uint4* cp = reinterpret_cast<const uint4*>(D.codes + (uint64_t)pool * D.M_pad);
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const uint4 a = __ldg(cp + 2 * g), b = __ldg(cp + 2 * g + 1);
+                    uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+                    rotate_words(wv, R);
+                    uint32_t x[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) x[i] = __funnelshift_r(wv[i], wv[(i + 1) & 7], sh);
+                    const float* L = s_lut + g * (kCodes * 64) + lane;
+#pragma unroll
+                    for (int st = 0; st < 32; st++) {
+                        const uint32_t c = __byte_perm(x[st >> 2], 0u, 0x4440u | (st & 3));
+                        sum += L[c * 64 + st];
+                    }
+                }
+                const uint32_t key = float_key(sum);
+                kmin = min(kmin, key);
+                kmax = max(kmax, key);
+                nf++;
+            }
+            dst[e] = sum;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            nf += __shfl_xor_sync(0xffffffffu, nf, o);
+        }
+        if (lane == 0 && nf) {
+            atomicMin(&w.mm[2 * qq], kmin);
+            atomicMax(&w.mm[2 * qq + 1], kmax);
+            atomicAdd(&w.nfin[qq], nf);
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    topk_maybe_compact(tk, true);
-    const int nres = s_cnt;
-    if (mode == kPre) {
-        for (int i = t; i < k_out; i += blockDim.x) {
-            if (i < nres) {
-                const uint64_t key = s_buf[i];
-                out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
-                out_ids[qi * k_out + i] = D.ids[(uint32_t)key];
-            } else {
-                out_dist[qi * k_out + i] = INFINITY;
-                out_ids[qi * k_out + i] = ~0ull;
+}
+
+// Generic ADC (any M): natural subspace order, LUT [G][256][32] in shared memory.
+__global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps, int pre, int lbl, uint64_t q,
+                                                      Workspace w) {
+    extern __shared__ __align__(16) float s_lut[];  // [G][256][32]
+    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 32);
+    uint32_t* s_start = s_pre + Ps + 1;
+    __shared__ ScanShared s;
+    __shared__ uint32_t s_warp[32];
+    __shared__ float s_box[2 * kMaxDims];
+    const int t = threadIdx.x, lane = t & 31;
+    const uint32_t n_items = w.item_off[q];
+    const int M = D.M;
+    int cur = -1;
+    for (;;) {
+        if (t == 0) {
+            const int item = (int)atomicAdd(w.counter, 1u);
+            s.item = item;
+            if (item < (int)n_items) {
+                int lo = 0, hi = (int)q - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (w.item_off[mid] <= (uint32_t)item) lo = mid;
+                    else hi = mid - 1;
+                }
+                s.query = lo;
             }
         }
-    } else {
-        for (int i = t; i < K; i += blockDim.x)
-            w.cand_pool[qi * w.kcand + i] = i < nres ? (uint32_t)s_buf[i] : kInvalid;
-        if (t == 0) w.cand_count[qi] = nres;
+        __syncthreads();
+        const int item = s.item;
+        if (item >= (int)n_items) break;
+        const int qq = s.query;
+        if (qq != cur) {
+            const float* src = w.lut + (uint64_t)qq * G * kCodes * 32;
+            for (int e = t; e < G * kCodes * 32; e += blockDim.x) s_lut[e] = src[e];
+            if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
+            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
+            cur = qq;
+        }
+        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
+        const uint32_t e1 = min(total, e0 + kChunk);
+        float* dst = w.dist + w.qoff[qq];
+        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
+        for (uint32_t e = e0 + t; e < e1; e += blockDim.x) {
+            int lo = 0, hi = Ps - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_pre[mid] <= e) lo = mid;
+                else hi = mid - 1;
+            }
+            const uint32_t pool = s_start[lo] + (e - s_pre[lo]);
+            bool pass = true;
+            if (pre) {
+                const float* lab = D.labels + (uint64_t)pool * lbl;
+                for (int i = 0; i < lbl; i++) {
+                    const float v = lab[i];
+                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
+                }
+            }
+            float sum = INFINITY;
+            if (pass) {
+                sum = 0.f;
+                const uint8_t* cp = D.codes + (uint64_t)pool * D.M_pad;
+                for (int m = 0; m < M; m++) sum += s_lut[(m >> 5) * (kCodes * 32) + cp[m] * 32 + (m & 31)];
+                const uint32_t key = float_key(sum);
+                kmin = min(kmin, key);
+                kmax = max(kmax, key);
+                nf++;
+            }
+            dst[e] = sum;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            nf += __shfl_xor_sync(0xffffffffu, nf, o);
+        }
+        if (lane == 0 && nf) {
+            atomicMin(&w.mm[2 * qq], kmin);
+            atomicMax(&w.mm[2 * qq + 1], kmax);
+            atomicAdd(&w.nfin[qq], nf);
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// k_select: the K smallest (distance, position) pairs of one query
+// ------------------------------------------------------------------------------------
+// Pass 1 histograms the finite distances over kBins linear bins between the query's
+// min and max; pass 2 emits every candidate below the bin that holds the K-th and gathers
+// that boundary bin, which is sorted by (distance key, position).  A boundary bin larger
+// than kBCap is split again over its own min/max (at most kMaxLevels levels); a bin whose
+// entries all share one distance is resolved by position order.
+constexpr int kMaxLevels = 4;
+constexpr int kSelThreads = 512;
+
+struct SelLevel {
+    float lo, inv;
+    int bin;
+};
+
+__device__ __forceinline__ int sel_bin(float d, float lo, float inv) {
+    const int b = (int)__fmul_rn(__fsub_rn(d, lo), inv);
+    return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+}
+
+__device__ __forceinline__ uint32_t pos_to_pool(const uint32_t* s_pre, const uint32_t* s_start, int Ps,
+                                                uint32_t e) {
+    int lo = 0, hi = Ps - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pre[mid] <= e) lo = mid;
+        else hi = mid - 1;
+    }
+    return s_start[lo] + (e - s_pre[lo]);
+}
+
+__global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int K, int sorted_out, Workspace w,
+                                                        float* __restrict__ out_dist,
+                                                        uint64_t* __restrict__ out_ids, int k_out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem);                   // [kBins]
+    uint64_t* s_bbuf = reinterpret_cast<uint64_t*>(s_hist + kBins);         // [kBCap]
+    uint64_t* s_sel = s_bbuf + kBCap;                                        // [sel_cap] (sorted mode)
+    const int sel_cap = sorted_out ? (int)next_pow2_dev((uint32_t)max(K, 2)) : 0;
+    uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_sel + sel_cap);        // [Ps + 1]
+    uint32_t* s_start = s_pre + Ps + 1;                                      // [Ps]
+    __shared__ uint32_t s_warp[32];
+    __shared__ SelLevel s_lv[kMaxLevels];
+    __shared__ int s_bin;
+    __shared__ uint32_t s_below, s_cntb, s_out, s_nb, s_bmin, s_bmax, s_need;
+    const uint64_t qi = blockIdx.x;
+    const int t = threadIdx.x;
+    const uint32_t total = w.qstat[qi * 4];
+    const float* dist = w.dist + w.qoff[qi];
+    for (int i = t; i < Ps; i += blockDim.x) {
+        s_pre[i] = w.range_len[qi * Ps + i];
+        s_start[i] = w.range_start[qi * Ps + i];
+    }
+    if (t == 0) {
+        s_pre[Ps] = 0;
+        s_out = 0;
+    }
+    __syncthreads();
+    block_exclusive_scan(s_pre, Ps + 1, s_warp);
+    const uint32_t nfin = w.nfin[qi];
+    const uint32_t need0 = min((uint32_t)K, nfin);
+    auto emit = [&](uint32_t e, float d) {
+        const uint32_t pos = atomicAdd(&s_out, 1u);
+        if (sorted_out)
+            s_sel[pos] = ((uint64_t)float_key(d) << 32) | e;
+        else
+            w.cand_pool[qi * w.kcand + pos] = pos_to_pool(s_pre, s_start, Ps, e);
+    };
+    auto inside = [&](float d, int nlv) {
+        for (int l = 0; l < nlv; l++)
+            if (sel_bin(d, s_lv[l].lo, s_lv[l].inv) != s_lv[l].bin) return false;
+        return true;
+    };
+    if (need0 > 0 && nfin <= (uint32_t)K) {
+        // every finite candidate is selected
+        for (uint32_t e = t; e < total; e += blockDim.x) {
+            const float d = dist[e];
+            if (d < INFINITY) emit(e, d);
+        }
+        __syncthreads();
+    } else if (need0 > 0) {
+        float lo = key_float(w.mm[2 * qi]), hi = key_float(w.mm[2 * qi + 1]);
+        uint32_t need = need0;
+        for (int level = 0; level < kMaxLevels; level++) {
+            const float inv = hi > lo ? (float)kBins / (hi - lo) : 0.f;
+            for (int i = t; i < kBins; i += blockDim.x) s_hist[i] = 0;
+            if (t == 0) {
+                s_bmin = 0xffffffffu;
+                s_bmax = 0u;
+                s_nb = 0;
+            }
+            __syncthreads();
+            for (uint32_t e = t; e < total; e += blockDim.x) {
+                const float d = dist[e];
+                if (d < INFINITY && inside(d, level)) atomicAdd(&s_hist[sel_bin(d, lo, inv)], 1u);
+            }
+            __syncthreads();
+            if (t < 32) {  // first bin whose cumulative count reaches need
+                uint32_t run = 0;
+                int found = -1;
+                uint32_t below = 0;
+                for (int base = 0; base < kBins && found < 0; base += 32) {
+                    const uint32_t v = s_hist[base + t];
+                    uint32_t x = v;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (t >= o) x += y;
+                    }
+                    const unsigned hit = __ballot_sync(0xffffffffu, run + x >= need);
+                    if (hit) {
+                        const int l0 = __ffs(hit) - 1;
+                        found = base + l0;
+                        below = run + __shfl_sync(0xffffffffu, x - v, l0);
+                    }
+                    run += __shfl_sync(0xffffffffu, x, 31);
+                }
+                if (t == 0) {
+                    s_bin = found;
+                    s_below = below;
+                    s_cntb = s_hist[found];
+                }
+            }
+            __syncthreads();
+            const int b = s_bin;
+            const bool fits = s_cntb <= (uint32_t)kBCap;
+            for (uint32_t e = t; e < total; e += blockDim.x) {
+                const float d = dist[e];
+                if (!(d < INFINITY) || !inside(d, level)) continue;
+                const int bb = sel_bin(d, lo, inv);
+                if (bb < b) {
+                    emit(e, d);
+                } else if (bb == b) {
+                    if (fits) {
+                        const uint32_t p = atomicAdd(&s_nb, 1u);
+                        s_bbuf[p] = ((uint64_t)float_key(d) << 32) | e;
+                    } else {
+                        atomicMin(&s_bmin, float_key(d));
+                        atomicMax(&s_bmax, float_key(d));
+                    }
+                }
+            }
+            __syncthreads();
+            need -= s_below;
+            if (fits) {
+                const int nb = (int)s_nb;
+                const int n2 = (int)next_pow2_dev((uint32_t)max(nb, 2));
+                for (int i = nb + t; i < n2; i += blockDim.x) s_bbuf[i] = ~0ull;
+                __syncthreads();
+                block_bitonic_sort(s_bbuf, n2);
+                for (uint32_t i = t; i < need; i += blockDim.x) {
+                    const uint64_t key = s_bbuf[i];
+                    emit((uint32_t)key, key_float((uint32_t)(key >> 32)));
+                }
+                __syncthreads();
+                break;
+            }
+            if (s_bmin == s_bmax || level == kMaxLevels - 1) {
+                // one distance value (or no levels left): take the boundary bin in position order
+                const uint32_t tie_key = s_bmin;
+                const int nlv = level;
+                if (t == 0) s_need = need;
+                __syncthreads();
+                for (uint32_t base = 0; base < total && s_need > 0; base += blockDim.x) {
+                    const uint32_t e = base + t;
+                    bool f = false;
+                    float d = 0.f;
+                    if (e < total) {
+                        d = dist[e];
+                        f = d < INFINITY && inside(d, nlv) && sel_bin(d, lo, inv) == b &&
+                            (s_bmin == s_bmax ? float_key(d) == tie_key : true);
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, f);
+                    if ((t & 31) == 0) s_warp[t >> 5] = __popc(bal);
+                    __syncthreads();
+                    uint32_t before = 0;
+                    for (int i = 0; i < (t >> 5); i++) before += s_warp[i];
+                    const uint32_t rank = before + __popc(bal & ((1u << (t & 31)) - 1));
+                    if (f && rank < s_need) emit(e, d);
+                    __syncthreads();
+                    if (t == 0) {
+                        uint32_t tot = 0;
+                        for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += s_warp[i];
+                        s_need = s_need > tot ? s_need - tot : 0;
+                    }
+                    __syncthreads();
+                }
+                break;
+            }
+            if (t == 0) {
+                s_lv[level].lo = lo;
+                s_lv[level].inv = inv;
+                s_lv[level].bin = b;
+            }
+            lo = key_float(s_bmin);
+            hi = key_float(s_bmax);
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    const uint32_t nsel = s_out;
+    if (!sorted_out) {
+        if (t == 0) w.cand_count[qi] = nsel;
+        return;
+    }
+    const int n2 = (int)next_pow2_dev((uint32_t)max((int)nsel, 2));
+    for (int i = nsel + t; i < n2; i += blockDim.x) s_sel[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(s_sel, n2);
+    for (int i = t; i < k_out; i += blockDim.x) {
+        if (i < (int)nsel) {
+            const uint64_t key = s_sel[i];
+            out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
+            out_ids[qi * k_out + i] = D.ids[pos_to_pool(s_pre, s_start, Ps, (uint32_t)key)];
+        } else {
+            out_dist[qi * k_out + i] = INFINITY;
+            out_ids[qi * k_out + i] = ~0ull;
+        }
     }
 }
 
 // ------------------------------------------------------------------------------------
 // k_refine: post-filter predicate, exact f32 L2, top-k
 // ------------------------------------------------------------------------------------
+// Candidates are taken in chunks of blockDim: the predicate survivors of a chunk are
+// compacted, each gets its exact distance from one warp, and the keys (distance, id) go
+// through a threshold buffer of pow2(k + blockDim) entries that is sorted and truncated
+// to k when it fills.
 __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __restrict__ queries,
-                                                     const float* __restrict__ data, int K, int cap,
-                                                     int apply_pred, int lbl, Workspace w,
-                                                     float* __restrict__ out_dist,
+                                                     const float* __restrict__ data, int cap, int apply_pred,
+                                                     int lbl, Workspace w, float* __restrict__ out_dist,
                                                      uint64_t* __restrict__ out_ids, int k_out) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);      // [cap]
-    uint32_t* s_surv = reinterpret_cast<uint32_t*>(s_keys + cap); // [K]
-    float* s_q = reinterpret_cast<float*>(s_surv + K + (K & 1)); // [d]
+    uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);           // [cap]
+    float* s_q = reinterpret_cast<float*>(s_keys + cap);             // [d]
+    __shared__ uint32_t s_chunk[kThreads];
     __shared__ float s_box[2 * kMaxDims];
-    __shared__ int s_ns;
     __shared__ int s_wsum[kThreads / 32];
+    __shared__ int s_cnt;
+    __shared__ uint64_t s_th;
     const uint64_t qi = blockIdx.x;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = kThreads / 32;
     const int d = D.d;
     for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
     if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
-    if (t == 0) s_ns = 0;
+    if (t == 0) {
+        s_cnt = 0;
+        s_th = ~0ull;
+    }
     __syncthreads();
-    const int nc = min((int)w.cand_count[qi], K);
-    // order-preserving compaction of the candidates that pass the predicate
-    for (int base = 0; base < nc; base += blockDim.x) {
+    const int nc = (int)w.cand_count[qi];
+    for (int base = 0; base < nc; base += kThreads) {
         const int e = base + t;
         bool keep = false;
         uint32_t pool = kInvalid;
@@ -469,33 +918,22 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
                 const float* lab = D.labels + (uint64_t)pool * lbl;
                 for (int i = 0; i < lbl; i++) {
                     const float v = lab[i];
-                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) {
-                        keep = false;
-                        break;
-                    }
+                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) keep = false;
                 }
             }
         }
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) s_wsum[warp] = __popc(bal);
         __syncthreads();
-        int before = 0;
-        for (int i = 0; i < warp; i++) before += s_wsum[i];
-        if (keep) s_surv[s_ns + before + __popc(bal & ((1u << lane) - 1))] = pool;
-        __syncthreads();
-        if (t == 0) {
-            int tot = 0;
-            for (int i = 0; i < (int)(blockDim.x / 32); i++) tot += s_wsum[i];
-            s_ns += tot;
+        int before = 0, tot = 0;
+        for (int i = 0; i < nw; i++) {
+            before += i < warp ? s_wsum[i] : 0;
+            tot += s_wsum[i];
         }
+        if (keep) s_chunk[before + __popc(bal & ((1u << lane) - 1))] = pool;
         __syncthreads();
-    }
-    const int ns = s_ns;
-    // exact distances, one warp per survivor
-    for (int i = warp; i < cap; i += blockDim.x / 32) {
-        uint64_t key = ~0ull;
-        if (i < ns) {
-            const uint32_t id = D.ids[s_surv[i]];
+        for (int i = warp; i < tot; i += nw) {
+            const uint32_t id = D.ids[s_chunk[i]];
             const float* row = data + (uint64_t)id * d;
             float s = 0.f;
             for (int j = lane; j < d; j += 32) {
@@ -503,14 +941,30 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
                 s = fmaf(df, df, s);
             }
             s = warp_sum(s);
-            key = ((uint64_t)float_key(s) << 32) | id;
+            const uint64_t key = ((uint64_t)float_key(s) << 32) | id;
+            if (lane == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
         }
-        if (lane == 0) s_keys[i] = key;
+        __syncthreads();
+        const int c = s_cnt;
+        __syncthreads();
+        if (c > cap - kThreads) {
+            for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+            __syncthreads();
+            block_bitonic_sort(s_keys, cap);
+            if (t == 0) {
+                s_cnt = min(c, k_out);
+                if (c >= k_out) s_th = s_keys[k_out - 1];
+            }
+            __syncthreads();
+        }
     }
+    const int c = s_cnt;
+    __syncthreads();
+    for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
     __syncthreads();
     block_bitonic_sort(s_keys, cap);
     for (int i = t; i < k_out; i += blockDim.x) {
-        if (i < ns) {
+        if (i < c) {
             const uint64_t key = s_keys[i];
             out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
             out_ids[qi * k_out + i] = (uint32_t)key;
@@ -524,10 +978,13 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
 // ------------------------------------------------------------------------------------
 // host orchestration
 // ------------------------------------------------------------------------------------
+static uint32_t lut_groups(const IndexDev& D) { return (D.M + 31) / 32; }
+
 static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) {
     const hdg_params& P = idx->params;
     const uint64_t l = idx->dev.l, L = idx->dev.n_lists, C = idx->dev.C;
     const uint64_t Pc = std::max<uint64_t>(1, P.n_list), Ps = std::max<uint64_t>(1, P.sub_lists);
+    const uint64_t G = lut_groups(idx->dev);
     size_t off = 0;
     char* base = static_cast<char*>(idx->work.ptr);
     auto take = [&](const char* name, size_t bytes) -> void* {
@@ -548,28 +1005,35 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.range_len = (uint32_t*)take("range_len", q * Ps * 4);
     w.qstat = (uint32_t*)take("qstat", q * 4 * 4);
     w.scal = (uint64_t*)take("scalars", 8 * 8);
+    w.qoff = (uint64_t*)take("qoff", (q + 1) * 8);
+    w.item_off = (uint32_t*)take("item_off", (q + 1) * 4);
+    w.mm = (uint32_t*)take("minmax", q * 2 * 4);
+    w.nfin = (uint32_t*)take("nfin", q * 4);
+    w.counter = (uint32_t*)take("counter", 16);
+    w.lut = (float*)take("lut", q * G * kCodes * 32 * 4);
     w.cand_count = (uint32_t*)take("cand_count", q * 4);
     w.cand_pool = (uint32_t*)take("cand_pool", q * kcand * 4);
     w.kcand = kcand;
+    w.dist = static_cast<float*>(idx->dist_buf.ptr);
     if (!base) idx->work.bytes = std::max(idx->work.bytes, off);  // size probe
     return w;
 }
 
 static size_t workspace_bytes(hdg_index* idx, uint64_t q, uint64_t kcand) {
-    size_t off = 0;
     void* saved = idx->work.ptr;
     idx->work.ptr = nullptr;
     const size_t before = idx->work.bytes;
     idx->work.bytes = 0;
     carve(idx, q, kcand, false);
-    off = idx->work.bytes;
+    const size_t need = idx->work.bytes;
     idx->work.ptr = saved;
     idx->work.bytes = before;
-    return off;
+    return need;
 }
 
 void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand) {
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
+    if (kcand == 0) kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
     const size_t need = workspace_bytes(idx, q, kcand);
     if (idx->work.ptr && idx->work.bytes >= need) return;
     idx->work.reset();
@@ -631,7 +1095,26 @@ struct StageTimer {
         for (auto e : ev) cudaEventDestroy(e);
     }
 };
+
+template <typename K>
+int occupancy_blocks(K kernel, int threads, size_t smem) {
+    int nb = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem));
+    return std::max(nb, 1);
+}
+
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return n;
+}
 }  // namespace
+
+enum ScanMode { kPre = 0, kPost = 1, kL1 = 2 };
 
 void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
@@ -639,7 +1122,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
     HDG_REQUIRE(q > 0 && q < (1ull << 31), HDG_ERR_INVALID_ARG, "query count out of range");
     HDG_REQUIRE(d_queries && d_query_labels && d_dist && d_ids, HDG_ERR_INVALID_ARG, "null pointer");
-    HDG_REQUIRE(k >= 1 && k <= 4096, HDG_ERR_INVALID_ARG, "k must be in [1, 4096]");
+    HDG_REQUIRE(k >= 1 && k <= 2048, HDG_ERR_INVALID_ARG, "k must be in [1, 2048]");
     const hdg_params& P = idx->params;
     const IndexDev& D = idx->dev;
     const int l = (int)D.l;
@@ -649,17 +1132,12 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     const int Pc = (int)std::max<uint64_t>(1, P.n_list);
     const int Ps = (int)std::max<uint64_t>(1, P.sub_lists);
     HDG_REQUIRE(Pc <= 1024 && Ps <= 2048, HDG_ERR_UNSUPPORTED, "n_list <= 1024 and sub_lists <= 2048");
+    HDG_REQUIRE(D.n_lists <= 32768, HDG_ERR_UNSUPPORTED, "at most 32768 inverted lists");
     const uint64_t exps0 = P.exps0;
     const int mode = exps0 <= 1 ? kPre : (l > 1 ? kPost : kL1);
-    HDG_REQUIRE(mode != kPost || d_data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
-    HDG_REQUIRE(mode != kL1 || d_data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
-    HDG_REQUIRE(D.n_lists <= 32768, HDG_ERR_UNSUPPORTED, "at most 32768 inverted lists");
-    const uint64_t k_l1 = exps0 * k;
-    // The candidate buffer is sized for the largest budget up front, so a query never
-    // reallocates between its stages (and never allocates once hdg_reserve has run).
+    HDG_REQUIRE(mode == kPre || d_data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
     const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
-    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand))
-        reserve_workspace(idx, q, kcand);
+    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) reserve_workspace(idx, q, kcand);
     Workspace w = carve(idx, q, kcand, true);
     const FilterDev f = filter_dev(idx);
     StageTimer tm(idx, st, P.break_down != 0);
@@ -681,16 +1159,22 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     CK_LAUNCH();
     tm.mark("coarse");
 
+    // candidate offsets, work items, batch sums; one host read sizes the distance buffer
+    k_batch<<<1, 1024, 0, st>>>(q, w);
+    CK_LAUNCH();
+    uint64_t sc[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const uint64_t coarse = sc[0], real = sc[1], max_row = sc[2];
+    if (idx->dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
+        idx->dist_buf.reset();
+        idx->dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
+    }
+    w.dist = static_cast<float*>(idx->dist_buf.ptr);
     uint64_t K = k;
     float beta = 0.f;
     if (mode == kPost) {
-        k_batch<<<1, 1024, 0, st>>>(w.qstat, q, w.scal);
-        CK_LAUNCH();
-        uint64_t sc[3];
-        CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
         // beta = coarse / real; n_cand = min(exps0*k*beta, max_row_len) (:1219-1222)
-        const uint64_t coarse = sc[0], real = sc[1], max_row = sc[2];
         if (real == 0) {
             K = max_row;
             beta = INFINITY;
@@ -700,9 +1184,8 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
             const uint64_t nc = want >= 1.8e19f ? ~0ull : (uint64_t)want;
             K = std::min<uint64_t>(nc, max_row);
         }
-        tm.mark("budget");
     } else if (mode == kL1) {
-        K = k_l1;
+        K = exps0 * k;
     }
     idx->last_ncand = K;
     if (mode != kPre) {
@@ -711,30 +1194,58 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     }
     idx->last_beta = beta;
     idx->last_q = q;
-
-    const int cap = (int)next_pow2((uint32_t)K + kThreads);
-    const bool fp16 = P.lut_fp16 != 0;
-    const size_t lut_bytes = (size_t)D.M * kCodes * (fp16 ? 2 : 4);
-    const size_t sm_scan = sizeof(uint64_t) * cap + sizeof(float) * D.d + sizeof(uint32_t) * (2 * Ps + 4) + 16 +
-                           lut_bytes;
-    HDG_REQUIRE(sm_scan <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan working set exceeds shared memory");
-    if (fp16) {
-        CK(cudaFuncSetAttribute(k_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_scan));
-        k_scan<true><<<(unsigned)q, kThreads, sm_scan, st>>>(D, d_queries, Ps, mode, (int)K, cap, l, w,
-                                                             d_dist, d_ids, (int)k);
-    } else {
-        CK(cudaFuncSetAttribute(k_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_scan));
-        k_scan<false><<<(unsigned)q, kThreads, sm_scan, st>>>(D, d_queries, Ps, mode, (int)K, cap, l, w,
-                                                              d_dist, d_ids, (int)k);
+    {
+        uint32_t bb;
+        std::memcpy(&bb, &beta, 4);
+        const uint64_t s[8] = {q, idx->last_ncand, K, coarse, real, max_row, bb, (uint64_t)mode};
+        std::memcpy(idx->last_stats, s, sizeof(s));
     }
+    tm.mark("budget");
+
+    const uint32_t G = lut_groups(D);
+    k_lut<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut);
     CK_LAUNCH();
+    tm.mark("lut");
+
+    const int pre = mode == kPre ? 1 : 0;
+    const size_t sm_tab = sizeof(uint32_t) * (2 * Ps + 1);
+    if (sc[3] > 0) {
+        const bool fast = (D.M % 32 == 0) && G <= 3;
+        if (fast) {
+            const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
+            HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
+            auto launch = [&](auto kern, int nt) {
+                CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
+                kern<<<blocks, nt, sm, st>>>(D, Ps, pre, l, q, w);
+            };
+            if (G == 1) launch(k_scan_fast<1, 512>, 512);
+            else if (G == 2) launch(k_scan_fast<2, 512>, 512);
+            else launch(k_scan_fast<3, 1024>, 1024);
+        } else {
+            const size_t sm = sizeof(float) * G * kCodes * 32 + sm_tab;
+            HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
+            CK(cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            const int blocks = sm_count() * occupancy_blocks(k_scan_generic, 512, sm);
+            k_scan_generic<<<blocks, 512, sm, st>>>(D, (int)G, Ps, pre, l, q, w);
+        }
+        CK_LAUNCH();
+    }
     tm.mark("scan");
+
+    const int sorted_out = mode == kPre ? 1 : 0;
+    const size_t sm_sel = sizeof(uint32_t) * kBins + sizeof(uint64_t) * kBCap +
+                          (sorted_out ? sizeof(uint64_t) * next_pow2((uint32_t)std::max<uint64_t>(K, 2)) : 0) + sm_tab + 16;
+    CK(cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sel));
+    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)K, sorted_out, w, d_dist, d_ids, (int)k);
+    CK_LAUNCH();
+    tm.mark("select");
     if (mode != kPre) {
-        const int rcap = (int)next_pow2((uint32_t)std::max<uint64_t>(K, k));
-        const size_t sm_ref = sizeof(uint64_t) * rcap + sizeof(uint32_t) * (K + 1) + sizeof(float) * D.d + 16;
+        const int rcap = (int)next_pow2(k + kThreads);
+        const size_t sm_ref = sizeof(uint64_t) * rcap + sizeof(float) * D.d + 16;
         CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ref));
-        k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, d_queries, d_data, (int)K, rcap,
-                                                       mode == kPost ? 1 : 0, l, w, d_dist, d_ids, (int)k);
+        k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, d_queries, d_data, rcap, mode == kPost ? 1 : 0, l, w,
+                                                       d_dist, d_ids, (int)k);
         CK_LAUNCH();
         tm.mark("refine");
     }

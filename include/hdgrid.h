@@ -106,6 +106,11 @@ hdg_status hdg_parse_config(const char* hdgrid_conf_text, hdg_params* out);
 /* interval_map of *out points into storage owned by the library until the next call. */
 hdg_status hdg_parse_filter(const char* filter_conf_text, hdg_filter_spec* out);
 hdg_status hdg_get_params(const hdg_index* index, hdg_params* out);
+/* Change a search-time key of a built index without rebuilding (no counterpart in the
+ * reference, whose parameters are fixed per run): N_LIST, SUB_LISTS, EXPS0, TOPK,
+ * BREAK_DOWN, IS_SPLIT, N_SPLIT, LUT_FP16, COARSE_BF16 (case-insensitive).  Build-time keys
+ * return HDG_ERR_INVALID_ARG. */
+hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value);
 
 /* ---- build / query --------------------------------------------------------------- */
 
@@ -124,6 +129,13 @@ hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries);
 hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q,
                      const float* d_query_labels, uint32_t label_cols, const float* d_data,
                      uint32_t k, float* d_dist, uint64_t* d_ids, void* stream);
+
+/* Scalars of the last hdg_query: out[0] queries, [1] candidate budget n_cand as the
+ * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget actually used (capped by the
+ * shared-memory top-K), [3] sum of Morton candidate-range sizes, [4] sum of exact filtered
+ * counts of the probed lists, [5] largest per-query candidate count, [6] beta as float bits,
+ * [7] schedule (0 pre-filter, 1 post-filter, 2 single label dim).  Returns entries written. */
+int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap);
 
 /* Per-stage device timings (ms) of the last hdg_query when break_down=1; returns the
  * number of stages written (<= cap) and their names via names (may be NULL). */

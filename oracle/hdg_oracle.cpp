@@ -571,6 +571,8 @@ int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, u
         }
         std::sort(sl.begin(), sl.end());
         const int nps = std::min<int>(Ps, (int)sl.size());
+        // the chosen lists in list-id (= pool) order; RAFT select_k returns them unsorted
+        std::sort(sl.begin(), sl.begin() + nps, [](const auto& a, const auto& b) { return a.second < b.second; });
         s.start.assign(Ps, 0);
         s.len.assign(Ps, 0);
         for (int i = 0; i < nps; i++) {

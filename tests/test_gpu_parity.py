@@ -156,15 +156,36 @@ def test_parity_config4_small_range_filters(cuda):
     _parity(ws, cuda)
 
 
-def test_parity_prefilter_exact(cuda):
-    # exps0 <= 1: predicate before ADC, ADC distances are the output; the ADC sums run in
-    # the reference's subspace order on both sides, so ids and distances match exactly
+def test_parity_prefilter_rotated_adc(cuda):
+    # exps0 <= 1: predicate before ADC, ADC distances are the output.  With M a multiple of
+    # 32 the scan sums each 32-subspace group in a lane-rotated order (bank-conflict-free
+    # LUT), so distances agree with the oracle's subspace-order sums to f32 rounding.
     ws = datasets.config2(scale=0.01, n_queries=200, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
                           max_grids=20_000, exps0=1)
+    _, r = _parity(ws, cuda)
+    g, o = r["g_ids"], r["o_ids"]
+    same = np.mean([len(set(a.tolist()) & set(b.tolist())) / max(1, len(set(b.tolist()))) for a, b in zip(g, o)])
+    assert same >= 0.995, same
+    both = (g == o) & (g != INV)
+    rel = np.abs(r["g_dist"][both] - r["o_dist"][both]) / np.maximum(np.abs(r["o_dist"][both]), 1e-12)
+    assert rel.max() <= 1e-5, rel.max()
+
+
+def test_parity_prefilter_generic_exact(cuda):
+    # M = 16 (not a multiple of 32) takes the natural-order scan: ids and ADC distances
+    # equal the oracle's bit for bit
+    ws = datasets.config1(scale=0.05, n_queries=200, max_grids=100_000, exps0=1, pq_dim=16)
     _, r = _parity(ws, cuda)
     valid = r["g_ids"] != INV
     assert np.array_equal(r["g_ids"], r["o_ids"])
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+
+
+def test_select_handles_large_budget(cuda):
+    # a candidate budget far above the old shared-memory top-K limit (exps0 = 40 -> 4000+)
+    ws = datasets.config2(scale=0.01, n_queries=100, clusters=16, sub_clusters=4, n_list=16, sub_lists=64,
+                          max_grids=20_000, exps0=40)
+    _parity(ws, cuda)
 
 
 def test_parity_masked_label_dim(cuda):
