@@ -290,7 +290,8 @@ def run_hdgrid(args):
         "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4),
                 "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},
-        "gpu_launches": args.steps * (5 if p["exps0"] > 1 and lbl > 1 else 4 if p["exps0"] > 1 else 3),
+        # prologue, coarse, batch, lut, scan, select (+ refine when exps0 > 1) per step
+        "gpu_launches": args.steps * (7 if p["exps0"] > 1 else 6),
         "clocks": clk.summary(),
         "stage_ms": idx.stage_times(),
     }

@@ -38,7 +38,7 @@ _PARAM_FIELDS = [
 
 class hdg_params(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in _PARAM_FIELDS] + [("path", C.c_char * 512)] + [
-        (f, C.c_uint64) for f in ("lut_fp16", "coarse_bf16", "kmeans_iters", "seed")]
+        (f, C.c_uint64) for f in ("lut_fp16", "coarse_bf16", "kmeans_iters", "seed", "scan_cpt")]
 
 
 class hdg_filter_spec(C.Structure):

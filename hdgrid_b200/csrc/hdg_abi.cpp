@@ -163,6 +163,7 @@ hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value) {
         else if (k == "N_SPLIT") f = &p.n_split;
         else if (k == "LUT_FP16") f = &p.lut_fp16;
         else if (k == "COARSE_BF16") f = &p.coarse_bf16;
+        else if (k == "SCAN_CPT") f = &p.scan_cpt;
         HDG_REQUIRE(f, HDG_ERR_INVALID_ARG, "not a search-time key: " + k);
         *f = value;
     });

@@ -121,6 +121,7 @@ void parse_hdgrid_conf(const std::string& text, hdg_params* p) {
         {"COARSE_BF16", &p->coarse_bf16},
         {"KMEANS_ITERS", &p->kmeans_iters},
         {"SEED", &p->seed},
+        {"SCAN_CPT", &p->scan_cpt},
     };
     std::istringstream in(text);
     std::string line;

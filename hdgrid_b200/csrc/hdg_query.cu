@@ -238,12 +238,17 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
         s_red[0] = s_red[1] = 0;
     }
     __syncthreads();
-    // clusters with a non-zero filtered count (filter_none_zero_data :1027-1028)
+    // clusters with a non-zero filtered count (filter_none_zero_data :1027-1028).  When all
+    // of them fit in n_list the ranking cannot change the chosen set: no distances needed.
+    for (int c = t; c < (int)D.C; c += blockDim.x)
+        if (w.cluster_counts[qi * D.C + c] > 0) atomicAdd(&s_nvalid, 1);
+    __syncthreads();
+    const bool all_c = s_nvalid <= Pc;
     for (int c = t; c < sort_n1; c += blockDim.x) {
         uint64_t key = ~0ull;
         if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
-            key = ((uint64_t)float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d)) << 32) | (uint32_t)c;
-            atomicAdd(&s_nvalid, 1);
+            const uint32_t dk = all_c ? 0u : float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d));
+            key = ((uint64_t)dk << 32) | (uint32_t)c;
         }
         s_keys[c] = key;
     }
@@ -258,8 +263,14 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     __syncthreads();
     if (t == 0) s_nvalid = 0;
     __syncthreads();
-    // the non-empty lists of the chosen clusters
+    // the non-empty lists of the chosen clusters (again no distances when all are taken)
     const uint32_t Smax = D.S_max;
+    for (int e = t; e < npc * (int)Smax; e += blockDim.x) {
+        const uint32_t c = s_chosen[e / Smax], j = D.cluster_off[c] + e % Smax;
+        if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) atomicAdd(&s_nvalid, 1);
+    }
+    __syncthreads();
+    const bool all_l = s_nvalid <= Ps;
     for (int e = t; e < sort_n2; e += blockDim.x) {
         uint64_t key = ~0ull;
         const int i = e / Smax, jj = e % Smax;
@@ -267,8 +278,9 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
             const uint32_t c = s_chosen[i];
             const uint32_t j = D.cluster_off[c] + jj;
             if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
-                key = ((uint64_t)float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d)) << 32) | j;
-                atomicAdd(&s_nvalid, 1);
+                const uint32_t dk =
+                    all_l ? 0u : float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d));
+                key = ((uint64_t)dk << 32) | j;
             }
         }
         s_keys[e] = key;
@@ -397,27 +409,75 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
 // (build_pq_lut_kernel, product-quantization.cu:4-35; the reference's `ans += (c-q)*(c-q)`
 // is an FMA under nvcc's default contraction), zero for m >= M.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_lut(IndexDev D, const float* __restrict__ queries, int G,
+constexpr int kLutQ = 64;          // queries per k_lut block
+constexpr int kLutMaxPqLen = 6;    // staged codebook group fits shared memory up to this pq_len
+
+// Block = (64 queries, one group of 32 subspaces).  The group's codebook is staged once in
+// shared memory as [c*pq_len + t][33] (conflict-free stores from coalesced global reads and
+// conflict-free lane reads); lane = subspace column j, so a warp stores one contiguous
+// 128-byte LUT row per codeword.
+__global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict__ queries, uint64_t q, int G,
                                              float* __restrict__ lut) {
-    extern __shared__ float s_q[];
+    extern __shared__ float smem_lut[];
+    const int g = blockIdx.y, pq_len = D.pq_len, d = D.d, M = D.M;
+    float* s_cb = smem_lut;                          // [(c * pq_len + t) * 33 + j]
+    const int n = 32 * kCodes * pq_len;
+    const float* src = D.pq_centers + (uint64_t)(32 * g) * kCodes * pq_len;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int j = e / (kCodes * pq_len), rem = e - j * (kCodes * pq_len);
+        s_cb[rem * 33 + j] = (32 * g + j < M) ? __ldg(src + e) : 0.f;
+    }
+    __syncthreads();
+    // one warp per query: lane j keeps the query's slice of subspace 32g+j in registers
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int m = 32 * g + lane;
+    const bool real = m < M;
+    for (int qq = warp; qq < kLutQ; qq += nw) {
+        const uint64_t qi = (uint64_t)blockIdx.x * kLutQ + qq;
+        if (qi >= q) break;
+        float qv[kLutMaxPqLen];
+#pragma unroll
+        for (int t = 0; t < kLutMaxPqLen; t++)
+            qv[t] = (real && t < pq_len) ? queries[qi * d + (uint64_t)m * pq_len + t] : 0.f;
+        float* out = lut + (qi * G + g) * (kCodes * 32);
+        for (int c = 0; c < kCodes; c++) {
+            float s = 0.f;
+#pragma unroll
+            for (int t = 0; t < kLutMaxPqLen; t++) {
+                if (t < pq_len) {
+                    const float df = __fsub_rn(s_cb[(c * pq_len + t) * 33 + lane], qv[t]);
+                    s = fmaf(df, df, s);
+                }
+            }
+            out[c * 32 + lane] = real ? s : 0.f;
+        }
+    }
+}
+
+// Fallback for long subspaces: one query per block, thread = codeword, transposed store.
+__global__ void __launch_bounds__(256) k_lut_plain(IndexDev D, const float* __restrict__ queries, int G,
+                                                   float* __restrict__ lut) {
+    extern __shared__ float s_q[];     // [d]
+    __shared__ float s_t[kCodes][33];  // [c][j]
     const uint64_t qi = blockIdx.x;
-    const int g = blockIdx.y;
-    const int d = D.d, pq_len = D.pq_len;
+    const int g = blockIdx.y, d = D.d, pq_len = D.pq_len, c = threadIdx.x;
     for (int i = threadIdx.x; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
     __syncthreads();
-    float* out = lut + ((uint64_t)qi * G + g) * (kCodes * 32);
-    for (int e = threadIdx.x; e < kCodes * 32; e += blockDim.x) {
-        const int c = e >> 5, j = e & 31, m = g * 32 + j;
+    for (int j = 0; j < 32; j++) {
+        const int m = g * 32 + j;
         float s = 0.f;
         if (m < (int)D.M) {
             const float* cw = D.pq_centers + ((uint64_t)m * kCodes + c) * pq_len;
             for (int tt = 0; tt < pq_len; tt++) {
-                const float df = __fsub_rn(cw[tt], s_q[m * pq_len + tt]);
+                const float df = __fsub_rn(__ldg(cw + tt), s_q[m * pq_len + tt]);
                 s = fmaf(df, df, s);
             }
         }
-        out[e] = s;
+        s_t[c][j] = s;
     }
+    __syncthreads();
+    float* out = lut + (qi * G + g) * (kCodes * 32);
+    for (int e = threadIdx.x; e < kCodes * 32; e += blockDim.x) out[e] = s_t[e >> 5][e & 31];
 }
 
 // ------------------------------------------------------------------------------------
@@ -457,9 +517,13 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
     block_exclusive_scan(s_pre, Ps + 1, s_warp);
 }
 
-template <int G, int NT>
-__global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre, int lbl, uint64_t q,
-                                                     Workspace w) {
+// Fast path (M a multiple of 32).  The CTA computes the query's LUT straight into shared
+// memory when it switches query (codeword-major loads, one subspace per lane), then streams
+// candidates; CPT candidates per thread are interleaved step by step so every thread keeps
+// CPT independent load->add chains in flight.
+template <int G, int NT, int CPT>
+__global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __restrict__ queries, int Ps,
+                                                     int pre, int lbl, uint64_t q, Workspace w) {
     extern __shared__ __align__(16) float s_lut[];  // [G][256][64]
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 64);  // [Ps + 1]
     uint32_t* s_start = s_pre + Ps + 1;                                       // [Ps]
@@ -467,7 +531,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre
     __shared__ uint32_t s_warp[32];
     __shared__ float s_box[2 * kMaxDims];
     const int t = threadIdx.x, lane = t & 31;
-    const uint32_t R = lane >> 2, sh = 8u * (lane & 3);
+    const uint32_t R = lane >> 2, sh = 8u * (lane & 3), lane4 = 4u * lane;
     const uint32_t n_items = w.item_off[q];
     int cur = -1;
     for (;;) {
@@ -491,11 +555,11 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre
         if (qq != cur) {
             const float4* src = reinterpret_cast<const float4*>(w.lut + (uint64_t)qq * G * kCodes * 32);
             for (int e = t; e < G * kCodes * 8; e += NT) {
-                const float4 v = src[e];
+                const float4 v = __ldg(src + e);
                 const int row = e >> 3, col = (e & 7) * 4;  // row = g*256 + c
-                float4* dst = reinterpret_cast<float4*>(s_lut + row * 64 + col);
-                dst[0] = v;
-                dst[8] = v;  // columns 32..63 repeat 0..31
+                float4* dstl = reinterpret_cast<float4*>(s_lut + row * 64 + col);
+                dstl[0] = v;
+                dstl[8] = v;  // columns 32..63 repeat 0..31
             }
             if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
             scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
@@ -506,53 +570,81 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre
         const uint32_t e1 = min(total, e0 + kChunk);
         float* dst = w.dist + w.qoff[qq];
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
-        int r = 0;
-        {
-            const uint32_t e = e0 + t;
+        int r[CPT];
+#pragma unroll
+        for (int u = 0; u < CPT; u++) {
+            const uint32_t e = e0 + t + u * NT;
             int lo = 0, hi = Ps - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
                 if (s_pre[mid] <= e) lo = mid;
                 else hi = mid - 1;
             }
-            r = lo;
+            r[u] = lo;
         }
-        for (uint32_t e = e0 + t; e < e1; e += NT) {
-            while (s_pre[r + 1] <= e) r++;
-            const uint32_t pool = s_start[r] + (e - s_pre[r]);
-            bool pass = true;
-            if (pre) {
-                const float* lab = D.labels + (uint64_t)pool * lbl;
-                for (int i = 0; i < lbl; i++) {
-                    const float v = lab[i];
-                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
-                }
-            }
-            float sum = INFINITY;
-            if (pass) {
-                sum = 0.f;
-                const uint4* cp = reinterpret_cast<const uint4*>(D.codes + (uint64_t)pool * D.M_pad);
+        for (uint32_t eb = e0 + t; eb < e1; eb += NT * CPT) {
+            const uint4* cp[CPT];
+            bool live[CPT];
+            float sum[CPT];
 #pragma unroll
-                for (int g = 0; g < G; g++) {
-                    const uint4 a = __ldg(cp + 2 * g), b = __ldg(cp + 2 * g + 1);
-                    uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-                    rotate_words(wv, R);
-                    uint32_t x[8];
-#pragma unroll
-                    for (int i = 0; i < 8; i++) x[i] = __funnelshift_r(wv[i], wv[(i + 1) & 7], sh);
-                    const float* L = s_lut + g * (kCodes * 64) + lane;
-#pragma unroll
-                    for (int st = 0; st < 32; st++) {
-                        const uint32_t c = __byte_perm(x[st >> 2], 0u, 0x4440u | (st & 3));
-                        sum += L[c * 64 + st];
+            for (int u = 0; u < CPT; u++) {
+                const uint32_t e = eb + u * NT;
+                live[u] = e < e1;
+                sum[u] = INFINITY;
+                uint32_t row = 0;  // dead / filtered candidates read row 0 (in bounds), result discarded
+                if (live[u]) {
+                    while (s_pre[r[u] + 1] <= e) r[u]++;
+                    const uint32_t pool = s_start[r[u]] + (e - s_pre[r[u]]);
+                    bool pass = true;
+                    if (pre) {
+                        const float* lab = D.labels + (uint64_t)pool * lbl;
+                        for (int i = 0; i < lbl; i++) {
+                            const float v = lab[i];
+                            if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
+                        }
+                    }
+                    if (pass) {
+                        sum[u] = 0.f;
+                        row = pool;
                     }
                 }
-                const uint32_t key = float_key(sum);
-                kmin = min(kmin, key);
-                kmax = max(kmax, key);
-                nf++;
+                cp[u] = reinterpret_cast<const uint4*>(D.codes + (uint64_t)row * D.M_pad);
             }
-            dst[e] = sum;
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                uint32_t x[CPT][8];
+#pragma unroll
+                for (int u = 0; u < CPT; u++) {
+                    const uint4 a = __ldg(cp[u] + 2 * g), b = __ldg(cp[u] + 2 * g + 1);
+                    uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+                    rotate_words(wv, R);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) x[u][i] = __funnelshift_r(wv[i], wv[(i + 1) & 7], sh);
+                }
+                const char* L = reinterpret_cast<const char*>(s_lut + g * (kCodes * 64));
+#pragma unroll
+                for (int st = 0; st < 32; st++) {
+#pragma unroll
+                    for (int u = 0; u < CPT; u++) {
+                        // one PRMT builds the byte offset c*256 + lane*4 (code byte -> byte 1,
+                        // the lane's column byte -> byte 0); the step's column is the immediate
+                        const uint32_t a = __byte_perm(x[u][st >> 2], lane4, 0x5504u | ((st & 3) << 4));
+                        sum[u] += reinterpret_cast<const float*>(L + a)[st];
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < CPT; u++) {
+                if (!live[u]) continue;
+                const uint32_t e = eb + u * NT;
+                if (sum[u] < INFINITY) {
+                    const uint32_t key = float_key(sum[u]);
+                    kmin = min(kmin, key);
+                    kmax = max(kmax, key);
+                    nf++;
+                }
+                dst[e] = sum[u];
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -568,7 +660,6 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, int Ps, int pre
         __syncthreads();
     }
 }
-
 // Generic ADC (any M): natural subspace order, LUT [G][256][32] in shared memory.
 __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps, int pre, int lbl, uint64_t q,
                                                       Workspace w) {
@@ -748,9 +839,16 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
                 s_nb = 0;
             }
             __syncthreads();
-            for (uint32_t e = t; e < total; e += blockDim.x) {
-                const float d = dist[e];
-                if (d < INFINITY && inside(d, level)) atomicAdd(&s_hist[sel_bin(d, lo, inv)], 1u);
+            for (uint32_t e0 = t; e0 < total; e0 += 4 * blockDim.x) {
+                float dv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {  // four independent loads in flight per thread
+                    const uint32_t e = e0 + u * blockDim.x;
+                    dv[u] = e < total ? __ldg(dist + e) : INFINITY;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (dv[u] < INFINITY && inside(dv[u], level)) atomicAdd(&s_hist[sel_bin(dv[u], lo, inv)], 1u);
             }
             __syncthreads();
             if (t < 32) {  // first bin whose cumulative count reaches need
@@ -782,19 +880,29 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             __syncthreads();
             const int b = s_bin;
             const bool fits = s_cntb <= (uint32_t)kBCap;
-            for (uint32_t e = t; e < total; e += blockDim.x) {
-                const float d = dist[e];
-                if (!(d < INFINITY) || !inside(d, level)) continue;
-                const int bb = sel_bin(d, lo, inv);
-                if (bb < b) {
-                    emit(e, d);
-                } else if (bb == b) {
-                    if (fits) {
-                        const uint32_t p = atomicAdd(&s_nb, 1u);
-                        s_bbuf[p] = ((uint64_t)float_key(d) << 32) | e;
-                    } else {
-                        atomicMin(&s_bmin, float_key(d));
-                        atomicMax(&s_bmax, float_key(d));
+            for (uint32_t e0 = t; e0 < total; e0 += 4 * blockDim.x) {
+                float dv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const uint32_t e = e0 + u * blockDim.x;
+                    dv[u] = e < total ? __ldg(dist + e) : INFINITY;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const float d = dv[u];
+                    const uint32_t e = e0 + u * blockDim.x;
+                    if (!(d < INFINITY) || !inside(d, level)) continue;
+                    const int bb = sel_bin(d, lo, inv);
+                    if (bb < b) {
+                        emit(e, d);
+                    } else if (bb == b) {
+                        if (fits) {
+                            const uint32_t p = atomicAdd(&s_nb, 1u);
+                            s_bbuf[p] = ((uint64_t)float_key(d) << 32) | e;
+                        } else {
+                            atomicMin(&s_bmin, float_key(d));
+                            atomicMax(&s_bmax, float_key(d));
+                        }
                     }
                 }
             }
@@ -1203,25 +1311,46 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     tm.mark("budget");
 
     const uint32_t G = lut_groups(D);
-    k_lut<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut);
-    CK_LAUNCH();
-    tm.mark("lut");
+    const bool fast = (D.M % 32 == 0) && G <= 3;
+    {
+        if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
+            const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
+            CK(cudaFuncSetAttribute(k_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, d_queries, q, (int)G, w.lut);
+        } else {
+            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut);
+        }
+        CK_LAUNCH();
+        tm.mark("lut");
+    }
 
     const int pre = mode == kPre ? 1 : 0;
     const size_t sm_tab = sizeof(uint32_t) * (2 * Ps + 1);
     if (sc[3] > 0) {
-        const bool fast = (D.M % 32 == 0) && G <= 3;
         if (fast) {
             const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
-                kern<<<blocks, nt, sm, st>>>(D, Ps, pre, l, q, w);
+                kern<<<blocks, nt, sm, st>>>(D, d_queries, Ps, pre, l, q, w);
             };
-            if (G == 1) launch(k_scan_fast<1, 512>, 512);
-            else if (G == 2) launch(k_scan_fast<2, 512>, 512);
-            else launch(k_scan_fast<3, 1024>, 1024);
+            // threads x candidates-per-thread (SCAN_CPT; 0 = measured default 1: more
+            // interleaved candidates per thread ran slower at M = 32 and M = 96)
+            const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
+            if (G == 1) {
+                if (cpt == 1) launch(k_scan_fast<1, 512, 1>, 512);
+                else if (cpt == 2) launch(k_scan_fast<1, 512, 2>, 512);
+                else launch(k_scan_fast<1, 256, 4>, 256);
+            } else if (G == 2) {
+                if (cpt == 1) launch(k_scan_fast<2, 512, 1>, 512);
+                else if (cpt == 2) launch(k_scan_fast<2, 512, 2>, 512);
+                else launch(k_scan_fast<2, 256, 4>, 256);
+            } else {
+                if (cpt == 1) launch(k_scan_fast<3, 1024, 1>, 1024);
+                else if (cpt == 2) launch(k_scan_fast<3, 512, 2>, 512);
+                else launch(k_scan_fast<3, 256, 4>, 256);
+            }
         } else {
             const size_t sm = sizeof(float) * G * kCodes * 32 + sm_tab;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");

@@ -76,6 +76,7 @@ typedef struct hdg_params {
     uint64_t coarse_bf16;   /* COARSE_BF16: coarse assignment as a BF16 tensor-core GEMM */
     uint64_t kmeans_iters;  /* KMEANS_ITERS: Lloyd iterations of the index build (default 20) */
     uint64_t seed;          /* SEED: build RNG seed (default 1234) */
+    uint64_t scan_cpt;      /* SCAN_CPT: ADC scan candidates per thread (1, 2 or 4; 0 = default) */
 } hdg_params;
 
 /* filter.conf contents (config_utils.h:112-172).  interval_map is the flat

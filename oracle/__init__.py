@@ -37,7 +37,7 @@ def _load() -> C.CDLL:
     lib.ora_check_layout.restype = C.c_uint64
     lib.ora_check_layout.argtypes = [vp]
     lib.ora_query.restype = C.c_int
-    lib.ora_query.argtypes = [vp, vp, C.c_uint64, vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, C.c_int]
+    lib.ora_query.argtypes = [vp, vp, C.c_uint64, vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, C.c_int, C.c_int]
     lib.ora_bruteforce_f64.argtypes = [vp, C.c_uint64, C.c_uint32, vp, C.c_uint32, vp, C.c_uint64, vp, C.c_uint32,
                                        vp, vp, C.c_int]
     lib.ora_pq_lut.argtypes = [vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp]
@@ -189,7 +189,7 @@ class OracleIndex:
     def check_layout(self) -> int:
         return int(LIB.ora_check_layout(self._h))
 
-    def query(self, queries, query_labels, data, k, threads=0, trace=True):
+    def query(self, queries, query_labels, data, k, threads=0, trace=True, adc_rotated=False):
         n_list, sub_lists = self.n_list, self.sub_lists
         queries = _c(queries, np.float32)
         ql = _c(query_labels, np.float32)
@@ -208,7 +208,7 @@ class OracleIndex:
                      scalars=np.zeros(4, np.float64))
             tr = _Trace(*(t[n].ctypes.data for n, _ in _Trace._fields_))
         rc = LIB.ora_query(self._h, _p(queries), q, _p(ql), ql.shape[1], _p(data), k, _p(dist), _p(ids),
-                           C.byref(tr) if tr is not None else None, threads)
+                           C.byref(tr) if tr is not None else None, threads, 1 if adc_rotated else 0)
         if rc != 0:
             raise RuntimeError(LIB.ora_last_error().decode())
         return dist, ids, t

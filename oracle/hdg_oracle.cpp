@@ -508,7 +508,8 @@ struct OraTrace {
 // super_grid::index::query (Super-Grid-IVF_PQ.cu:985-1249) on the CPU.
 // Outputs dist [q x k] f32 and ids [q x k] u64 (ascending; +inf / UINT64_MAX when empty).
 int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, uint32_t label_cols,
-              const float* data, uint32_t k, float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads) {
+              const float* data, uint32_t k, float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads,
+              int adc_mode) {
     const Index& ix = *static_cast<Index*>(h);
     const Grid& g = ix.g;
     const int l = (int)ix.l, d = (int)ix.d, M = (int)ix.M;
@@ -655,17 +656,31 @@ int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, u
             }
             return true;
         };
-        auto adc = [&](uint32_t pool) {
+        // adc_mode 0: subspace order 0..M-1 (compute_batched_L2_distance_kernel :69-72).
+        // adc_mode 1 (test mode): the order of the GPU scan's bank-rotated LUT, where the
+        // candidate at position e of the query sums each group of 32 subspaces starting at
+        // subspace (e mod 32) and wrapping -- used to check that scan bit for bit.
+        auto adc = [&](uint32_t pool, uint32_t pos) {
             float sum = 0.f;
             const uint8_t* cp = &ix.codes[(uint64_t)pool * ix.M_pad];
-            for (int m = 0; m < M; m++) sum += lut[(size_t)m * kCodes + cp[m]];
+            if (adc_mode == 1) {
+                const int lane = (int)(pos & 31);
+                for (int g0 = 0; g0 < M; g0 += 32)
+                    for (int st = 0; st < 32; st++) {
+                        const int m = g0 + ((lane + st) & 31);
+                        sum += lut[(size_t)m * kCodes + cp[m]];
+                    }
+            } else {
+                for (int m = 0; m < M; m++) sum += lut[(size_t)m * kCodes + cp[m]];
+            }
             return sum;
         };
         std::vector<std::pair<float, uint32_t>> cand;
+        uint32_t pos = 0;
         for (int r = 0; r < Ps; r++)
-            for (uint32_t p = s.start[r]; p < s.start[r] + s.len[r]; p++) {
+            for (uint32_t p = s.start[r]; p < s.start[r] + s.len[r]; p++, pos++) {
                 if (mode == 0 && !pred(p)) continue;  // query_prefilter (prefiltering.cu:36-51)
-                cand.push_back({adc(p), p});
+                cand.push_back({adc(p, pos), p});
             }
         std::sort(cand.begin(), cand.end());
         if (mode == 0) {
