@@ -85,6 +85,7 @@ def _load() -> C.CDLL:
         "hdg_pq_adc": [vp, u64, vp, u64, u32, u32, vp, u64, vp, vp],
         "hdg_label_mask": [vp, vp, u32, u64, u64, vp, u64, vp, vp],
         "hdg_recover_filters": [C.POINTER(hdg_filter_spec), vp, u64, vp, vp],
+        "hdg_recover_filters_noalloc": [C.POINTER(hdg_filter_spec), vp, u64, vp, vp],
         "hdg_bruteforce_knn": [vp, u64, u32, vp, u32, vp, u64, vp, u32, vp, vp, vp],
     }
     for name, args in sigs.items():
@@ -102,6 +103,7 @@ def _load() -> C.CDLL:
 
 LIB = _load()
 EXPORTED = [n for n in dir(LIB) if n.startswith("hdg_")]
+LIB_NOALLOC_MAP_MAX = 65536  # HDG_NOALLOC_MAP_MAX of include/hdgrid.h
 
 
 def _check(status: int) -> None:

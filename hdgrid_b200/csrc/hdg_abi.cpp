@@ -325,6 +325,29 @@ hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query
     });
 }
 
+hdg_status hdg_recover_filters_noalloc(const hdg_filter_spec* spec, const float* d_query_labels, uint64_t n_queries,
+                                       float* d_ranges, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(spec && d_query_labels && d_ranges, HDG_ERR_INVALID_ARG, "null pointer");
+        HDG_REQUIRE(spec->l >= 1 && spec->l <= HDG_MAX_LABEL_DIMS, HDG_ERR_INVALID_ARG, "bad l");
+        HDG_REQUIRE(spec->n_map == 0 || spec->interval_map, HDG_ERR_INVALID_ARG, "null interval map");
+        FilterDev f{};
+        f.l = spec->l;
+        bool range = false;
+        for (int i = 0; i < HDG_MAX_LABEL_DIMS; i++) {
+            f.type[i] = spec->type[i];
+            f.div_value[i] = spec->div_value[i] ? spec->div_value[i] : 1;
+            f.shift_val[2 * i] = spec->shift_val[2 * i];
+            f.shift_val[2 * i + 1] = spec->shift_val[2 * i + 1];
+            if (i < spec->l && spec->type[i] == 3) range = true;
+        }
+        f.filter_dim = range ? 2 : 1;
+        f.n_map = spec->n_map;
+        recover_filters_noalloc(f, spec->interval_map, d_query_labels, n_queries, d_ranges,
+                                static_cast<cudaStream_t>(stream));
+    });
+}
+
 hdg_status hdg_bruteforce_knn(const float* d_data, uint64_t n, uint32_t d, const float* d_labels, uint32_t l,
                               const float* d_queries, uint64_t q, const float* d_ranges, uint32_t k,
                               float* d_dist, uint64_t* d_ids, void* stream) {

@@ -55,6 +55,8 @@ void label_mask(const float* ranges, const float* labels, uint32_t l, uint64_t n
                 const uint64_t* indices, uint64_t n_cand, int32_t* mask, cudaStream_t st);
 void recover_filters(const FilterDev& f, const float* qlabels, uint64_t nq, float* ranges,
                      cudaStream_t st);
+void recover_filters_noalloc(const FilterDev& f, const float* host_map, const float* qlabels, uint64_t nq,
+                             float* ranges, cudaStream_t st);
 void bruteforce_knn(const float* data, uint64_t n, uint32_t d, const float* labels, uint32_t l,
                     const float* queries, uint64_t q, const float* ranges, uint32_t k, float* dist,
                     uint64_t* ids, cudaStream_t st);

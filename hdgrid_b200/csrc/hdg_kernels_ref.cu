@@ -7,6 +7,8 @@
 //   bruteforce_knn  brute_forece_vector_search     (src/verification/ground_truth.cuh:165-232),
 //                   with the filter.conf predicate instead of its hard-coded window.
 #include <cfloat>
+#include <mutex>
+#include <vector>
 
 #include "hdg_device.cuh"
 #include "hdg_internal.h"
@@ -107,6 +109,46 @@ void recover_filters(const FilterDev& f, const float* qlabels, uint64_t nq, floa
     if (!nq) return;
     k_recover<<<nblk(nq, 128), 128, 0, st>>>(f, qlabels, nq, ranges);
     CK_LAUNCH();
+}
+
+// ---- allocation-free filter recovery ---------------------------------------------------
+// Scratch for the interval-map table of hdg_recover_filters_noalloc: a fixed array in the
+// library's own device memory, present on every GPU that loads the library until the
+// process exits.  Host code must not pass `g_noalloc_map` itself to a kernel (on the host it
+// is only a stand-in symbol); it passes the device address fetched below.
+static __device__ __align__(256) float g_noalloc_map[HDG_NOALLOC_MAP_MAX];
+
+namespace {
+std::mutex g_noalloc_mu;
+std::vector<float*> g_noalloc_ptr;  // per device ordinal, filled on first use
+}  // namespace
+
+// Device address of the scratch array on the current device.  The first call on a device
+// resolves it with cudaGetSymbolAddress (that device must be current); later calls reuse it.
+static float* noalloc_map_scratch() {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if ((int)g_noalloc_ptr.size() <= dev) g_noalloc_ptr.resize(dev + 1, nullptr);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_map));
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+void recover_filters_noalloc(const FilterDev& f0, const float* host_map, const float* qlabels, uint64_t nq,
+                             float* ranges, cudaStream_t st) {
+    HDG_REQUIRE(f0.n_map >= 0 && f0.n_map <= HDG_NOALLOC_MAP_MAX, HDG_ERR_INVALID_ARG,
+                "interval map of " + std::to_string(f0.n_map) + " entries exceeds the " +
+                    std::to_string(HDG_NOALLOC_MAP_MAX) + "-entry limit of hdg_recover_filters_noalloc");
+    FilterDev f = f0;
+    f.map = noalloc_map_scratch();
+    // the whole used prefix is rewritten every call, so nothing has to start at zero
+    if (f.n_map) CK(cudaMemcpyAsync(const_cast<float*>(f.map), host_map, sizeof(float) * f.n_map,
+                                    cudaMemcpyHostToDevice, st));
+    recover_filters(f, qlabels, nq, ranges, st);
 }
 
 // ---- filtered exact kNN ------------------------------------------------------------------

@@ -184,6 +184,22 @@ hdg_status hdg_label_mask(const float* d_ranges, const float* d_labels, uint32_t
 /* filters [q x 2l] f32 from the query labels and a filter spec. */
 hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query_labels,
                                uint64_t n_queries, float* d_ranges, void* stream);
+/* Allocation-free variant of hdg_recover_filters -- no counterpart in the reference.
+ * For callers that must not allocate device memory while they run: a host application
+ * whose own allocator owns the GPU's memory, or a serving loop that cannot afford the
+ * device-wide synchronisation cudaMalloc / cudaFree may cause.  hdg_recover_filters keeps
+ * a per-call device copy of the filter's interval-map table; this variant keeps it in a
+ * fixed scratch array of HDG_NOALLOC_MAP_MAX floats inside the library (present on every
+ * GPU that loads the library until the process exits) and allocates nothing.  The caller
+ * still passes the labels and the output.  Maps longer than HDG_NOALLOC_MAP_MAX entries
+ * return HDG_ERR_INVALID_ARG.  The first call on a device looks up the scratch array's
+ * device address (make that device current, and make that first call before any stream
+ * capture).  All calls share the one array: calls whose work overlaps on the GPU (other
+ * streams, other threads) race on it and must be serialised by the caller. */
+#define HDG_NOALLOC_MAP_MAX 65536
+hdg_status hdg_recover_filters_noalloc(const hdg_filter_spec* spec, const float* d_query_labels,
+                                       uint64_t n_queries, float* d_ranges, void* stream);
+
 /* Exact filtered kNN in FP32: distances of every base vector whose labels pass the
  * per-query box d_ranges [q x 2l]; k smallest, ascending, ties by lower id. */
 hdg_status hdg_bruteforce_knn(const float* d_data, uint64_t n, uint32_t d,
