@@ -87,6 +87,7 @@ def _load() -> C.CDLL:
         "hdg_recover_filters": [C.POINTER(hdg_filter_spec), vp, u64, vp, vp],
         "hdg_recover_filters_noalloc": [C.POINTER(hdg_filter_spec), vp, u64, vp, vp],
         "hdg_bruteforce_knn": [vp, u64, u32, vp, u32, vp, u64, vp, u32, vp, vp, vp],
+        "hdg_bf16_gemm": [vp, u64, vp, u64, u32, vp, u64, vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -344,6 +345,12 @@ def bruteforce_knn(data, labels, queries, ranges, k: int, out_dist, out_ids, str
     _check(LIB.hdg_bruteforce_knn(_ptr(data), data.shape[0], data.shape[1], _ptr(labels), labels.shape[1],
                                   _ptr(queries), queries.shape[0], _ptr(ranges), k, _ptr(out_dist), _ptr(out_ids),
                                   _stream_ptr(stream)))
+
+
+def bf16_gemm(a_bf16, b_bf16, out, stream=None) -> None:
+    """out[r][c] = a[r] . b[c] on the tcgen05 tensor cores (bf16 in, f32 out)."""
+    _check(LIB.hdg_bf16_gemm(_ptr(a_bf16), a_bf16.shape[0], _ptr(b_bf16), b_bf16.shape[0], a_bf16.shape[1],
+                             _ptr(out), out.stride(0), _stream_ptr(stream)))
 
 
 def version() -> str:

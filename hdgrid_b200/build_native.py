@@ -27,6 +27,7 @@ LIB_SOURCES = [
     "hdg_build.cu",
     "hdg_query.cu",
     "hdg_kernels_ref.cu",
+    "hdg_gemm.cu",
 ]
 
 

@@ -325,6 +325,22 @@ hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query
     });
 }
 
+hdg_status hdg_bf16_gemm(const void* d_a, uint64_t rows, const void* d_b, uint64_t cols, uint32_t d, float* d_out,
+                         uint64_t ldo, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_a && d_b && d_out && d > 0, HDG_ERR_INVALID_ARG, "bad argument");
+        DeviceBuffer err;
+        err.ensure(sizeof(int));
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        CK(cudaMemsetAsync(err.ptr, 0, sizeof(int), st));
+        umma_dot(d_a, rows, d_b, cols, (int)d, d_out, ldo, static_cast<int*>(err.ptr), st);
+        int h = 0;
+        CK(cudaMemcpyAsync(&h, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        HDG_REQUIRE(h == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
+    });
+}
+
 hdg_status hdg_recover_filters_noalloc(const hdg_filter_spec* spec, const float* d_query_labels, uint64_t n_queries,
                                        float* d_ranges, void* stream) {
     return guarded([&] {

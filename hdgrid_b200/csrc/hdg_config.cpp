@@ -89,6 +89,7 @@ void default_params(hdg_params* p) {
     p->n_split = 1;
     p->kmeans_iters = 20;
     p->seed = 1234;
+    p->coarse_bf16 = 1;
 }
 
 void parse_hdgrid_conf(const std::string& text, hdg_params* p) {

@@ -57,6 +57,10 @@ void recover_filters(const FilterDev& f, const float* qlabels, uint64_t nq, floa
                      cudaStream_t st);
 void recover_filters_noalloc(const FilterDev& f, const float* host_map, const float* qlabels, uint64_t nq,
                              float* ranges, cudaStream_t st);
+// tcgen05 BF16 GEMM (hdg_gemm.cu)
+void umma_dot(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
+              uint64_t ldo, int* err, cudaStream_t st);
+void rows_to_bf16(const float* x, uint64_t n, int d, void* y, float* norms, cudaStream_t st);
 void bruteforce_knn(const float* data, uint64_t n, uint32_t d, const float* labels, uint32_t l,
                     const float* queries, uint64_t q, const float* ranges, uint32_t k, float* dist,
                     uint64_t* ids, cudaStream_t st);

@@ -61,6 +61,11 @@ struct Workspace {
     uint32_t* cand_count;    // [q]
     uint64_t kcand;
     float* dist;             // [sum of candidates]
+    float* S;                // [q x (C + L)] tensor-core dot products (nullptr: exact path only)
+    uint64_t ldS;
+    float* qnorm;            // [q] squared query norms
+    void* qbf;               // [q x d] bf16 queries
+    int* gemm_err;           // tensor-core wait expiry flag
 };
 
 // Exclusive block-wide scan of n u32 values in shared memory (in place).  All threads.
@@ -221,6 +226,19 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* __restrict__
     return lo;
 }
 
+// Band [lo, hi] around the exact f32 distance of query qi to centroid col (clusters first,
+// then lists) from the tensor-core dot product S: |(|q|^2 + |c|^2 - 2 q.c) - exact| is below
+// 2 * 2^-8 |q||c| for BF16-rounded inputs, plus f32 rounding of the norms and sums; the band
+// doubles both terms.
+__device__ __forceinline__ void approx_band(const IndexDev& D, const Workspace& w, uint64_t qi, uint32_t col,
+                                            float* lo, float* hi) {
+    const float qn = w.qnorm[qi], cn = D.cnorm[col];
+    const float a = qn + cn - 2.f * w.S[qi * w.ldS + col];
+    const float e = 0.015625f * sqrtf(qn * cn) + 1e-4f * (qn + cn);
+    *lo = a - e;
+    *hi = a + e;
+}
+
 __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __restrict__ queries,
                                                      int Pc, int Ps, int sort_n1, int sort_n2,
                                                      Workspace w) {
@@ -229,6 +247,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     __shared__ uint32_t s_chosen[1024];
     __shared__ uint32_t s_red[2];
     __shared__ int s_nvalid;
+    __shared__ float s_bound;
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
     const int d = D.d;
@@ -244,11 +263,37 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
         if (w.cluster_counts[qi * D.C + c] > 0) atomicAdd(&s_nvalid, 1);
     __syncthreads();
     const bool all_c = s_nvalid <= Pc;
+    // With the tensor-core estimates, only clusters whose lower bound is below the n_list-th
+    // smallest upper bound can be in the exact top n_list; only those get exact distances.
+    const bool prune_c = !all_c && w.S != nullptr;
+    if (prune_c) {
+        for (int c = t; c < sort_n1; c += blockDim.x) {
+            uint64_t key = ~0ull;
+            if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
+                float lo, hi;
+                approx_band(D, w, qi, c, &lo, &hi);
+                key = ((uint64_t)float_key(hi) << 32) | (uint32_t)c;
+            }
+            s_keys[c] = key;
+        }
+        __syncthreads();
+        block_bitonic_sort(s_keys, sort_n1);
+        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Pc - 1] >> 32));
+        __syncthreads();
+    }
     for (int c = t; c < sort_n1; c += blockDim.x) {
         uint64_t key = ~0ull;
         if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
-            const uint32_t dk = all_c ? 0u : float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d));
-            key = ((uint64_t)dk << 32) | (uint32_t)c;
+            bool cand = true;
+            if (prune_c) {
+                float lo, hi;
+                approx_band(D, w, qi, c, &lo, &hi);
+                cand = lo <= s_bound;
+            }
+            if (cand) {
+                const uint32_t dk = all_c ? 0u : float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d));
+                key = ((uint64_t)dk << 32) | (uint32_t)c;
+            }
         }
         s_keys[c] = key;
     }
@@ -271,6 +316,27 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     }
     __syncthreads();
     const bool all_l = s_nvalid <= Ps;
+    const bool prune_l = !all_l && w.S != nullptr;
+    if (prune_l) {
+        for (int e = t; e < sort_n2; e += blockDim.x) {
+            uint64_t key = ~0ull;
+            const int i = e / Smax, jj = e % Smax;
+            if (i < npc) {
+                const uint32_t c = s_chosen[i];
+                const uint32_t j = D.cluster_off[c] + jj;
+                if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
+                    float lo, hi;
+                    approx_band(D, w, qi, D.C + j, &lo, &hi);
+                    key = ((uint64_t)float_key(hi) << 32) | j;
+                }
+            }
+            s_keys[e] = key;
+        }
+        __syncthreads();
+        block_bitonic_sort(s_keys, sort_n2);
+        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Ps - 1] >> 32));
+        __syncthreads();
+    }
     for (int e = t; e < sort_n2; e += blockDim.x) {
         uint64_t key = ~0ull;
         const int i = e / Smax, jj = e % Smax;
@@ -278,9 +344,17 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
             const uint32_t c = s_chosen[i];
             const uint32_t j = D.cluster_off[c] + jj;
             if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
-                const uint32_t dk =
-                    all_l ? 0u : float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d));
-                key = ((uint64_t)dk << 32) | j;
+                bool cand = true;
+                if (prune_l) {
+                    float lo, hi;
+                    approx_band(D, w, qi, D.C + j, &lo, &hi);
+                    cand = lo <= s_bound;
+                }
+                if (cand) {
+                    const uint32_t dk =
+                        all_l ? 0u : float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d));
+                    key = ((uint64_t)dk << 32) | j;
+                }
             }
         }
         s_keys[e] = key;
@@ -1122,6 +1196,11 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.cand_count = (uint32_t*)take("cand_count", q * 4);
     w.cand_pool = (uint32_t*)take("cand_pool", q * kcand * 4);
     w.kcand = kcand;
+    w.ldS = C + L;
+    w.S = (float*)take("gemm_s", q * (C + L) * 4);
+    w.qnorm = (float*)take("qnorm", q * 4);
+    w.qbf = take("qbf", q * idx->dev.d * 2);
+    w.gemm_err = (int*)take("gemm_err", 16);
     w.dist = static_cast<float*>(idx->dist_buf.ptr);
     if (!base) idx->work.bytes = std::max(idx->work.bytes, off);  // size probe
     return w;
@@ -1263,6 +1342,18 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     HDG_REQUIRE(sm_co <= 200 * 1024, HDG_ERR_UNSUPPORTED, "coarse selection does not fit shared memory");
     if (sm_co > 48 * 1024)
         CK(cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co));
+    // tensor-core estimates of every query-centroid dot product, used to prune the exact
+    // ranking when n_list or sub_lists leaves part of the candidates out (COARSE_BF16=1)
+    const bool use_gemm = P.coarse_bf16 != 0 && D.d % 8 == 0 && (Pc < (int)D.C || Ps < Pc * (int)D.S_max);
+    if (use_gemm) {
+        CK(cudaMemsetAsync(w.gemm_err, 0, sizeof(int), st));
+        rows_to_bf16(d_queries, q, (int)D.d, w.qbf, w.qnorm, st);
+        umma_dot(w.qbf, q, D.centers_bf16, D.C, (int)D.d, w.S, w.ldS, w.gemm_err, st);
+        umma_dot(w.qbf, q, D.sub_centers_bf16, D.n_lists, (int)D.d, w.S + D.C, w.ldS, w.gemm_err, st);
+        tm.mark("coarse_gemm");
+    } else {
+        w.S = nullptr;
+    }
     k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, d_queries, Pc, Ps, sort_n1, sort_n2, w);
     CK_LAUNCH();
     tm.mark("coarse");
@@ -1271,8 +1362,11 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     k_batch<<<1, 1024, 0, st>>>(q, w);
     CK_LAUNCH();
     uint64_t sc[4] = {0, 0, 0, 0};
+    int gemm_err = 0;
     CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+    if (use_gemm) CK(cudaMemcpyAsync(&gemm_err, w.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    HDG_REQUIRE(gemm_err == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
     const uint64_t coarse = sc[0], real = sc[1], max_row = sc[2];
     if (idx->dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
         idx->dist_buf.reset();

@@ -184,6 +184,14 @@ hdg_status hdg_label_mask(const float* d_ranges, const float* d_labels, uint32_t
 /* filters [q x 2l] f32 from the query labels and a filter spec. */
 hdg_status hdg_recover_filters(const hdg_filter_spec* spec, const float* d_query_labels,
                                uint64_t n_queries, float* d_ranges, void* stream);
+/* out[r][c] = sum_k a[r][k] * b[c][k] for bf16 a [rows x d] and b [cols x d] (row-major,
+ * d % 8 == 0), FP32 accumulation on the tcgen05 tensor cores; out has row stride ldo.
+ * The query-by-centroid contraction of the coarse assignment (the dot products inside
+ * ::refine, src/core/refine.cu:36-75, before its select_k).  Returns HDG_ERR_TIMEOUT if a
+ * tensor-core wait expired. */
+hdg_status hdg_bf16_gemm(const void* d_a, uint64_t rows, const void* d_b, uint64_t cols, uint32_t d,
+                         float* d_out, uint64_t ldo, void* stream);
+
 /* Allocation-free variant of hdg_recover_filters -- no counterpart in the reference.
  * For callers that must not allocate device memory while they run: a host application
  * whose own allocator owns the GPU's memory, or a serving loop that cannot afford the
