@@ -41,14 +41,15 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
-def workload(name: str, scale: float):
+def workload(name: str, scale: float, n_queries: int = 0):
     from hdgrid_b200 import datasets
     if name == "config1":
-        return datasets.config1(scale=scale, break_down=1)
+        return datasets.config1(scale=scale, n_queries=n_queries or 1000, break_down=1)
     if name == "config2":
-        return datasets.config2(scale=scale, n_queries=max(1000, int(10_000 * min(1.0, scale * 4))), break_down=1)
+        nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
+        return datasets.config2(scale=scale, n_queries=nq, break_down=1)
     if name == "config4":
-        return datasets.config4(scale=scale, n_queries=max(2000, int(100_000 * scale)), break_down=1)
+        return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1)
     raise SystemExit(f"unknown config {name}")
 
 
@@ -150,7 +151,7 @@ def run_reference(args):
     import hdgrid_b200 as hg
     import oracle
     from tests.helpers import build_gpu
-    ws = workload(args.config, args.scale)
+    ws = workload(args.config, args.scale, args.queries)
     idx, base, _ = build_gpu(ws, "cuda:0")
     d = tempfile.mkdtemp(prefix="hdg_ref_")
     path = os.path.join(d, "index.hdg")
@@ -198,7 +199,7 @@ def run_hdgrid(args):
     rank, world, local = dist_setup(args)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    ws = workload(args.config, args.scale)
+    ws = workload(args.config, args.scale, args.queries)
     k = ws["k"]
     idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
     base = torch.from_numpy(ws["base"]).to(dev)
@@ -308,6 +309,7 @@ def main():
     ap.add_argument("--impl", default="hdgrid", choices=["hdgrid", "reference"])
     ap.add_argument("--config", default="config2")
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--queries", type=int, default=0, help="query batch size (0 = the workload's own)")
     ap.add_argument("--cpu-sample", type=int, default=100)
     ap.add_argument("--ref-sample", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -24,6 +24,7 @@ _PKG = Path(__file__).resolve().parent
 _LIB_PATH = _PKG / "libhdgrid.so"
 
 HDG_OK = 0
+HDG_ERR_INVALID_ARG = 1
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "IO", 3: "CUDA", 4: "OOM", 5: "TIMEOUT",
                 6: "UNSUPPORTED", 7: "STATE"}
 MAX_DIMS = 8
@@ -77,6 +78,7 @@ def _load() -> C.CDLL:
         "hdg_build": [vp, vp, u64, u32, vp, u32, vp],
         "hdg_reserve": [vp, u64],
         "hdg_query": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp],
+        "hdg_query_ex": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp],
         "hdg_debug_fetch": [vp, C.c_char_p, vp, C.c_size_t, C.POINTER(C.c_size_t)],
         "hdg_get_info": [vp, C.POINTER(hdg_index_info)],
         "hdg_save": [vp, C.c_char_p],
@@ -270,6 +272,31 @@ class SuperGridIndex:
         k = dist.shape[1]
         _check(LIB.hdg_query(self._h, _ptr(q), q.shape[0], _ptr(ql), ql.shape[1],
                              _ptr(ds) if ds is not None else None, k, _ptr(dist), _ptr(ids), _stream_ptr(stream)))
+
+    def query_ex(self, query_in: query_input_t, query_out: query_output_t, k=None, n_probe=None,
+                 schedule=None, stream=None) -> None:
+        """Query with per-query parameters: ``k`` and ``n_probe`` CUDA uint32 tensors and
+        ``schedule`` a CUDA uint8 tensor of q entries each (None = the batch value).  The
+        output width is the largest k; slots past a query's own k hold id 2**64-1 and +inf."""
+        q, ql, ds = query_in.queries, query_in.query_labels, query_in.dataset
+        _require_cuda_f32(q, 2)
+        _require_cuda_f32(ql, 2)
+        dist, ids = query_out.distances, query_out.neighbors
+        nq = q.shape[0]
+
+        def arr(t, dtype):
+            if t is None:
+                return None
+            import torch
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()
+                    and t.numel() == nq):
+                raise HDGError(HDG_ERR_INVALID_ARG, f"per-query array must be a contiguous CUDA {dtype} of {nq}")
+            return _ptr(t)
+
+        import torch
+        _check(LIB.hdg_query_ex(self._h, _ptr(q), nq, _ptr(ql), ql.shape[1], _ptr(ds) if ds is not None else None,
+                                dist.shape[1], arr(k, torch.uint32), arr(n_probe, torch.uint32),
+                                arr(schedule, torch.uint8), _ptr(dist), _ptr(ids), _stream_ptr(stream)))
 
     def save(self, path: str) -> None:
         _check(LIB.hdg_save(self._h, str(path).encode()))

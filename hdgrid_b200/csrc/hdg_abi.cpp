@@ -194,6 +194,17 @@ hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q, const
     });
 }
 
+hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q, const float* d_query_labels,
+                        uint32_t label_cols, const float* d_data, uint32_t k_max, const uint32_t* d_k,
+                        const uint32_t* d_nprobe, const uint8_t* d_schedule, float* d_dist, uint64_t* d_ids,
+                        void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        run_query(index, d_queries, q, d_query_labels, label_cols, d_data, k_max, d_dist, d_ids,
+                  static_cast<cudaStream_t>(stream), d_k, d_nprobe, d_schedule);
+    });
+}
+
 int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap) {
     if (!index || !out) return 0;
     const int n = std::min(cap, 8);

@@ -245,6 +245,15 @@ __global__ void k_scan_axis(uint32_t* __restrict__ prefix, uint64_t n_lines, uin
     }
 }
 
+// codes [n][chunks] (16-byte chunks, row-major) -> [chunks][n]: chunk j of point p at j*n + p
+__global__ void k_interleave_codes(const uint4* __restrict__ rows, uint64_t n, uint32_t chunks,
+                                   uint4* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * chunks) return;
+    const uint64_t j = i / n, p = i - j * n;
+    out[i] = rows[p * chunks + j];
+}
+
 __global__ void k_gather_codes_labels(const uint8_t* __restrict__ codes_by_id, int M_pad,
                                       const float* __restrict__ labels_by_id, int l,
                                       const uint32_t* __restrict__ ids, uint64_t n,
@@ -671,7 +680,19 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.list_off = (const uint32_t*)up(o_lo, H.list_off.data(), H.list_off.size() * 4);
     D.zcodes = (const uint64_t*)up(o_z, H.zcodes.data(), H.zcodes.size() * 8);
     D.ids = (const uint32_t*)up(o_id, H.ids.data(), H.ids.size() * 4);
-    D.codes = (const uint8_t*)up(o_code, H.codes.data(), H.codes.size());
+    {
+        // pool-ordered rows -> 16-byte chunk planes (the scan's coalesced layout)
+        DevMem<uint8_t> rows(std::max<size_t>(H.codes.size(), 16));
+        if (!H.codes.empty()) {
+            CK(cudaMemcpyAsync(rows.p, H.codes.data(), H.codes.size(), cudaMemcpyHostToDevice, st));
+            const uint64_t chunks = H.M_pad / 16;
+            k_interleave_codes<<<blocks_for(H.n * chunks, 256), 256, 0, st>>>(
+                reinterpret_cast<const uint4*>(rows.p), H.n, (uint32_t)chunks, reinterpret_cast<uint4*>(base + o_code));
+            CK_LAUNCH();
+        }
+        CK(cudaStreamSynchronize(st));
+        D.codes = (const uint8_t*)(base + o_code);
+    }
     D.labels = (const float*)up(o_lab, H.labels.data(), H.labels.size() * 4);
     D.pq_centers = (const float*)up(o_pq, H.pq_centers.data(), H.pq_centers.size() * 4);
     D.prefix = (const uint32_t*)up(o_pre, H.prefix.data(), H.prefix.size() * 4);

@@ -9,7 +9,11 @@
 //   list_off     u32 [L + 1]            pool range of each list (zorder_array_offsets/lengthes, :70-71)
 //   zcodes       u64 [N]                Morton code of every point, sorted inside each list (:69)
 //   ids          u32 [N]                original point id in pool order (zorder_node_arrays, :68)
-//   codes        u8  [N x M_pad]        PQ codes in pool order, one 16-byte-aligned row per point
+//   codes        u8  [M_pad/16][N][16]  PQ codes in pool order as 16-byte chunk planes: bytes
+//                                       16j..16j+15 of point p at (j*N + p)*16, so the lanes of a
+//                                       warp scanning consecutive pool positions load one
+//                                       contiguous 512-byte span per chunk (the saved file and
+//                                       HostIndex keep the row-major [N x M_pad] form)
 //   labels       f32 [N x l]            labels in pool order (read by the fused predicate)
 //   pq_centers   f32 [M x 256 x pq_len] PQ codebooks (pq::index_data_t::centers, product-quantization.cuh:9)
 //   prefix       u32 [cells x L]        inclusive multi-dim prefix counts per list, cell-major,

@@ -42,7 +42,8 @@ FilterDev filter_dev(const hdg_index* idx);
 void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand);
 void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
-               cudaStream_t st);
+               cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,
+               const uint8_t* d_sched = nullptr);
 void save_index(const hdg_index* idx, const std::string& path);
 hdg_index* load_index(const std::string& path);
 

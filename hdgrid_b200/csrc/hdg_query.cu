@@ -66,7 +66,46 @@ struct Workspace {
     float* qnorm;            // [q] squared query norms
     void* qbf;               // [q x d] bf16 queries
     int* gemm_err;           // tensor-core wait expiry flag
+    // per-query parameters (nullptr: the batch-wide value)
+    const uint32_t* qk;      // [q] k of each query (<= k_max)
+    const uint32_t* qps;     // [q] lists probed (<= sub_lists)
+    const uint8_t* qsched;   // [q] 0 = the index's reference schedule, 1 = predicate-first + re-rank
+    uint32_t k_max;          // output row stride
+    int mode;                // batch schedule: 0 pre-filter (exps0 <= 1), 1 post-filter, 2 single dim
+    uint32_t exps0;
+    float beta;              // batch-wide coarse / exact candidate ratio (post-filter budget)
+    uint64_t max_row;        // largest per-query candidate count of the batch
 };
+
+enum ScanMode { kPre = 0, kPost = 1, kL1 = 2 };
+
+__device__ __forceinline__ uint32_t q_k(const Workspace& w, uint64_t qi) {
+    return w.qk ? max(1u, min(w.qk[qi], w.k_max)) : w.k_max;
+}
+__device__ __forceinline__ int q_sched(const Workspace& w, uint64_t qi) { return w.qsched ? (int)w.qsched[qi] : 0; }
+// true when query qi evaluates the label predicate inside the scan
+__device__ __forceinline__ bool q_prefilter(const Workspace& w, uint64_t qi) {
+    return w.mode == kPre || q_sched(w, qi) == 1;
+}
+// Candidate budget of query qi: k for the reference pre-filter schedule (exps0 <= 1),
+// exps0 * k for the single-dim schedule and the predicate-first schedule, and the
+// reference's min(exps0 * k * beta, max_row_len) for the post-filter schedule
+// (Super-Grid-IVF_PQ.cu:1219-1222); capped by kMaxCand.
+__device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) {
+    const uint32_t k = q_k(w, qi);
+    if (w.mode == kPre) return k;
+    uint64_t K;
+    if (w.mode == kL1 || q_sched(w, qi) == 1) {
+        K = (uint64_t)w.exps0 * k;
+    } else if (!(w.beta < INFINITY)) {
+        K = w.max_row;
+    } else {
+        const float want = (float)((uint64_t)w.exps0 * k) * w.beta;
+        K = want >= 1.8e19f ? ~0ull : (uint64_t)want;
+        K = min(K, w.max_row);
+    }
+    return (uint32_t)max((uint64_t)1, min(K, (uint64_t)kMaxCand));
+}
 
 // Exclusive block-wide scan of n u32 values in shared memory (in place).  All threads.
 __device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_t* s_warp) {
@@ -315,7 +354,9 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
         if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) atomicAdd(&s_nvalid, 1);
     }
     __syncthreads();
-    const bool all_l = s_nvalid <= Ps;
+    // lists probed by this query: sub_lists, or the query's own n_probe when given
+    const int Psq = w.qps ? max(1, min(Ps, (int)w.qps[qi])) : Ps;
+    const bool all_l = s_nvalid <= Psq;
     const bool prune_l = !all_l && w.S != nullptr;
     if (prune_l) {
         for (int e = t; e < sort_n2; e += blockDim.x) {
@@ -334,7 +375,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
         }
         __syncthreads();
         block_bitonic_sort(s_keys, sort_n2);
-        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Ps - 1] >> 32));
+        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Psq - 1] >> 32));
         __syncthreads();
     }
     for (int e = t; e < sort_n2; e += blockDim.x) {
@@ -361,7 +402,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     }
     __syncthreads();
     block_bitonic_sort(s_keys, sort_n2);
-    const int nps = min(Ps, s_nvalid);
+    const int nps = min(Psq, s_nvalid);
     // the probed lists in list-id (= pool) order, so candidate positions follow pool order
     const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
     for (int i = t; i < sort_n3; i += blockDim.x) s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
@@ -643,6 +684,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
         const uint32_t e1 = min(total, e0 + kChunk);
         float* dst = w.dist + w.qoff[qq];
+        const bool preq = pre || q_prefilter(w, qq);
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
         int r[CPT];
 #pragma unroll
@@ -656,6 +698,8 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
             }
             r[u] = lo;
         }
+        const uint4* planes = reinterpret_cast<const uint4*>(D.codes);
+        const uint64_t n_pts = D.n;
         for (uint32_t eb = e0 + t; eb < e1; eb += NT * CPT) {
             const uint4* cp[CPT];
             bool live[CPT];
@@ -670,7 +714,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
                     while (s_pre[r[u] + 1] <= e) r[u]++;
                     const uint32_t pool = s_start[r[u]] + (e - s_pre[r[u]]);
                     bool pass = true;
-                    if (pre) {
+                    if (preq) {
                         const float* lab = D.labels + (uint64_t)pool * lbl;
                         for (int i = 0; i < lbl; i++) {
                             const float v = lab[i];
@@ -682,14 +726,14 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
                         row = pool;
                     }
                 }
-                cp[u] = reinterpret_cast<const uint4*>(D.codes + (uint64_t)row * D.M_pad);
+                cp[u] = planes + row;  // chunk j of this point at cp[u][j * n_pts]
             }
 #pragma unroll
             for (int g = 0; g < G; g++) {
                 uint32_t x[CPT][8];
 #pragma unroll
                 for (int u = 0; u < CPT; u++) {
-                    const uint4 a = __ldg(cp[u] + 2 * g), b = __ldg(cp[u] + 2 * g + 1);
+                    const uint4 a = __ldg(cp[u] + (2 * g) * n_pts), b = __ldg(cp[u] + (2 * g + 1) * n_pts);
                     uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
                     rotate_words(wv, R);
 #pragma unroll
@@ -776,6 +820,7 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
         const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
         const uint32_t e1 = min(total, e0 + kChunk);
         float* dst = w.dist + w.qoff[qq];
+        const bool preq = pre || q_prefilter(w, qq);
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
         for (uint32_t e = e0 + t; e < e1; e += blockDim.x) {
             int lo = 0, hi = Ps - 1;
@@ -786,7 +831,7 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
             }
             const uint32_t pool = s_start[lo] + (e - s_pre[lo]);
             bool pass = true;
-            if (pre) {
+            if (preq) {
                 const float* lab = D.labels + (uint64_t)pool * lbl;
                 for (int i = 0; i < lbl; i++) {
                     const float v = lab[i];
@@ -796,8 +841,16 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
             float sum = INFINITY;
             if (pass) {
                 sum = 0.f;
-                const uint8_t* cp = D.codes + (uint64_t)pool * D.M_pad;
-                for (int m = 0; m < M; m++) sum += s_lut[(m >> 5) * (kCodes * 32) + cp[m] * 32 + (m & 31)];
+                const uint4* cp = reinterpret_cast<const uint4*>(D.codes) + pool;
+                for (int j = 0; j * 16 < M; j++) {
+                    const uint4 v = __ldg(cp + (uint64_t)j * D.n);
+                    const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+                    for (int b = 0; b < 16 && j * 16 + b < M; b++) {
+                        const int m = j * 16 + b;
+                        const uint32_t c = (wv[b >> 2] >> (8 * (b & 3))) & 0xffu;
+                        sum += s_lut[(m >> 5) * (kCodes * 32) + c * 32 + (m & 31)];
+                    }
+                }
                 const uint32_t key = float_key(sum);
                 kmin = min(kmin, key);
                 kmax = max(kmax, key);
@@ -852,14 +905,16 @@ __device__ __forceinline__ uint32_t pos_to_pool(const uint32_t* s_pre, const uin
     return s_start[lo] + (e - s_pre[lo]);
 }
 
-__global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int K, int sorted_out, Workspace w,
+__global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int Kcap, int sorted_out, Workspace w,
                                                         float* __restrict__ out_dist,
                                                         uint64_t* __restrict__ out_ids, int k_out) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem);                   // [kBins]
     uint64_t* s_bbuf = reinterpret_cast<uint64_t*>(s_hist + kBins);         // [kBCap]
     uint64_t* s_sel = s_bbuf + kBCap;                                        // [sel_cap] (sorted mode)
-    const int sel_cap = sorted_out ? (int)next_pow2_dev((uint32_t)max(K, 2)) : 0;
+    const int sel_cap = sorted_out ? (int)next_pow2_dev((uint32_t)max(Kcap, 2)) : 0;
+    // this query's budget: its k for the sorted pre-filter output, else the candidate budget
+    const int K = sorted_out ? (int)q_k(w, blockIdx.x) : (int)q_budget(w, blockIdx.x);
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_sel + sel_cap);        // [Ps + 1]
     uint32_t* s_start = s_pre + Ps + 1;                                      // [Ps]
     __shared__ uint32_t s_warp[32];
@@ -1089,6 +1144,8 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
     }
     __syncthreads();
     const int nc = (int)w.cand_count[qi];
+    const int kq = (int)q_k(w, qi);
+    const bool pred_q = apply_pred && q_sched(w, qi) == 0;  // predicate-first queries already passed it
     for (int base = 0; base < nc; base += kThreads) {
         const int e = base + t;
         bool keep = false;
@@ -1096,7 +1153,7 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
         if (e < nc) {
             pool = w.cand_pool[qi * w.kcand + e];
             keep = pool != kInvalid;
-            if (keep && apply_pred) {
+            if (keep && pred_q) {
                 const float* lab = D.labels + (uint64_t)pool * lbl;
                 for (int i = 0; i < lbl; i++) {
                     const float v = lab[i];
@@ -1134,8 +1191,8 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
             __syncthreads();
             block_bitonic_sort(s_keys, cap);
             if (t == 0) {
-                s_cnt = min(c, k_out);
-                if (c >= k_out) s_th = s_keys[k_out - 1];
+                s_cnt = min(c, kq);
+                if (c >= kq) s_th = s_keys[kq - 1];
             }
             __syncthreads();
         }
@@ -1146,7 +1203,7 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
     __syncthreads();
     block_bitonic_sort(s_keys, cap);
     for (int i = t; i < k_out; i += blockDim.x) {
-        if (i < c) {
+        if (i < min(c, kq)) {
             const uint64_t key = s_keys[i];
             out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
             out_ids[qi * k_out + i] = (uint32_t)key;
@@ -1301,11 +1358,9 @@ int sm_count() {
 }
 }  // namespace
 
-enum ScanMode { kPre = 0, kPost = 1, kL1 = 2 };
-
 void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
-               cudaStream_t st) {
+               cudaStream_t st, const uint32_t* d_k, const uint32_t* d_nprobe, const uint8_t* d_sched) {
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
     HDG_REQUIRE(q > 0 && q < (1ull << 31), HDG_ERR_INVALID_ARG, "query count out of range");
     HDG_REQUIRE(d_queries && d_query_labels && d_dist && d_ids, HDG_ERR_INVALID_ARG, "null pointer");
@@ -1323,9 +1378,17 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     const uint64_t exps0 = P.exps0;
     const int mode = exps0 <= 1 ? kPre : (l > 1 ? kPost : kL1);
     HDG_REQUIRE(mode == kPre || d_data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
+    HDG_REQUIRE(mode != kPre || !d_sched, HDG_ERR_INVALID_ARG,
+                "per-query schedules need exps0 > 1 (the pre-filter schedule has no re-rank)");
     const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
     if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) reserve_workspace(idx, q, kcand);
     Workspace w = carve(idx, q, kcand, true);
+    w.qk = d_k;
+    w.qps = d_nprobe;
+    w.qsched = d_sched;
+    w.k_max = k;
+    w.mode = mode;
+    w.exps0 = (uint32_t)std::min<uint64_t>(exps0, 1u << 20);
     const FilterDev f = filter_dev(idx);
     StageTimer tm(idx, st, P.break_down != 0);
 
@@ -1373,27 +1436,24 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         idx->dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
     }
     w.dist = static_cast<float*>(idx->dist_buf.ptr);
-    uint64_t K = k;
+    // beta = coarse / real (Super-Grid-IVF_PQ.cu:1219); budgets per query in q_budget
     float beta = 0.f;
+    if (mode == kPost) beta = real == 0 ? INFINITY : (float)coarse / (float)real;
+    w.beta = beta;
+    w.max_row = max_row;
+    uint64_t K = k;  // the budget of a query with the batch k and the reference schedule
     if (mode == kPost) {
-        // beta = coarse / real; n_cand = min(exps0*k*beta, max_row_len) (:1219-1222)
         if (real == 0) {
             K = max_row;
-            beta = INFINITY;
         } else {
-            beta = (float)coarse / (float)real;
             const float want = (float)(exps0 * (uint64_t)k) * beta;
-            const uint64_t nc = want >= 1.8e19f ? ~0ull : (uint64_t)want;
-            K = std::min<uint64_t>(nc, max_row);
+            K = std::min<uint64_t>(want >= 1.8e19f ? ~0ull : (uint64_t)want, max_row);
         }
     } else if (mode == kL1) {
         K = exps0 * k;
     }
     idx->last_ncand = K;
-    if (mode != kPre) {
-        K = std::min<uint64_t>(K, (uint64_t)kMaxCand);
-        if (K == 0) K = 1;
-    }
+    if (mode != kPre) K = std::max<uint64_t>(1, std::min<uint64_t>(K, (uint64_t)kMaxCand));
     idx->last_beta = beta;
     idx->last_q = q;
     {
@@ -1458,9 +1518,9 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
 
     const int sorted_out = mode == kPre ? 1 : 0;
     const size_t sm_sel = sizeof(uint32_t) * kBins + sizeof(uint64_t) * kBCap +
-                          (sorted_out ? sizeof(uint64_t) * next_pow2((uint32_t)std::max<uint64_t>(K, 2)) : 0) + sm_tab + 16;
+                          (sorted_out ? sizeof(uint64_t) * next_pow2(std::max<uint32_t>(k, 2)) : 0) + sm_tab + 16;
     CK(cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sel));
-    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)K, sorted_out, w, d_dist, d_ids, (int)k);
+    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)k, sorted_out, w, d_dist, d_ids, (int)k);
     CK_LAUNCH();
     tm.mark("select");
     if (mode != kPre) {

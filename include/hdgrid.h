@@ -131,6 +131,20 @@ hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q,
                      const float* d_query_labels, uint32_t label_cols, const float* d_data,
                      uint32_t k, float* d_dist, uint64_t* d_ids, void* stream);
 
+/* hdg_query with per-query parameters, each an optional device array of q entries (NULL =
+ * the uniform value).  No reference counterpart: super_grid::index::query
+ * (Super-Grid-IVF_PQ.cu:985-1249) takes one k and one probe count for the whole batch.
+ *   d_k        result count of each query, clamped to [1, k_max]; rows keep stride k_max and
+ *              the slots past a query's k hold id UINT64_MAX and distance +inf;
+ *   d_nprobe   sub-lists probed per query, clamped to [1, sub_lists];
+ *   d_schedule 0 = the index's schedule (Super-Grid-IVF_PQ.cu:1151-1241), 1 = predicate-first
+ *              scan (label test fused into the ADC pass) with a budget of exps0*k and an exact
+ *              re-rank; needs exps0 > 1. */
+hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q,
+                        const float* d_query_labels, uint32_t label_cols, const float* d_data,
+                        uint32_t k_max, const uint32_t* d_k, const uint32_t* d_nprobe,
+                        const uint8_t* d_schedule, float* d_dist, uint64_t* d_ids, void* stream);
+
 /* Scalars of the last hdg_query: out[0] queries, [1] candidate budget n_cand as the
  * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget actually used (capped by the
  * shared-memory top-K), [3] sum of Morton candidate-range sizes, [4] sum of exact filtered

@@ -38,6 +38,9 @@ def _load() -> C.CDLL:
     lib.ora_check_layout.argtypes = [vp]
     lib.ora_query.restype = C.c_int
     lib.ora_query.argtypes = [vp, vp, C.c_uint64, vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, C.c_int, C.c_int]
+    lib.ora_query_ex.restype = C.c_int
+    lib.ora_query_ex.argtypes = [vp, vp, C.c_uint64, vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, vp, vp, vp,
+                                 C.c_int, C.c_int]
     lib.ora_bruteforce_f64.argtypes = [vp, C.c_uint64, C.c_uint32, vp, C.c_uint32, vp, C.c_uint64, vp, C.c_uint32,
                                        vp, vp, C.c_int]
     lib.ora_pq_lut.argtypes = [vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp]
@@ -189,8 +192,14 @@ class OracleIndex:
     def check_layout(self) -> int:
         return int(LIB.ora_check_layout(self._h))
 
-    def query(self, queries, query_labels, data, k, threads=0, trace=True, adc_rotated=False):
+    def query(self, queries, query_labels, data, k, threads=0, trace=True, adc_rotated=False,
+              qk=None, n_probe=None, schedule=None):
+        """The reference query; qk / n_probe (uint32) and schedule (uint8) are the optional
+        per-query arrays of hdg_query_ex."""
         n_list, sub_lists = self.n_list, self.sub_lists
+        qk = None if qk is None else _c(qk, np.uint32)
+        n_probe = None if n_probe is None else _c(n_probe, np.uint32)
+        schedule = None if schedule is None else _c(schedule, np.uint8)
         queries = _c(queries, np.float32)
         ql = _c(query_labels, np.float32)
         data = _c(data, np.float32)
@@ -207,8 +216,9 @@ class OracleIndex:
                      range_start=np.zeros((q, sub_lists), np.uint32), range_len=np.zeros((q, sub_lists), np.uint32),
                      scalars=np.zeros(4, np.float64))
             tr = _Trace(*(t[n].ctypes.data for n, _ in _Trace._fields_))
-        rc = LIB.ora_query(self._h, _p(queries), q, _p(ql), ql.shape[1], _p(data), k, _p(dist), _p(ids),
-                           C.byref(tr) if tr is not None else None, threads, 1 if adc_rotated else 0)
+        opt = [None if a is None else _p(a) for a in (qk, n_probe, schedule)]
+        rc = LIB.ora_query_ex(self._h, _p(queries), q, _p(ql), ql.shape[1], _p(data), k, *opt, _p(dist), _p(ids),
+                              C.byref(tr) if tr is not None else None, threads, 1 if adc_rotated else 0)
         if rc != 0:
             raise RuntimeError(LIB.ora_last_error().decode())
         return dist, ids, t

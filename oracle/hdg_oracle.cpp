@@ -507,9 +507,14 @@ struct OraTrace {
 
 // super_grid::index::query (Super-Grid-IVF_PQ.cu:985-1249) on the CPU.
 // Outputs dist [q x k] f32 and ids [q x k] u64 (ascending; +inf / UINT64_MAX when empty).
-int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, uint32_t label_cols,
-              const float* data, uint32_t k, float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads,
-              int adc_mode) {
+// Optional per-query arrays (NULL = uniform), the semantics of hdg_query_ex: qk result
+// count clamped to [1, k] (rows keep stride k); qps probed sub-lists clamped to
+// [1, sub_lists]; qsched 1 = label predicate during the ADC pass, budget exps0*k_q, exact
+// re-rank without a second predicate.  These have no reference counterpart; with all three
+// NULL this is the reference's query.
+int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels, uint32_t label_cols,
+                 const float* data, uint32_t k, const uint32_t* qk, const uint32_t* qps, const uint8_t* qsched,
+                 float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads, int adc_mode) {
     const Index& ix = *static_cast<Index*>(h);
     const Grid& g = ix.g;
     const int l = (int)ix.l, d = (int)ix.d, M = (int)ix.M;
@@ -571,7 +576,8 @@ int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, u
                 if (lc[j]) sl.push_back({ref_l2(queries + qi * d, &ix.sub_centers[(uint64_t)j * d], d), j});
         }
         std::sort(sl.begin(), sl.end());
-        const int nps = std::min<int>(Ps, (int)sl.size());
+        const int psq = qps ? std::max(1, std::min(Ps, (int)qps[qi])) : Ps;
+        const int nps = std::min<int>(psq, (int)sl.size());
         // the chosen lists in list-id (= pool) order; RAFT select_k returns them unsorted
         std::sort(sl.begin(), sl.begin() + nps, [](const auto& a, const auto& b) { return a.second < b.second; });
         s.start.assign(Ps, 0);
@@ -628,6 +634,13 @@ int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, u
     } else if (mode == 2) {
         K = exps0 * k;
     }
+    // the same budget for a query's own k and schedule
+    auto budget = [&](uint32_t kq, bool sched1) -> uint64_t {
+        if (mode == 2 || sched1) return exps0 * (uint64_t)kq;
+        if (real == 0) return max_row;
+        const float want = (float)(exps0 * (uint64_t)kq) * (float)beta;
+        return std::min<uint64_t>(want >= 1.8e19f ? ~0ull : (uint64_t)want, max_row);
+    };
     if (tr && tr->scalars) {
         tr->scalars[0] = (double)K;
         tr->scalars[1] = beta;
@@ -675,35 +688,46 @@ int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, u
             }
             return sum;
         };
+        const uint32_t kq = qk ? std::max(1u, std::min(qk[qi], k)) : k;
+        const bool sched1 = mode != 0 && qsched && qsched[qi] == 1;
+        const bool pre = mode == 0 || sched1;
         std::vector<std::pair<float, uint32_t>> cand;
         uint32_t pos = 0;
         for (int r = 0; r < Ps; r++)
             for (uint32_t p = s.start[r]; p < s.start[r] + s.len[r]; p++, pos++) {
-                if (mode == 0 && !pred(p)) continue;  // query_prefilter (prefiltering.cu:36-51)
+                if (pre && !pred(p)) continue;  // query_prefilter (prefiltering.cu:36-51)
                 cand.push_back({adc(p, pos), p});
             }
         std::sort(cand.begin(), cand.end());
         if (mode == 0) {
             for (uint32_t j = 0; j < k; j++) {
-                out_dist[qi * k + j] = j < cand.size() ? cand[j].first : INFINITY;
-                out_ids[qi * k + j] = j < cand.size() ? ix.ids[cand[j].second] : ~0ull;
+                out_dist[qi * k + j] = j < std::min<size_t>(cand.size(), kq) ? cand[j].first : INFINITY;
+                out_ids[qi * k + j] = j < std::min<size_t>(cand.size(), kq) ? ix.ids[cand[j].second] : ~0ull;
             }
             continue;
         }
-        if (cand.size() > K) cand.resize(K);
+        const uint64_t Kq = (qk || qsched) ? budget(kq, sched1) : K;
+        if (cand.size() > Kq) cand.resize(Kq);
         std::vector<std::pair<float, uint32_t>> fin;
         for (const auto& c : cand) {
-            if (mode == 1 && !pred(c.second)) continue;  // post-filter predicate (:1227-1236)
+            if (mode == 1 && !sched1 && !pred(c.second)) continue;  // post-filter predicate (:1227-1236)
             const uint32_t id = ix.ids[c.second];
             fin.push_back({ref_l2(qv, data + (uint64_t)id * d, d), id});
         }
         std::sort(fin.begin(), fin.end());
         for (uint32_t j = 0; j < k; j++) {
-            out_dist[qi * k + j] = j < fin.size() ? fin[j].first : INFINITY;
-            out_ids[qi * k + j] = j < fin.size() ? fin[j].second : ~0ull;
+            out_dist[qi * k + j] = j < std::min<size_t>(fin.size(), kq) ? fin[j].first : INFINITY;
+            out_ids[qi * k + j] = j < std::min<size_t>(fin.size(), kq) ? fin[j].second : ~0ull;
         }
     }
     return 0;
+}
+
+int ora_query(void* h, const float* queries, uint64_t q, const float* qlabels, uint32_t label_cols,
+              const float* data, uint32_t k, float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads,
+              int adc_mode) {
+    return ora_query_ex(h, queries, q, qlabels, label_cols, data, k, nullptr, nullptr, nullptr, out_dist, out_ids,
+                        tr, threads, adc_mode);
 }
 
 }  // extern "C"
