@@ -48,6 +48,9 @@ def workload(name: str, scale: float, n_queries: int = 0):
     if name == "config2":
         nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
         return datasets.config2(scale=scale, n_queries=nq, break_down=1)
+    if name == "config3":
+        nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
+        return datasets.config3(scale=scale, n_queries=nq, break_down=1)
     if name == "config4":
         return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1)
     raise SystemExit(f"unknown config {name}")
@@ -193,6 +196,36 @@ def workload_config(ws, args):
             "l2_flush": "256 MiB buffer written between timed steps", "parallelism": f"replicas{args.gpus}"}
 
 
+def max_relative_error(ws, dist, ids, n_sample):
+    """Largest |d - d64| / d64 over the returned ids of the first n_sample queries, d64 the
+    FP64 distance of the same id (the brute-force oracle's arithmetic)."""
+    inv = np.uint64(0xFFFFFFFFFFFFFFFF)
+    worst = 0.0
+    base = ws["base"]
+    for i in range(min(n_sample, ids.shape[0])):
+        ok = ids[i] != inv
+        if not ok.any():
+            continue
+        rows = base[ids[i][ok].astype(np.int64)].astype(np.float64)
+        d64 = ((rows - ws["queries"][i].astype(np.float64)) ** 2).sum(1)
+        rel = np.abs(dist[i][ok].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
+        worst = max(worst, float(rel.max()))
+    return worst
+
+
+def scan_traffic(ws, candidates):
+    """DRAM bytes of one k_scan_fast launch: the per-candidate figure of the committed ncu
+    summary for this workload (dram__bytes_read.sum + dram__bytes_write.sum over the
+    candidates of the captured launch) times this launch's candidates; None without one."""
+    f = ROOT / "profiles" / f"k_scan_fast_{ws['name']}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_candidate:"):
+            return float(line.split(":", 1)[1]) * candidates
+    return None
+
+
 def run_hdgrid(args):
     import torch
     import hdgrid_b200 as hg
@@ -230,7 +263,10 @@ def run_hdgrid(args):
         idx.query(qin, qout)
     torch.cuda.synchronize()
     from hdgrid_b200 import datasets
-    rec = datasets.recall(ids.cpu().numpy().view(np.uint64), gt_i.cpu().numpy().view(np.uint64))
+    ids_np = ids.cpu().numpy().view(np.uint64)
+    rec = datasets.recall(ids_np, gt_i.cpu().numpy().view(np.uint64))
+    launches_per_step = int(idx.last_query_stats()["launches"])
+    max_rel = max_relative_error(ws, dist.cpu().numpy(), ids_np, args.err_sample)
     cand = int(np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64).sum())
 
     barrier(world)
@@ -284,15 +320,17 @@ def run_hdgrid(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture, configs of the benchmark)",
         "config": workload_config(ws, args) | {"recall_at_k": rec, "build_s": round(t_build, 2),
-                                               "candidates_per_step": cand},
+                                               "candidates_per_step": cand,
+                                               "max_rel_dist_err_vs_fp64": max_rel},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_scan", "peak_kind": f"{peak_kind} hbm_gbs",
+                     "traffic": scan_traffic(ws, cand), "kernel": "k_scan_fast", "peak_kind": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg},
         "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4),
                 "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},
-        # prologue, coarse, batch, lut, scan, select (+ refine when exps0 > 1) per step
-        "gpu_launches": args.steps * (7 if p["exps0"] > 1 else 6),
+        # kernels the library launched per query (prologue, [coarse GEMM x3], coarse, batch,
+        # lut, scan, select, [refine]) times the timed steps
+        "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
         "stage_ms": idx.stage_times(),
     }
@@ -313,6 +351,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=100)
     ap.add_argument("--ref-sample", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--err-sample", type=int, default=200, help="queries checked against FP64 distances")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

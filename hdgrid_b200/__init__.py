@@ -311,11 +311,11 @@ class SuperGridIndex:
 
     def last_query_stats(self) -> dict:
         import struct
-        v = (C.c_uint64 * 8)()
-        LIB.hdg_last_query_stats(self._h, v, 8)
+        v = (C.c_uint64 * 10)()
+        LIB.hdg_last_query_stats(self._h, v, 10)
         return {"queries": v[0], "n_cand_ref": v[1], "n_cand_used": v[2], "coarse_total": v[3], "exact_total": v[4],
                 "max_row": v[5], "beta": struct.unpack("f", struct.pack("I", v[6] & 0xFFFFFFFF))[0],
-                "schedule": ["pre-filter", "post-filter", "single-dim"][v[7]]}
+                "schedule": ["pre-filter", "post-filter", "single-dim"][v[7]], "launches": v[8]}
 
     def stage_times(self) -> dict:
         ms = (C.c_float * 16)()

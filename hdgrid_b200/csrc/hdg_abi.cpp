@@ -207,7 +207,7 @@ hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q, co
 
 int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap) {
     if (!index || !out) return 0;
-    const int n = std::min(cap, 8);
+    const int n = std::min(cap, 10);
     for (int i = 0; i < n; i++) out[i] = index->last_stats[i];
     return n;
 }

@@ -116,6 +116,6 @@ struct hdg_index {
     std::vector<float> stage_ms;
     // last-query scalars (host copy)
     uint64_t last_q = 0, last_ncand = 0;
-    uint64_t last_stats[8] = {0};
+    uint64_t last_stats[10] = {0};
     float last_beta = 0.f;
 };

@@ -56,7 +56,8 @@ struct Workspace {
     uint32_t* mm;            // [q x 2] min / max finite distance key
     uint32_t* nfin;          // [q] finite distances (predicate passed)
     uint32_t* counter;       // [4] work counter
-    float* lut;              // [q x G x 256 x 32]
+    float* lut;              // [q x G x 256 x 32] f32, or __half when lut16
+    int lut16;               // LUT stored in FP16 (LUT_FP16=1); the scan sums in FP32
     uint32_t* cand_pool;     // [q x kcand]
     uint32_t* cand_count;    // [q]
     uint64_t kcand;
@@ -527,12 +528,20 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
 constexpr int kLutQ = 64;          // queries per k_lut block
 constexpr int kLutMaxPqLen = 6;    // staged codebook group fits shared memory up to this pq_len
 
+// one LUT entry, FP32 or rounded to FP16 (round to nearest even)
+__device__ __forceinline__ void store_lut(float* lut, int f16, uint64_t i, float v) {
+    if (f16)
+        reinterpret_cast<__half*>(lut)[i] = __float2half_rn(v);
+    else
+        lut[i] = v;
+}
+
 // Block = (64 queries, one group of 32 subspaces).  The group's codebook is staged once in
 // shared memory as [c*pq_len + t][33] (conflict-free stores from coalesced global reads and
 // conflict-free lane reads); lane = subspace column j, so a warp stores one contiguous
 // 128-byte LUT row per codeword.
 __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict__ queries, uint64_t q, int G,
-                                             float* __restrict__ lut) {
+                                             float* __restrict__ lut, int f16) {
     extern __shared__ float smem_lut[];
     const int g = blockIdx.y, pq_len = D.pq_len, d = D.d, M = D.M;
     float* s_cb = smem_lut;                          // [(c * pq_len + t) * 33 + j]
@@ -554,7 +563,7 @@ __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict
 #pragma unroll
         for (int t = 0; t < kLutMaxPqLen; t++)
             qv[t] = (real && t < pq_len) ? queries[qi * d + (uint64_t)m * pq_len + t] : 0.f;
-        float* out = lut + (qi * G + g) * (kCodes * 32);
+        const uint64_t row0 = (qi * G + g) * (kCodes * 32);
         for (int c = 0; c < kCodes; c++) {
             float s = 0.f;
 #pragma unroll
@@ -564,14 +573,14 @@ __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict
                     s = fmaf(df, df, s);
                 }
             }
-            out[c * 32 + lane] = real ? s : 0.f;
+            store_lut(lut, f16, row0 + c * 32 + lane, real ? s : 0.f);
         }
     }
 }
 
 // Fallback for long subspaces: one query per block, thread = codeword, transposed store.
 __global__ void __launch_bounds__(256) k_lut_plain(IndexDev D, const float* __restrict__ queries, int G,
-                                                   float* __restrict__ lut) {
+                                                   float* __restrict__ lut, int f16) {
     extern __shared__ float s_q[];     // [d]
     __shared__ float s_t[kCodes][33];  // [c][j]
     const uint64_t qi = blockIdx.x;
@@ -591,8 +600,8 @@ __global__ void __launch_bounds__(256) k_lut_plain(IndexDev D, const float* __re
         s_t[c][j] = s;
     }
     __syncthreads();
-    float* out = lut + (qi * G + g) * (kCodes * 32);
-    for (int e = threadIdx.x; e < kCodes * 32; e += blockDim.x) out[e] = s_t[e >> 5][e & 31];
+    const uint64_t row0 = (qi * G + g) * (kCodes * 32);
+    for (int e = threadIdx.x; e < kCodes * 32; e += blockDim.x) store_lut(lut, f16, row0 + e, s_t[e >> 5][e & 31]);
 }
 
 // ------------------------------------------------------------------------------------
@@ -603,6 +612,14 @@ __global__ void __launch_bounds__(256) k_lut_plain(IndexDev D, const float* __re
 // the group left by r, so at step s it looks up subspace (r + s) mod 32 at column r + s:
 // the 32 lanes of a warp read 32 different banks, the column offset 4*s is an immediate,
 // and no wrap-around arithmetic is needed.
+
+// (a0, a1) += (b0, b1) as one packed FP32x2 add (round to nearest, like two FADDs)
+__device__ __forceinline__ void add_f32x2(float& a0, float& a1, float b0, float b1) {
+    asm("{\n\t.reg .b64 ra, rb;\n\tmov.b64 ra, {%0, %1};\n\tmov.b64 rb, {%2, %3};\n\t"
+        "add.rn.f32x2 ra, ra, rb;\n\tmov.b64 {%0, %1}, ra;\n\t}"
+        : "+f"(a0), "+f"(a1)
+        : "f"(b0), "f"(b1));
+}
 
 // rotate 8 words left by R words (out[i] = in[(i + R) & 7]) with selects only
 __device__ __forceinline__ void rotate_words(uint32_t (&w)[8], uint32_t R) {
@@ -668,13 +685,30 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         if (item >= (int)n_items) break;
         const int qq = s.query;
         if (qq != cur) {
-            const float4* src = reinterpret_cast<const float4*>(w.lut + (uint64_t)qq * G * kCodes * 32);
-            for (int e = t; e < G * kCodes * 8; e += NT) {
-                const float4 v = __ldg(src + e);
-                const int row = e >> 3, col = (e & 7) * 4;  // row = g*256 + c
-                float4* dstl = reinterpret_cast<float4*>(s_lut + row * 64 + col);
-                dstl[0] = v;
-                dstl[8] = v;  // columns 32..63 repeat 0..31
+            if (w.lut16) {  // FP16 entries widened to FP32 in shared memory
+                const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const __half*>(w.lut) +
+                                                                  (uint64_t)qq * G * kCodes * 32);
+                for (int e = t; e < G * kCodes * 4; e += NT) {
+                    const uint4 v = __ldg(src + e);
+                    const int row = e >> 2, col = (e & 3) * 8;
+                    const __half2* h = reinterpret_cast<const __half2*>(&v);
+                    const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]);
+                    const float2 f2 = __half22float2(h[2]), f3 = __half22float2(h[3]);
+                    float4* dstl = reinterpret_cast<float4*>(s_lut + row * 64 + col);
+                    dstl[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+                    dstl[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
+                    dstl[8] = dstl[0];
+                    dstl[9] = dstl[1];
+                }
+            } else {
+                const float4* src = reinterpret_cast<const float4*>(w.lut + (uint64_t)qq * G * kCodes * 32);
+                for (int e = t; e < G * kCodes * 8; e += NT) {
+                    const float4 v = __ldg(src + e);
+                    const int row = e >> 3, col = (e & 7) * 4;  // row = g*256 + c
+                    float4* dstl = reinterpret_cast<float4*>(s_lut + row * 64 + col);
+                    dstl[0] = v;
+                    dstl[8] = v;  // columns 32..63 repeat 0..31
+                }
             }
             if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
             scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
@@ -703,7 +737,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         for (uint32_t eb = e0 + t; eb < e1; eb += NT * CPT) {
             const uint4* cp[CPT];
             bool live[CPT];
-            float sum[CPT];
+            float sum[CPT], sum1[CPT];  // even / odd steps, added at the end
 #pragma unroll
             for (int u = 0; u < CPT; u++) {
                 const uint32_t e = eb + u * NT;
@@ -726,6 +760,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
                         row = pool;
                     }
                 }
+                sum1[u] = sum[u];
                 cp[u] = planes + row;  // chunk j of this point at cp[u][j * n_pts]
             }
 #pragma unroll
@@ -741,18 +776,21 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
                 }
                 const char* L = reinterpret_cast<const char*>(s_lut + g * (kCodes * 64));
 #pragma unroll
-                for (int st = 0; st < 32; st++) {
+                for (int st = 0; st < 32; st += 2) {
 #pragma unroll
                     for (int u = 0; u < CPT; u++) {
                         // one PRMT builds the byte offset c*256 + lane*4 (code byte -> byte 1,
                         // the lane's column byte -> byte 0); the step's column is the immediate
-                        const uint32_t a = __byte_perm(x[u][st >> 2], lane4, 0x5504u | ((st & 3) << 4));
-                        sum[u] += reinterpret_cast<const float*>(L + a)[st];
+                        const uint32_t a0 = __byte_perm(x[u][st >> 2], lane4, 0x5504u | ((st & 3) << 4));
+                        const uint32_t a1 = __byte_perm(x[u][st >> 2], lane4, 0x5504u | (((st + 1) & 3) << 4));
+                        add_f32x2(sum[u], sum1[u], reinterpret_cast<const float*>(L + a0)[st],
+                                  reinterpret_cast<const float*>(L + a1)[st + 1]);
                     }
                 }
             }
 #pragma unroll
             for (int u = 0; u < CPT; u++) {
+                sum[u] += sum1[u];
                 if (!live[u]) continue;
                 const uint32_t e = eb + u * NT;
                 if (sum[u] < INFINITY) {
@@ -810,8 +848,14 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
         if (item >= (int)n_items) break;
         const int qq = s.query;
         if (qq != cur) {
-            const float* src = w.lut + (uint64_t)qq * G * kCodes * 32;
-            for (int e = t; e < G * kCodes * 32; e += blockDim.x) s_lut[e] = src[e];
+            const uint64_t src0 = (uint64_t)qq * G * kCodes * 32;
+            if (w.lut16) {
+                const __half* src = reinterpret_cast<const __half*>(w.lut) + src0;
+                for (int e = t; e < G * kCodes * 32; e += blockDim.x) s_lut[e] = __half2float(src[e]);
+            } else {
+                const float* src = w.lut + src0;
+                for (int e = t; e < G * kCodes * 32; e += blockDim.x) s_lut[e] = src[e];
+            }
             if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
             scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
             cur = qq;
@@ -1249,7 +1293,8 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.mm = (uint32_t*)take("minmax", q * 2 * 4);
     w.nfin = (uint32_t*)take("nfin", q * 4);
     w.counter = (uint32_t*)take("counter", 16);
-    w.lut = (float*)take("lut", q * G * kCodes * 32 * 4);
+    w.lut16 = P.lut_fp16 != 0;
+    w.lut = (float*)take("lut", q * G * kCodes * 32 * (w.lut16 ? 2 : 4));
     w.cand_count = (uint32_t*)take("cand_count", q * 4);
     w.cand_pool = (uint32_t*)take("cand_pool", q * kcand * 4);
     w.kcand = kcand;
@@ -1395,8 +1440,10 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
     if (sm_pro > 48 * 1024)
         CK(cudaFuncSetAttribute(k_prologue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pro));
+    uint64_t launches = 0;  // kernels of this query, reported in the stats
     k_prologue<<<(unsigned)q, kThreads, sm_pro, st>>>(D, idx->grid, f, d_query_labels, (int)label_cols, w);
     CK_LAUNCH();
+    launches++;
     tm.mark("prologue");
 
     const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
@@ -1413,17 +1460,20 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         rows_to_bf16(d_queries, q, (int)D.d, w.qbf, w.qnorm, st);
         umma_dot(w.qbf, q, D.centers_bf16, D.C, (int)D.d, w.S, w.ldS, w.gemm_err, st);
         umma_dot(w.qbf, q, D.sub_centers_bf16, D.n_lists, (int)D.d, w.S + D.C, w.ldS, w.gemm_err, st);
+        launches += 3;
         tm.mark("coarse_gemm");
     } else {
         w.S = nullptr;
     }
     k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, d_queries, Pc, Ps, sort_n1, sort_n2, w);
     CK_LAUNCH();
+    launches++;
     tm.mark("coarse");
 
     // candidate offsets, work items, batch sums; one host read sizes the distance buffer
     k_batch<<<1, 1024, 0, st>>>(q, w);
     CK_LAUNCH();
+    launches++;
     uint64_t sc[4] = {0, 0, 0, 0};
     int gemm_err = 0;
     CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
@@ -1470,11 +1520,13 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
             const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
             CK(cudaFuncSetAttribute(k_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, d_queries, q, (int)G, w.lut);
+            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, d_queries, q, (int)G, w.lut,
+                                                                                w.lut16);
         } else {
-            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut);
+            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut, w.lut16);
         }
         CK_LAUNCH();
+        launches++;
         tm.mark("lut");
     }
 
@@ -1513,6 +1565,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
             k_scan_generic<<<blocks, 512, sm, st>>>(D, (int)G, Ps, pre, l, q, w);
         }
         CK_LAUNCH();
+        launches++;
     }
     tm.mark("scan");
 
@@ -1522,6 +1575,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     CK(cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sel));
     k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)k, sorted_out, w, d_dist, d_ids, (int)k);
     CK_LAUNCH();
+    launches++;
     tm.mark("select");
     if (mode != kPre) {
         const int rcap = (int)next_pow2(k + kThreads);
@@ -1530,8 +1584,10 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, d_queries, d_data, rcap, mode == kPost ? 1 : 0, l, w,
                                                        d_dist, d_ids, (int)k);
         CK_LAUNCH();
+        launches++;
         tm.mark("refine");
     }
+    idx->last_stats[8] = launches;
     tm.finish();
 }
 

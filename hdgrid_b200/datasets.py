@@ -11,6 +11,7 @@ distributions.  Seeds: base 1001, queries 1002, labels 1003, filters 1004.
   over a 10-entry interval table / div 10.  The fixed 604800-wide window over a 3e7 span
   caps any query's selectivity at 2.02 %, so per-query selectivity is log-uniform in
   [0.1 %, 2 %] (the map interval and the div threshold set it).
+* ``config3``  config2 with LUT_FP16=1, the BF16 coarse GEMM pruning the list ranking, exps0 4.
 * ``config4``  10M x 128 mixture, 4 int labels in [0, 1e6), type-3 range filters
   (filter_dim = 2); per-query selectivity log-uniform in [0.01 %, 90 %] split evenly over
   1-4 random dims; k drawn from {10, 100}.
@@ -110,6 +111,17 @@ def config2(scale: float = 1.0, n_queries: int = 10_000, **conf):
     c.update(conf)
     return dict(name="config2", base=base, labels=labels, queries=queries, query_labels=qlabels,
                 hdgrid_conf=hdgrid_conf(**c), filter_conf=filt, k=int(c["topk"]), selectivity=sel)
+
+
+def config3(scale: float = 1.0, n_queries: int = 10_000, **conf):
+    """Precision variant of config2: BF16 tensor-core coarse GEMM over all C + C*S centroids
+    (sub_lists below the list count, so the ranking is pruned by it), FP16 LUT summed in
+    FP32, and an exact FP32 re-rank of exps0*k*beta candidates with exps0 = 4."""
+    c = dict(lut_fp16=1, coarse_bf16=1, sub_lists=448, exps0=4)
+    c.update(conf)
+    ws = config2(scale=scale, n_queries=n_queries, **c)
+    ws["name"] = "config3"
+    return ws
 
 
 def config4(scale: float = 1.0, n_queries: int = 100_000, **conf):

@@ -149,7 +149,8 @@ hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q,
  * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget actually used (capped by the
  * shared-memory top-K), [3] sum of Morton candidate-range sizes, [4] sum of exact filtered
  * counts of the probed lists, [5] largest per-query candidate count, [6] beta as float bits,
- * [7] schedule (0 pre-filter, 1 post-filter, 2 single label dim).  Returns entries written. */
+ * [7] schedule (0 pre-filter, 1 post-filter, 2 single label dim), [8] kernels launched,
+ * [9] reserved.  Returns entries written (<= 10). */
 int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap);
 
 /* Per-stage device timings (ms) of the last hdg_query when break_down=1; returns the

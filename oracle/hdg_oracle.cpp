@@ -171,6 +171,7 @@ struct Index {
     uint64_t exps0() const { return params[4]; }
     uint64_t n_list() const { return params[8]; }
     uint64_t sub_lists() const { return params[9]; }
+    uint64_t lut_fp16() const { return params[20]; }
 };
 
 template <typename T>
@@ -660,7 +661,8 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
                     const float df = ix.pq_centers[((uint64_t)m * kCodes + c) * ix.pq_len + t] - qv[m * ix.pq_len + t];
                     acc = std::fmaf(df, df, acc);
                 }
-                lut[(size_t)m * kCodes + c] = acc;
+                // LUT_FP16=1: entries stored in binary16 (round to nearest even), summed in f32
+                lut[(size_t)m * kCodes + c] = ix.lut_fp16() ? (float)(_Float16)acc : acc;
             }
         auto pred = [&](uint32_t pool) {
             for (int i = 0; i < l; i++) {
@@ -672,17 +674,24 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
         // adc_mode 0: subspace order 0..M-1 (compute_batched_L2_distance_kernel :69-72).
         // adc_mode 1 (test mode): the order of the GPU scan's bank-rotated LUT, where the
         // candidate at position e of the query sums each group of 32 subspaces starting at
-        // subspace (e mod 32) and wrapping -- used to check that scan bit for bit.
+        // subspace (e mod 32) and wrapping, alternate steps into two partial sums that are
+        // added last -- used to check that scan bit for bit.
         auto adc = [&](uint32_t pool, uint32_t pos) {
             float sum = 0.f;
             const uint8_t* cp = &ix.codes[(uint64_t)pool * ix.M_pad];
             if (adc_mode == 1) {
+                // even steps and odd steps in two running sums, added at the end
                 const int lane = (int)(pos & 31);
+                float s1 = 0.f;
                 for (int g0 = 0; g0 < M; g0 += 32)
                     for (int st = 0; st < 32; st++) {
                         const int m = g0 + ((lane + st) & 31);
-                        sum += lut[(size_t)m * kCodes + cp[m]];
+                        if (st & 1)
+                            s1 += lut[(size_t)m * kCodes + cp[m]];
+                        else
+                            sum += lut[(size_t)m * kCodes + cp[m]];
                     }
+                sum += s1;
             } else {
                 for (int m = 0; m < M; m++) sum += lut[(size_t)m * kCodes + cp[m]];
             }

@@ -171,6 +171,25 @@ def test_parity_prefilter_rotated_adc(cuda):
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
 
 
+def test_parity_prefilter_rotated_adc_fp16_lut(cuda):
+    # LUT_FP16=1: entries rounded to binary16 and widened back to f32 in shared memory; the
+    # oracle rounds the same way, so ids and distances still match bit for bit
+    ws = datasets.config2(scale=0.01, n_queries=200, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000, exps0=1, lut_fp16=1)
+    _, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
+    valid = r["g_ids"] != INV
+    assert np.array_equal(r["g_ids"], r["o_ids"])
+    assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+
+
+def test_parity_precision_variant(cuda):
+    # BF16 coarse GEMM pruning + FP16 LUT + exact FP32 re-rank: integer stages bit-exact,
+    # final distances within 1e-4 relative of FP64 (checked inside _parity)
+    ws = datasets.config3(scale=0.01, n_queries=300, clusters=16, sub_clusters=4, n_list=12, sub_lists=20,
+                          max_grids=20_000)
+    _parity(ws, cuda)
+
+
 def test_parity_prefilter_generic_exact(cuda):
     # M = 16 (not a multiple of 32) takes the natural-order scan: ids and ADC distances
     # equal the oracle's bit for bit
