@@ -39,7 +39,8 @@ _PARAM_FIELDS = [
 
 class hdg_params(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in _PARAM_FIELDS] + [("path", C.c_char * 512)] + [
-        (f, C.c_uint64) for f in ("lut_fp16", "coarse_bf16", "kmeans_iters", "seed", "scan_cpt")]
+        (f, C.c_uint64) for f in ("lut_fp16", "coarse_bf16", "kmeans_iters", "seed", "scan_cpt", "scan_chunk",
+                                  "query_graph")]
 
 
 class hdg_filter_spec(C.Structure):
@@ -79,6 +80,8 @@ def _load() -> C.CDLL:
         "hdg_reserve": [vp, u64],
         "hdg_query": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp],
         "hdg_query_ex": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp],
+        "hdg_query_status": [vp],
+        "hdg_autotune": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp, C.POINTER(C.c_float)],
         "hdg_debug_fetch": [vp, C.c_char_p, vp, C.c_size_t, C.POINTER(C.c_size_t)],
         "hdg_get_info": [vp, C.POINTER(hdg_index_info)],
         "hdg_save": [vp, C.c_char_p],
@@ -297,6 +300,23 @@ class SuperGridIndex:
         _check(LIB.hdg_query_ex(self._h, _ptr(q), nq, _ptr(ql), ql.shape[1], _ptr(ds) if ds is not None else None,
                                 dist.shape[1], arr(k, torch.uint32), arr(n_probe, torch.uint32),
                                 arr(schedule, torch.uint8), _ptr(dist), _ptr(ids), _stream_ptr(stream)))
+
+    def status(self) -> None:
+        """Waits for the last CUDA-graph replay (QUERY_GRAPH=1) and raises its device status."""
+        _check(LIB.hdg_query_status(self._h))
+
+    def autotune(self, query_in: query_input_t, query_out: query_output_t, stream=None) -> dict:
+        """Times the scan variants on this batch, keeps the fastest (scan_cpt, scan_chunk)."""
+        q, ql, ds = query_in.queries, query_in.query_labels, query_in.dataset
+        _require_cuda_f32(q, 2)
+        _require_cuda_f32(ql, 2)
+        dist, ids = query_out.distances, query_out.neighbors
+        best = C.c_float()
+        _check(LIB.hdg_autotune(self._h, _ptr(q), q.shape[0], _ptr(ql), ql.shape[1],
+                                _ptr(ds) if ds is not None else None, dist.shape[1], _ptr(dist), _ptr(ids),
+                                _stream_ptr(stream), C.byref(best)))
+        p = self.params
+        return {"scan_cpt": int(p["scan_cpt"]), "scan_chunk": int(p["scan_chunk"]), "scan_ms": best.value}
 
     def save(self, path: str) -> None:
         _check(LIB.hdg_save(self._h, str(path).encode()))

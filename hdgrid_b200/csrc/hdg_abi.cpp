@@ -164,8 +164,14 @@ hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value) {
         else if (k == "LUT_FP16") f = &p.lut_fp16;
         else if (k == "COARSE_BF16") f = &p.coarse_bf16;
         else if (k == "SCAN_CPT") f = &p.scan_cpt;
+        else if (k == "SCAN_CHUNK") f = &p.scan_chunk;
+        else if (k == "QUERY_GRAPH") f = &p.query_graph;
         HDG_REQUIRE(f, HDG_ERR_INVALID_ARG, "not a search-time key: " + k);
+        if (k == "SCAN_CHUNK")
+            HDG_REQUIRE(value == 0 || (value >= 4096 && value <= 262144 && (value & (value - 1)) == 0),
+                        HDG_ERR_INVALID_ARG, "SCAN_CHUNK must be 0 or a power of two in [4096, 262144]");
         *f = value;
+        invalidate_graphs(index);  // captured graphs bake the old values in
     });
 }
 
@@ -205,8 +211,26 @@ hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q, co
     });
 }
 
-int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap) {
+hdg_status hdg_query_status(hdg_index* index) {
+    if (!index) return HDG_ERR_INVALID_ARG;
+    hdg_status st = HDG_OK;
+    const hdg_status g = guarded([&] { st = finish_async_query(index); });
+    return g != HDG_OK ? g : st;
+}
+
+hdg_status hdg_autotune(hdg_index* index, const float* d_queries, uint64_t q, const float* d_query_labels,
+                        uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+                        void* stream, float* best_scan_ms) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        autotune_query(index, d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids,
+                       static_cast<cudaStream_t>(stream), best_scan_ms);
+    });
+}
+
+int hdg_last_query_stats(hdg_index* index, uint64_t* out, int cap) {
     if (!index || !out) return 0;
+    guarded([&] { finish_async_query(index); });
     const int n = std::min(cap, 10);
     for (int i = 0; i < n; i++) out[i] = index->last_stats[i];
     return n;

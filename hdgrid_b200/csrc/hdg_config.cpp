@@ -123,6 +123,8 @@ void parse_hdgrid_conf(const std::string& text, hdg_params* p) {
         {"KMEANS_ITERS", &p->kmeans_iters},
         {"SEED", &p->seed},
         {"SCAN_CPT", &p->scan_cpt},
+        {"SCAN_CHUNK", &p->scan_chunk},
+        {"QUERY_GRAPH", &p->query_graph},
     };
     std::istringstream in(text);
     std::string line;

@@ -95,6 +95,9 @@ struct DeviceBuffer {
     ~DeviceBuffer() { reset(); }
 };
 
+struct GraphState;                 // captured query graphs (hdg_query.cu)
+void release_graphs(GraphState* g);
+
 }  // namespace hdg
 
 struct hdg_index {
@@ -118,4 +121,11 @@ struct hdg_index {
     uint64_t last_q = 0, last_ncand = 0;
     uint64_t last_stats[10] = {0};
     float last_beta = 0.f;
+    // CUDA-graph query path (QUERY_GRAPH=1): graphs keyed by the call's pointers and sizes,
+    // the replay stream and the pinned status words of the last replay
+    hdg::GraphState* graphs = nullptr;
+    hdg_index() = default;
+    hdg_index(const hdg_index&) = delete;
+    hdg_index& operator=(const hdg_index&) = delete;
+    ~hdg_index() { hdg::release_graphs(graphs); }
 };

@@ -44,6 +44,15 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
                cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,
                const uint8_t* d_sched = nullptr);
+void invalidate_graphs(hdg_index* idx);
+// waits for the last graph replay's status words; HDG_ERR_TIMEOUT (coarse GEMM wait
+// expired) or HDG_ERR_OOM (queries cut by the distance capacity) when they report one
+hdg_status finish_async_query(hdg_index* idx);
+// the autotuner: times the scan's (threads x candidates-per-thread, chunk) variants on
+// this batch and keeps the fastest in params.scan_cpt / params.scan_chunk
+void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+                    uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+                    cudaStream_t st, float* best_ms);
 void save_index(const hdg_index* idx, const std::string& path);
 hdg_index* load_index(const std::string& path);
 

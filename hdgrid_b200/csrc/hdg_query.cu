@@ -35,7 +35,7 @@ namespace hdg {
 constexpr int kThreads = 256;
 constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr int kMaxCand = 16384;     // largest candidate budget n_cand
-constexpr uint32_t kChunk = 32768;  // candidates per scan work item
+constexpr uint32_t kChunk = 32768;  // default candidates per scan work item (SCAN_CHUNK)
 constexpr int kBins = 4096;         // select histogram
 constexpr int kBCap = 4096;         // boundary-bin buffer of the select
 
@@ -50,7 +50,8 @@ struct Workspace {
     uint32_t* range_start;   // [q x Ps]
     uint32_t* range_len;     // [q x Ps]
     uint32_t* qstat;         // [q x 4]: cand_total, exact_total, n_lists, n_clusters
-    uint64_t* scal;          // [8]: cand sum, exact sum, max cand, items
+    uint64_t* scal;          // [8]: cand sum, exact sum, max cand, items, beta (f32 bits),
+                             //      queries dropped by the distance capacity, kept candidates
     uint64_t* qoff;          // [q + 1] candidate offsets into dist
     uint32_t* item_off;      // [q + 1] work-item offsets
     uint32_t* mm;            // [q x 2] min / max finite distance key
@@ -74,8 +75,8 @@ struct Workspace {
     uint32_t k_max;          // output row stride
     int mode;                // batch schedule: 0 pre-filter (exps0 <= 1), 1 post-filter, 2 single dim
     uint32_t exps0;
-    float beta;              // batch-wide coarse / exact candidate ratio (post-filter budget)
-    uint64_t max_row;        // largest per-query candidate count of the batch
+    uint32_t chunk;          // candidates per scan work item
+    uint64_t cap;            // distance-buffer capacity in candidates
 };
 
 enum ScanMode { kPre = 0, kPost = 1, kL1 = 2 };
@@ -98,12 +99,17 @@ __device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) {
     uint64_t K;
     if (w.mode == kL1 || q_sched(w, qi) == 1) {
         K = (uint64_t)w.exps0 * k;
-    } else if (!(w.beta < INFINITY)) {
-        K = w.max_row;
     } else {
-        const float want = (float)((uint64_t)w.exps0 * k) * w.beta;
-        K = want >= 1.8e19f ? ~0ull : (uint64_t)want;
-        K = min(K, w.max_row);
+        // beta and max_row of the batch, written by k_batch
+        const float beta = __uint_as_float((uint32_t)w.scal[4]);
+        const uint64_t max_row = w.scal[2];
+        if (!(beta < INFINITY)) {
+            K = max_row;
+        } else {
+            const float want = (float)((uint64_t)w.exps0 * k) * beta;
+            K = want >= 1.8e19f ? ~0ull : (uint64_t)want;
+            K = min(K, max_row);
+        }
     }
     return (uint32_t)max((uint64_t)1, min(K, (uint64_t)kMaxCand));
 }
@@ -444,9 +450,9 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     __shared__ unsigned long long s_tot[32], s_items[32];
-    __shared__ unsigned long long s_red[3];
+    __shared__ unsigned long long s_red[3], s_drop[2];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    if (t == 0) s_red[0] = s_red[1] = s_red[2] = 0;
+    if (t == 0) s_red[0] = s_red[1] = s_red[2] = s_drop[0] = s_drop[1] = 0;
     __syncthreads();
     const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
     const uint64_t b = t * per, e = min(q, b + per);
@@ -454,7 +460,7 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     for (uint64_t i = b; i < e; i++) {
         const uint32_t c = w.qstat[i * 4];
         cand += c;
-        items += (c + kChunk - 1) / kChunk;
+        items += (c + w.chunk - 1) / w.chunk;
         exact += w.qstat[i * 4 + 1];
         mx = max(mx, (unsigned long long)c);
     }
@@ -492,12 +498,23 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     __syncthreads();
     unsigned long long rc = xc - cand + (warp ? s_tot[warp - 1] : 0);
     unsigned long long ri = xi - items + (warp ? s_items[warp - 1] : 0);
+    unsigned long long dropped = 0, kept = 0;
     for (uint64_t i = b; i < e; i++) {
         const uint32_t c = w.qstat[i * 4];
         w.qoff[i] = rc;
         w.item_off[i] = (uint32_t)ri;
+        // queries past the distance capacity (a prefix cut: offsets grow with i) get no
+        // candidates; the batch's beta and max_row above still count them
+        if (rc + c > w.cap) {
+            if (c) {
+                w.qstat[i * 4] = 0;
+                dropped++;
+            }
+        } else {
+            kept += c;
+        }
         rc += c;
-        ri += (c + kChunk - 1) / kChunk;
+        ri += (c + w.chunk - 1) / w.chunk;
         w.mm[2 * i] = 0xffffffffu;
         w.mm[2 * i + 1] = 0u;
         w.nfin[i] = 0;
@@ -510,12 +527,19 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     atomicAdd(&s_red[0], cand);
     atomicAdd(&s_red[1], exact);
     atomicMax(&s_red[2], mx);
+    atomicAdd(&s_drop[0], dropped);
+    atomicAdd(&s_drop[1], kept);
     __syncthreads();
     if (t == 0) {
         w.scal[0] = s_red[0];
         w.scal[1] = s_red[1];
         w.scal[2] = s_red[2];
         w.scal[3] = s_items[(blockDim.x >> 5) - 1];
+        // beta = coarse / real as the reference computes it (Super-Grid-IVF_PQ.cu:1219)
+        const float beta = s_red[1] == 0 ? INFINITY : __fdiv_rn((float)s_red[0], (float)s_red[1]);
+        w.scal[4] = __float_as_uint(beta);
+        w.scal[5] = s_drop[0];
+        w.scal[6] = s_drop[1];
         w.counter[0] = 0;
     }
 }
@@ -684,6 +708,12 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         const int item = s.item;
         if (item >= (int)n_items) break;
         const int qq = s.query;
+        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * w.chunk;
+        if (e0 >= total) {  // a query cut by the distance capacity
+            __syncthreads();
+            continue;
+        }
         if (qq != cur) {
             if (w.lut16) {  // FP16 entries widened to FP32 in shared memory
                 const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const __half*>(w.lut) +
@@ -714,9 +744,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
             scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
             cur = qq;
         }
-        const uint32_t total = w.qstat[(uint64_t)qq * 4];
-        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
-        const uint32_t e1 = min(total, e0 + kChunk);
+        const uint32_t e1 = min(total, e0 + w.chunk);
         float* dst = w.dist + w.qoff[qq];
         const bool preq = pre || q_prefilter(w, qq);
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
@@ -847,6 +875,12 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
         const int item = s.item;
         if (item >= (int)n_items) break;
         const int qq = s.query;
+        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * w.chunk;
+        if (e0 >= total) {  // a query cut by the distance capacity
+            __syncthreads();
+            continue;
+        }
         if (qq != cur) {
             const uint64_t src0 = (uint64_t)qq * G * kCodes * 32;
             if (w.lut16) {
@@ -860,9 +894,7 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
             scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
             cur = qq;
         }
-        const uint32_t total = w.qstat[(uint64_t)qq * 4];
-        const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * kChunk;
-        const uint32_t e1 = min(total, e0 + kChunk);
+        const uint32_t e1 = min(total, e0 + w.chunk);
         float* dst = w.dist + w.qoff[qq];
         const bool preq = pre || q_prefilter(w, qq);
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
@@ -1403,94 +1435,65 @@ int sm_count() {
 }
 }  // namespace
 
-void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
-               uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
-               cudaStream_t st, const uint32_t* d_k, const uint32_t* d_nprobe, const uint8_t* d_sched) {
-    HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
-    HDG_REQUIRE(q > 0 && q < (1ull << 31), HDG_ERR_INVALID_ARG, "query count out of range");
-    HDG_REQUIRE(d_queries && d_query_labels && d_dist && d_ids, HDG_ERR_INVALID_ARG, "null pointer");
-    HDG_REQUIRE(k >= 1 && k <= 2048, HDG_ERR_INVALID_ARG, "k must be in [1, 2048]");
-    const hdg_params& P = idx->params;
-    const IndexDev& D = idx->dev;
-    const int l = (int)D.l;
-    const int fd = (int)std::max<uint64_t>(1, P.filter_dim);
-    HDG_REQUIRE(label_cols == (uint32_t)(l * fd), HDG_ERR_INVALID_ARG,
-                "query label columns must equal l * filter_dim");
-    const int Pc = (int)std::max<uint64_t>(1, P.n_list);
-    const int Ps = (int)std::max<uint64_t>(1, P.sub_lists);
-    HDG_REQUIRE(Pc <= 1024 && Ps <= 2048, HDG_ERR_UNSUPPORTED, "n_list <= 1024 and sub_lists <= 2048");
-    HDG_REQUIRE(D.n_lists <= 32768, HDG_ERR_UNSUPPORTED, "at most 32768 inverted lists");
-    const uint64_t exps0 = P.exps0;
-    const int mode = exps0 <= 1 ? kPre : (l > 1 ? kPost : kL1);
-    HDG_REQUIRE(mode == kPre || d_data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
-    HDG_REQUIRE(mode != kPre || !d_sched, HDG_ERR_INVALID_ARG,
-                "per-query schedules need exps0 > 1 (the pre-filter schedule has no re-rank)");
-    const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
-    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) reserve_workspace(idx, q, kcand);
-    Workspace w = carve(idx, q, kcand, true);
-    w.qk = d_k;
-    w.qps = d_nprobe;
-    w.qsched = d_sched;
-    w.k_max = k;
-    w.mode = mode;
-    w.exps0 = (uint32_t)std::min<uint64_t>(exps0, 1u << 20);
-    const FilterDev f = filter_dev(idx);
-    StageTimer tm(idx, st, P.break_down != 0);
+struct QueryCall {
+    const float* queries;
+    uint64_t q;
+    const float* qlabels;
+    uint32_t label_cols;
+    const float* data;
+    uint32_t k;
+    float* dist;
+    uint64_t* ids;
+    const uint32_t* qk;
+    const uint32_t* qps;
+    const uint8_t* qsched;
+};
 
-    const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
-    if (sm_pro > 48 * 1024)
-        CK(cudaFuncSetAttribute(k_prologue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pro));
-    uint64_t launches = 0;  // kernels of this query, reported in the stats
-    k_prologue<<<(unsigned)q, kThreads, sm_pro, st>>>(D, idx->grid, f, d_query_labels, (int)label_cols, w);
-    CK_LAUNCH();
-    launches++;
-    tm.mark("prologue");
+struct GraphEntry {
+    uint64_t key[24];
+    cudaGraphExec_t exec = nullptr;
+    uint64_t q = 0, launches = 0;
+    int mode = 0;
+    uint32_t k = 0;
+};
 
-    const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
-    const int sort_n2 = (int)next_pow2(std::max<uint32_t>((uint32_t)Pc * D.S_max, 2));
-    const size_t sm_co = sizeof(uint64_t) * std::max(sort_n1, sort_n2) + sizeof(float) * D.d;
-    HDG_REQUIRE(sm_co <= 200 * 1024, HDG_ERR_UNSUPPORTED, "coarse selection does not fit shared memory");
-    if (sm_co > 48 * 1024)
-        CK(cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co));
-    // tensor-core estimates of every query-centroid dot product, used to prune the exact
-    // ranking when n_list or sub_lists leaves part of the candidates out (COARSE_BF16=1)
-    const bool use_gemm = P.coarse_bf16 != 0 && D.d % 8 == 0 && (Pc < (int)D.C || Ps < Pc * (int)D.S_max);
-    if (use_gemm) {
-        CK(cudaMemsetAsync(w.gemm_err, 0, sizeof(int), st));
-        rows_to_bf16(d_queries, q, (int)D.d, w.qbf, w.qnorm, st);
-        umma_dot(w.qbf, q, D.centers_bf16, D.C, (int)D.d, w.S, w.ldS, w.gemm_err, st);
-        umma_dot(w.qbf, q, D.sub_centers_bf16, D.n_lists, (int)D.d, w.S + D.C, w.ldS, w.gemm_err, st);
-        launches += 3;
-        tm.mark("coarse_gemm");
-    } else {
-        w.S = nullptr;
-    }
-    k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, d_queries, Pc, Ps, sort_n1, sort_n2, w);
-    CK_LAUNCH();
-    launches++;
-    tm.mark("coarse");
+struct GraphState {
+    std::vector<GraphEntry> entries;
+    cudaStream_t stream = nullptr;  // capture and replay stream
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    uint64_t* pinned = nullptr;     // [8] scalars + [8] gemm status of the last replay
+    bool pending = false;
+    GraphEntry last;                // description of the last replay (stats)
+};
 
-    // candidate offsets, work items, batch sums; one host read sizes the distance buffer
-    k_batch<<<1, 1024, 0, st>>>(q, w);
-    CK_LAUNCH();
-    launches++;
-    uint64_t sc[4] = {0, 0, 0, 0};
-    int gemm_err = 0;
-    CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
-    if (use_gemm) CK(cudaMemcpyAsync(&gemm_err, w.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    HDG_REQUIRE(gemm_err == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
+void release_graphs(GraphState* g) {
+    if (!g) return;
+    for (auto& e : g->entries)
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (g->ev_in) cudaEventDestroy(g->ev_in);
+    if (g->ev_out) cudaEventDestroy(g->ev_out);
+    if (g->stream) cudaStreamDestroy(g->stream);
+    if (g->pinned) cudaFreeHost(g->pinned);
+    delete g;
+}
+
+void invalidate_graphs(hdg_index* idx) {
+    if (!idx->graphs) return;
+    if (idx->graphs->pending) cudaEventSynchronize(idx->graphs->ev_out);
+    for (auto& e : idx->graphs->entries)
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+    idx->graphs->entries.clear();
+    idx->graphs->pending = false;
+}
+
+// The stats of a query from its batch scalars (scal of k_batch).
+static void fill_stats(hdg_index* idx, uint64_t q, uint32_t k, int mode, uint64_t exps0, const uint64_t* sc,
+                       uint64_t launches) {
     const uint64_t coarse = sc[0], real = sc[1], max_row = sc[2];
-    if (idx->dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
-        idx->dist_buf.reset();
-        idx->dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
-    }
-    w.dist = static_cast<float*>(idx->dist_buf.ptr);
-    // beta = coarse / real (Super-Grid-IVF_PQ.cu:1219); budgets per query in q_budget
-    float beta = 0.f;
-    if (mode == kPost) beta = real == 0 ? INFINITY : (float)coarse / (float)real;
-    w.beta = beta;
-    w.max_row = max_row;
+    const uint32_t bb = (uint32_t)sc[4];
+    float beta;
+    std::memcpy(&beta, &bb, 4);
+    if (mode != kPost) beta = 0.f;
     uint64_t K = k;  // the budget of a query with the batch k and the reference schedule
     if (mode == kPost) {
         if (real == 0) {
@@ -1506,12 +1509,111 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     if (mode != kPre) K = std::max<uint64_t>(1, std::min<uint64_t>(K, (uint64_t)kMaxCand));
     idx->last_beta = beta;
     idx->last_q = q;
-    {
-        uint32_t bb;
-        std::memcpy(&bb, &beta, 4);
-        const uint64_t s[8] = {q, idx->last_ncand, K, coarse, real, max_row, bb, (uint64_t)mode};
-        std::memcpy(idx->last_stats, s, sizeof(s));
+    uint32_t bits;
+    std::memcpy(&bits, &beta, 4);
+    const uint64_t s[10] = {q, idx->last_ncand, K, coarse, real, max_row, bits, (uint64_t)mode, launches, sc[5]};
+    std::memcpy(idx->last_stats, s, sizeof(s));
+}
+
+// Enqueues one query batch on st.  sync_sizing: one host read after k_batch sizes the
+// distance buffer and fills the stats (the plain path).  Otherwise nothing waits on the
+// host (the CUDA-graph path): the distance buffer keeps its capacity, queries past it are
+// cut by k_batch, and the scalars and the GEMM status word are copied to pinned memory.
+static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, bool sync_sizing,
+                          uint64_t* pinned, uint64_t* launches_out, int* mode_out) {
+    const uint64_t q = c.q;
+    const uint32_t k = c.k;
+    HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
+    HDG_REQUIRE(q > 0 && q < (1ull << 31), HDG_ERR_INVALID_ARG, "query count out of range");
+    HDG_REQUIRE(c.queries && c.qlabels && c.dist && c.ids, HDG_ERR_INVALID_ARG, "null pointer");
+    HDG_REQUIRE(k >= 1 && k <= 2048, HDG_ERR_INVALID_ARG, "k must be in [1, 2048]");
+    const hdg_params& P = idx->params;
+    const IndexDev& D = idx->dev;
+    const int l = (int)D.l;
+    const int fd = (int)std::max<uint64_t>(1, P.filter_dim);
+    HDG_REQUIRE(c.label_cols == (uint32_t)(l * fd), HDG_ERR_INVALID_ARG,
+                "query label columns must equal l * filter_dim");
+    const int Pc = (int)std::max<uint64_t>(1, P.n_list);
+    const int Ps = (int)std::max<uint64_t>(1, P.sub_lists);
+    HDG_REQUIRE(Pc <= 1024 && Ps <= 2048, HDG_ERR_UNSUPPORTED, "n_list <= 1024 and sub_lists <= 2048");
+    HDG_REQUIRE(D.n_lists <= 32768, HDG_ERR_UNSUPPORTED, "at most 32768 inverted lists");
+    const uint64_t exps0 = P.exps0;
+    const int mode = exps0 <= 1 ? kPre : (l > 1 ? kPost : kL1);
+    if (mode_out) *mode_out = mode;
+    HDG_REQUIRE(mode == kPre || c.data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
+    HDG_REQUIRE(mode != kPre || !c.qsched, HDG_ERR_INVALID_ARG,
+                "per-query schedules need exps0 > 1 (the pre-filter schedule has no re-rank)");
+    const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
+    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) {
+        HDG_REQUIRE(sync_sizing, HDG_ERR_STATE, "workspace too small for a captured query");
+        reserve_workspace(idx, q, kcand);
     }
+    Workspace w = carve(idx, q, kcand, true);
+    w.qk = c.qk;
+    w.qps = c.qps;
+    w.qsched = c.qsched;
+    w.k_max = k;
+    w.mode = mode;
+    w.exps0 = (uint32_t)std::min<uint64_t>(exps0, 1u << 20);
+    w.chunk = P.scan_chunk ? (uint32_t)P.scan_chunk : kChunk;
+    w.cap = sync_sizing ? ~0ull : idx->dist_buf.bytes / 4;
+    const FilterDev f = filter_dev(idx);
+    StageTimer tm(idx, st, sync_sizing && P.break_down != 0);
+
+    const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
+    if (sm_pro > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_prologue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pro));
+    uint64_t launches = 0;  // kernels of this query, reported in the stats
+    k_prologue<<<(unsigned)q, kThreads, sm_pro, st>>>(D, idx->grid, f, c.qlabels, (int)c.label_cols, w);
+    CK_LAUNCH();
+    launches++;
+    tm.mark("prologue");
+
+    const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
+    const int sort_n2 = (int)next_pow2(std::max<uint32_t>((uint32_t)Pc * D.S_max, 2));
+    const size_t sm_co = sizeof(uint64_t) * std::max(sort_n1, sort_n2) + sizeof(float) * D.d;
+    HDG_REQUIRE(sm_co <= 200 * 1024, HDG_ERR_UNSUPPORTED, "coarse selection does not fit shared memory");
+    if (sm_co > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co));
+    // tensor-core estimates of every query-centroid dot product, used to prune the exact
+    // ranking when n_list or sub_lists leaves part of the candidates out (COARSE_BF16=1)
+    const bool use_gemm = P.coarse_bf16 != 0 && D.d % 8 == 0 && (Pc < (int)D.C || Ps < Pc * (int)D.S_max);
+    CK(cudaMemsetAsync(w.gemm_err, 0, sizeof(int), st));
+    if (use_gemm) {
+        rows_to_bf16(c.queries, q, (int)D.d, w.qbf, w.qnorm, st);
+        umma_dot(w.qbf, q, D.centers_bf16, D.C, (int)D.d, w.S, w.ldS, w.gemm_err, st);
+        umma_dot(w.qbf, q, D.sub_centers_bf16, D.n_lists, (int)D.d, w.S + D.C, w.ldS, w.gemm_err, st);
+        launches += 3;
+        tm.mark("coarse_gemm");
+    } else {
+        w.S = nullptr;
+    }
+    k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, c.queries, Pc, Ps, sort_n1, sort_n2, w);
+    CK_LAUNCH();
+    launches++;
+    tm.mark("coarse");
+
+    // candidate offsets, work items, batch sums, beta and the per-query budgets' inputs
+    k_batch<<<1, 1024, 0, st>>>(q, w);
+    CK_LAUNCH();
+    launches++;
+    uint64_t sc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (sync_sizing) {
+        int gemm_err = 0;
+        CK(cudaMemcpyAsync(sc, w.scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&gemm_err, w.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        HDG_REQUIRE(gemm_err == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
+        const uint64_t coarse = sc[0];
+        if (idx->dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
+            invalidate_graphs(idx);  // their distance pointer dies with the old buffer
+            idx->dist_buf.reset();
+            idx->dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
+        }
+    } else {
+        HDG_REQUIRE(idx->dist_buf.ptr, HDG_ERR_STATE, "no distance buffer for a captured query");
+    }
+    w.dist = static_cast<float*>(idx->dist_buf.ptr);
     tm.mark("budget");
 
     const uint32_t G = lut_groups(D);
@@ -1520,10 +1622,11 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
             const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
             CK(cudaFuncSetAttribute(k_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, d_queries, q, (int)G, w.lut,
+            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, c.queries, q, (int)G, w.lut,
                                                                                 w.lut16);
         } else {
-            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, d_queries, (int)G, w.lut, w.lut16);
+            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, c.queries, (int)G, w.lut,
+                                                                              w.lut16);
         }
         CK_LAUNCH();
         launches++;
@@ -1532,17 +1635,16 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
 
     const int pre = mode == kPre ? 1 : 0;
     const size_t sm_tab = sizeof(uint32_t) * (2 * Ps + 1);
-    if (sc[3] > 0) {
+    if (!sync_sizing || sc[3] > 0) {
         if (fast) {
             const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
-                kern<<<blocks, nt, sm, st>>>(D, d_queries, Ps, pre, l, q, w);
+                kern<<<blocks, nt, sm, st>>>(D, c.queries, Ps, pre, l, q, w);
             };
-            // threads x candidates-per-thread (SCAN_CPT; 0 = measured default 1: more
-            // interleaved candidates per thread ran slower at M = 32 and M = 96)
+            // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
             const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
             if (G == 1) {
                 if (cpt == 1) launch(k_scan_fast<1, 512, 1>, 512);
@@ -1573,7 +1675,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     const size_t sm_sel = sizeof(uint32_t) * kBins + sizeof(uint64_t) * kBCap +
                           (sorted_out ? sizeof(uint64_t) * next_pow2(std::max<uint32_t>(k, 2)) : 0) + sm_tab + 16;
     CK(cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sel));
-    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)k, sorted_out, w, d_dist, d_ids, (int)k);
+    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)k, sorted_out, w, c.dist, c.ids, (int)k);
     CK_LAUNCH();
     launches++;
     tm.mark("select");
@@ -1581,14 +1683,155 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         const int rcap = (int)next_pow2(k + kThreads);
         const size_t sm_ref = sizeof(uint64_t) * rcap + sizeof(float) * D.d + 16;
         CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ref));
-        k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, d_queries, d_data, rcap, mode == kPost ? 1 : 0, l, w,
-                                                       d_dist, d_ids, (int)k);
+        k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, c.queries, c.data, rcap, mode == kPost ? 1 : 0, l, w,
+                                                       c.dist, c.ids, (int)k);
         CK_LAUNCH();
         launches++;
         tm.mark("refine");
     }
-    idx->last_stats[8] = launches;
+    if (!sync_sizing && pinned) {
+        CK(cudaMemcpyAsync(pinned, w.scal, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(pinned + 8, w.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    if (launches_out) *launches_out = launches;
+    if (sync_sizing) fill_stats(idx, q, k, mode, exps0, sc, launches);
     tm.finish();
+}
+
+hdg_status finish_async_query(hdg_index* idx) {
+    GraphState* g = idx->graphs;
+    if (!g || !g->pending) return HDG_OK;
+    CK(cudaEventSynchronize(g->ev_out));
+    g->pending = false;
+    fill_stats(idx, g->last.q, g->last.k, g->last.mode, idx->params.exps0, g->pinned, g->last.launches);
+    if (static_cast<int>(g->pinned[8] & 0xffffffffu) != 0) return HDG_ERR_TIMEOUT;
+    if (g->pinned[5] != 0) return HDG_ERR_OOM;
+    return HDG_OK;
+}
+
+static void make_graph_key(const hdg_index* idx, const QueryCall& c, uint64_t* key) {
+    const hdg_params& P = idx->params;
+    const uint64_t v[24] = {(uint64_t)c.queries, c.q, (uint64_t)c.qlabels, c.label_cols, (uint64_t)c.data, c.k,
+                            (uint64_t)c.dist, (uint64_t)c.ids, (uint64_t)c.qk, (uint64_t)c.qps, (uint64_t)c.qsched,
+                            (uint64_t)idx->work.ptr, idx->work.bytes, (uint64_t)idx->dist_buf.ptr,
+                            idx->dist_buf.bytes, P.n_list, P.sub_lists, P.exps0, P.lut_fp16, P.coarse_bf16,
+                            P.scan_cpt, P.scan_chunk, P.filter_dim, 0};
+    std::memcpy(key, v, sizeof(v));
+}
+
+void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+               uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+               cudaStream_t st, const uint32_t* d_k, const uint32_t* d_nprobe, const uint8_t* d_sched) {
+    const QueryCall c{d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids, d_k, d_nprobe, d_sched};
+    if (idx->params.query_graph == 0) {
+        finish_async_query(idx);
+        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
+        return;
+    }
+    if (!idx->graphs) {
+        GraphState* g = new GraphState();
+        idx->graphs = g;
+        CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming));
+        CK(cudaMallocHost(reinterpret_cast<void**>(&g->pinned), 16 * sizeof(uint64_t)));
+        std::memset(g->pinned, 0, 16 * sizeof(uint64_t));
+    }
+    GraphState* g = idx->graphs;
+    finish_async_query(idx);  // the pinned status words are reused by this replay
+    uint64_t key[24];
+    make_graph_key(idx, c, key);
+    GraphEntry* hit = nullptr;
+    for (auto& e : g->entries)
+        if (std::memcmp(e.key, key, sizeof(key)) == 0) hit = &e;
+    if (!hit) {
+        // first call of this shape: the plain path computes this call's results and sizes
+        // the buffers; the captured graph serves the next calls
+        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
+        const uint64_t need = std::max<uint64_t>(idx->last_stats[3], 1) * 4 * 2;  // 2x this batch
+        if (idx->dist_buf.bytes < need) {
+            invalidate_graphs(idx);
+            idx->dist_buf.reset();
+            idx->dist_buf.ensure(need);
+        }
+        make_graph_key(idx, c, key);
+        CK(cudaStreamSynchronize(st));
+        GraphEntry e;
+        std::memcpy(e.key, key, sizeof(key));
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed));
+        try {
+            enqueue_query(idx, c, g->stream, false, g->pinned, &e.launches, &e.mode);
+        } catch (...) {
+            cudaStreamEndCapture(g->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        CK(cudaStreamEndCapture(g->stream, &graph));
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        e.q = q;
+        e.k = k;
+        if (g->entries.size() >= 8) {
+            cudaGraphExecDestroy(g->entries.front().exec);
+            g->entries.erase(g->entries.begin());
+        }
+        g->entries.push_back(e);
+        return;
+    }
+    CK(cudaEventRecord(g->ev_in, st));
+    CK(cudaStreamWaitEvent(g->stream, g->ev_in, 0));
+    CK(cudaGraphLaunch(hit->exec, g->stream));
+    CK(cudaEventRecord(g->ev_out, g->stream));
+    CK(cudaStreamWaitEvent(st, g->ev_out, 0));
+    g->last = *hit;
+    g->pending = true;
+}
+
+void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+                    uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
+                    cudaStream_t st, float* best_ms) {
+    hdg_params& P = idx->params;
+    const uint64_t saved_bd = P.break_down, saved_graph = P.query_graph;
+    P.break_down = 1;
+    P.query_graph = 0;
+    const QueryCall c{d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids, nullptr, nullptr, nullptr};
+    float best = INFINITY;
+    uint64_t best_cpt = 1, best_chunk = kChunk;
+    try {
+        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);  // warm-up, buffers sized
+        const uint64_t cpts[3] = {1, 2, 4};
+        const uint64_t chunks[4] = {8192, 16384, 32768, 65536};
+        for (uint64_t cpt : cpts)
+            for (uint64_t ch : chunks) {
+                P.scan_cpt = cpt;
+                P.scan_chunk = ch;
+                float t = INFINITY;
+                for (int rep = 0; rep < 2; rep++) {  // the faster of two runs
+                    enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
+                    float s = 0.f;
+                    for (size_t i = 0; i < idx->stage_names.size(); i++)
+                        if (idx->stage_names[i] == "scan") s = idx->stage_ms[i];
+                    t = std::min(t, s);
+                }
+                if (t < best) {
+                    best = t;
+                    best_cpt = cpt;
+                    best_chunk = ch;
+                }
+            }
+    } catch (...) {
+        P.break_down = saved_bd;
+        P.query_graph = saved_graph;
+        throw;
+    }
+    P.scan_cpt = best_cpt;
+    P.scan_chunk = best_chunk;
+    P.break_down = saved_bd;
+    P.query_graph = saved_graph;
+    invalidate_graphs(idx);
+    if (best_ms) *best_ms = best;
 }
 
 }  // namespace hdg

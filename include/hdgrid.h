@@ -77,6 +77,10 @@ typedef struct hdg_params {
     uint64_t kmeans_iters;  /* KMEANS_ITERS: Lloyd iterations of the index build (default 20) */
     uint64_t seed;          /* SEED: build RNG seed (default 1234) */
     uint64_t scan_cpt;      /* SCAN_CPT: ADC scan candidates per thread (1, 2 or 4; 0 = default) */
+    uint64_t scan_chunk;    /* SCAN_CHUNK: candidates per scan work item (power of two in
+                             * [4096, 262144]; 0 = 32768) -- the list/query split of the scan */
+    uint64_t query_graph;   /* QUERY_GRAPH: 1 = hdg_query replays a captured CUDA graph per
+                             * (pointers, q, k); status of a replay via hdg_query_status */
 } hdg_params;
 
 /* filter.conf contents (config_utils.h:112-172).  interval_map is the flat
@@ -151,7 +155,27 @@ hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q,
  * counts of the probed lists, [5] largest per-query candidate count, [6] beta as float bits,
  * [7] schedule (0 pre-filter, 1 post-filter, 2 single label dim), [8] kernels launched,
  * [9] reserved.  Returns entries written (<= 10). */
-int hdg_last_query_stats(const hdg_index* index, uint64_t* out, int cap);
+int hdg_last_query_stats(hdg_index* index, uint64_t* out, int cap);
+
+/* With QUERY_GRAPH=1 hdg_query returns once the captured graph is enqueued; this waits for
+ * the last replay and returns its device status: HDG_OK, HDG_ERR_TIMEOUT (a tensor-core
+ * wait of the coarse GEMM expired) or HDG_ERR_OOM (the batch had more candidates than the
+ * distance buffer sized at capture -- twice the first batch of the shape -- and the
+ * queries past it returned no results).  HDG_OK when no replay is pending.  No reference
+ * counterpart: the reference synchronises after every stage. */
+hdg_status hdg_query_status(hdg_index* index);
+
+/* The project autotuner: runs the batch through the plain path once per scan variant --
+ * threads x candidates-per-thread (SCAN_CPT 1, 2, 4) and work-item size (SCAN_CHUNK 8192 ..
+ * 65536 candidates, the split of the scan between lists and queries) -- and keeps the
+ * fastest scan in the index's parameters.  Outputs as hdg_query; best_scan_ms (may be
+ * NULL) receives the chosen variant's scan time.  Replaces the reference's memory
+ * predictor (search-engine/search-engine-auto-batch.cu:178-190, 381-430, 431-490), which
+ * picks batch sizes instead. */
+hdg_status hdg_autotune(hdg_index* index, const float* d_queries, uint64_t q,
+                        const float* d_query_labels, uint32_t label_cols, const float* d_data,
+                        uint32_t k, float* d_dist, uint64_t* d_ids, void* stream,
+                        float* best_scan_ms);
 
 /* Per-stage device timings (ms) of the last hdg_query when break_down=1; returns the
  * number of stages written (<= cap) and their names via names (may be NULL). */
