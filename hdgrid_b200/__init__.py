@@ -40,7 +40,7 @@ _PARAM_FIELDS = [
 class hdg_params(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in _PARAM_FIELDS] + [("path", C.c_char * 512)] + [
         (f, C.c_uint64) for f in ("lut_fp16", "coarse_bf16", "kmeans_iters", "seed", "scan_cpt", "scan_chunk",
-                                  "query_graph")]
+                                  "query_graph", "learned")]
 
 
 class hdg_filter_spec(C.Structure):
@@ -81,6 +81,13 @@ def _load() -> C.CDLL:
         "hdg_query": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp],
         "hdg_query_ex": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp],
         "hdg_query_status": [vp],
+        "hdg_query_features": [vp, vp, u64, vp, u32, vp, u32, vp, vp],
+        "hdg_mlp_init": [vp, u64],
+        "hdg_mlp_set_weights": [vp, vp, u64],
+        "hdg_mlp_get_weights": [vp, vp, u64],
+        "hdg_mlp_forward": [vp, vp, u64, vp, vp],
+        "hdg_mlp_gradients": [vp, vp, vp, u64, vp, C.POINTER(C.c_double), vp],
+        "hdg_mlp_train": [vp, vp, vp, u64, u32, u32, C.c_float, u64, C.POINTER(C.c_double), vp],
         "hdg_autotune": [vp, vp, u64, vp, u32, vp, u32, vp, vp, vp, C.POINTER(C.c_float)],
         "hdg_debug_fetch": [vp, C.c_char_p, vp, C.c_size_t, C.POINTER(C.c_size_t)],
         "hdg_get_info": [vp, C.POINTER(hdg_index_info)],
@@ -104,6 +111,8 @@ def _load() -> C.CDLL:
     lib.hdg_last_stage_times.restype = C.c_int
     lib.hdg_last_query_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.c_int]
     lib.hdg_last_query_stats.restype = C.c_int
+    lib.hdg_mlp_param_count.restype = C.c_uint64
+    lib.hdg_mlp_param_count.argtypes = []
     return lib
 
 
@@ -300,6 +309,60 @@ class SuperGridIndex:
         _check(LIB.hdg_query_ex(self._h, _ptr(q), nq, _ptr(ql), ql.shape[1], _ptr(ds) if ds is not None else None,
                                 dist.shape[1], arr(k, torch.uint32), arr(n_probe, torch.uint32),
                                 arr(schedule, torch.uint8), _ptr(dist), _ptr(ids), _stream_ptr(stream)))
+
+    # ---- learned per-query schedule -------------------------------------------------
+    def query_features(self, queries, query_labels, k_max: int, k=None, stream=None):
+        """[q x 48] features of each query (CUDA float32 tensor)."""
+        import torch
+        _require_cuda_f32(queries, 2)
+        _require_cuda_f32(query_labels, 2)
+        out = torch.empty((queries.shape[0], 48), dtype=torch.float32, device=queries.device)
+        if k is not None and not (k.is_cuda and k.dtype == torch.uint32 and k.numel() == queries.shape[0]):
+            raise HDGError(HDG_ERR_INVALID_ARG, "k must be a CUDA uint32 tensor of q entries")
+        _check(LIB.hdg_query_features(self._h, _ptr(queries), queries.shape[0], _ptr(query_labels),
+                                      query_labels.shape[1], _ptr(k) if k is not None else None, k_max, _ptr(out),
+                                      _stream_ptr(stream)))
+        return out
+
+    def mlp_init(self, seed: int = 1) -> None:
+        _check(LIB.hdg_mlp_init(self._h, seed))
+
+    def mlp_weights(self):
+        import numpy as np
+        w = np.empty(int(LIB.hdg_mlp_param_count()), np.float32)
+        _check(LIB.hdg_mlp_get_weights(self._h, w.ctypes.data, w.size))
+        return w
+
+    def set_mlp_weights(self, w) -> None:
+        import numpy as np
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(LIB.hdg_mlp_set_weights(self._h, w.ctypes.data, w.size))
+
+    def mlp_forward(self, x, stream=None):
+        import torch
+        _require_cuda_f32(x, 2)
+        z = torch.empty((x.shape[0], 2), dtype=torch.float32, device=x.device)
+        _check(LIB.hdg_mlp_forward(self._h, _ptr(x), x.shape[0], _ptr(z), _stream_ptr(stream)))
+        return z
+
+    def mlp_gradients(self, x, y, stream=None):
+        import torch
+        _require_cuda_f32(x, 2)
+        _require_cuda_f32(y, 2)
+        g = torch.empty(int(LIB.hdg_mlp_param_count()), dtype=torch.float32, device=x.device)
+        loss = C.c_double()
+        _check(LIB.hdg_mlp_gradients(self._h, _ptr(x), _ptr(y), x.shape[0], _ptr(g), C.byref(loss),
+                                     _stream_ptr(stream)))
+        return g, loss.value
+
+    def mlp_train(self, x, y, epochs: int = 50, batch: int = 1024, lr: float = 2e-3, seed: int = 1,
+                  stream=None) -> float:
+        _require_cuda_f32(x, 2)
+        _require_cuda_f32(y, 2)
+        loss = C.c_double()
+        _check(LIB.hdg_mlp_train(self._h, _ptr(x), _ptr(y), x.shape[0], epochs, batch, lr, seed, C.byref(loss),
+                                 _stream_ptr(stream)))
+        return loss.value
 
     def status(self) -> None:
         """Waits for the last CUDA-graph replay (QUERY_GRAPH=1) and raises its device status."""

@@ -28,6 +28,7 @@ LIB_SOURCES = [
     "hdg_query.cu",
     "hdg_kernels_ref.cu",
     "hdg_gemm.cu",
+    "hdg_learned.cu",
 ]
 
 

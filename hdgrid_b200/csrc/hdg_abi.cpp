@@ -166,6 +166,7 @@ hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value) {
         else if (k == "SCAN_CPT") f = &p.scan_cpt;
         else if (k == "SCAN_CHUNK") f = &p.scan_chunk;
         else if (k == "QUERY_GRAPH") f = &p.query_graph;
+        else if (k == "LEARNED") f = &p.learned;
         HDG_REQUIRE(f, HDG_ERR_INVALID_ARG, "not a search-time key: " + k);
         if (k == "SCAN_CHUNK")
             HDG_REQUIRE(value == 0 || (value >= 4096 && value <= 262144 && (value & (value - 1)) == 0),
@@ -225,6 +226,65 @@ hdg_status hdg_autotune(hdg_index* index, const float* d_queries, uint64_t q, co
         HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
         autotune_query(index, d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids,
                        static_cast<cudaStream_t>(stream), best_scan_ms);
+    });
+}
+
+hdg_status hdg_query_features(hdg_index* index, const float* d_queries, uint64_t q, const float* d_query_labels,
+                              uint32_t label_cols, const uint32_t* d_k, uint32_t k_max, float* d_features,
+                              void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        HDG_REQUIRE(k_max >= 1, HDG_ERR_INVALID_ARG, "k_max must be >= 1");
+        query_features(index, d_queries, q, d_query_labels, label_cols, d_k, k_max, d_features,
+                       static_cast<cudaStream_t>(stream));
+    });
+}
+
+uint64_t hdg_mlp_param_count(void) { return (uint64_t)kMlpParams; }
+
+hdg_status hdg_mlp_init(hdg_index* index, uint64_t seed) {
+    return guarded([&] {
+        HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
+        mlp_init(index, seed);
+    });
+}
+
+hdg_status hdg_mlp_set_weights(hdg_index* index, const float* host, uint64_t count) {
+    return guarded([&] {
+        HDG_REQUIRE(index && host, HDG_ERR_INVALID_ARG, "null argument");
+        mlp_set(index, host, count);
+    });
+}
+
+hdg_status hdg_mlp_get_weights(hdg_index* index, float* host, uint64_t count) {
+    return guarded([&] {
+        HDG_REQUIRE(index && host, HDG_ERR_INVALID_ARG, "null argument");
+        mlp_get(index, host, count);
+    });
+}
+
+hdg_status hdg_mlp_forward(hdg_index* index, const float* d_x, uint64_t n, float* d_z, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index && d_x && d_z && n > 0, HDG_ERR_INVALID_ARG, "bad argument");
+        mlp_forward(index, d_x, n, d_z, static_cast<cudaStream_t>(stream));
+    });
+}
+
+hdg_status hdg_mlp_gradients(hdg_index* index, const float* d_x, const float* d_y, uint64_t n, float* d_grad,
+                             double* loss, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index && d_x && d_y && d_grad, HDG_ERR_INVALID_ARG, "null argument");
+        const double l = mlp_gradients(index, d_x, d_y, n, d_grad, static_cast<cudaStream_t>(stream));
+        if (loss) *loss = l;
+    });
+}
+
+hdg_status hdg_mlp_train(hdg_index* index, const float* d_x, const float* d_y, uint64_t n, uint32_t epochs,
+                         uint32_t batch, float lr, uint64_t seed, double* final_loss, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(index && d_x && d_y, HDG_ERR_INVALID_ARG, "null argument");
+        const double l = mlp_train(index, d_x, d_y, n, epochs, batch, lr, seed, static_cast<cudaStream_t>(stream));
+        if (final_loss) *final_loss = l;
     });
 }
 

@@ -125,6 +125,7 @@ void parse_hdgrid_conf(const std::string& text, hdg_params* p) {
         {"SCAN_CPT", &p->scan_cpt},
         {"SCAN_CHUNK", &p->scan_chunk},
         {"QUERY_GRAPH", &p->query_graph},
+        {"LEARNED", &p->learned},
     };
     std::istringstream in(text);
     std::string line;

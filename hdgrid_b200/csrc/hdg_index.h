@@ -124,6 +124,10 @@ struct hdg_index {
     // CUDA-graph query path (QUERY_GRAPH=1): graphs keyed by the call's pointers and sizes,
     // the replay stream and the pinned status words of the last replay
     hdg::GraphState* graphs = nullptr;
+    // learned per-query schedule: f32 master | Adam m | Adam v | gradient | bf16 weights
+    hdg::DeviceBuffer mlp;
+    bool mlp_ready = false;
+    uint64_t mlp_step = 0;
     hdg_index() = default;
     hdg_index(const hdg_index&) = delete;
     hdg_index& operator=(const hdg_index&) = delete;

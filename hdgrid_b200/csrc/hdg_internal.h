@@ -44,6 +44,30 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
                cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,
                const uint8_t* d_sched = nullptr);
+// learned per-query schedule (hdg_learned.cu): 48 features -> 128 -> 128 -> 2 BF16 MLP,
+// parameters W1 [128 x 48], b1, W2 [128 x 128], b2, W3 [2 x 128], b3 in one f32 vector
+constexpr int kMlpFeatures = 48, kMlpHidden = 128, kMlpOut = 2;
+constexpr int kMlpW1 = 0;
+constexpr int kMlpB1 = kMlpW1 + kMlpHidden * kMlpFeatures;
+constexpr int kMlpW2 = kMlpB1 + kMlpHidden;
+constexpr int kMlpB2 = kMlpW2 + kMlpHidden * kMlpHidden;
+constexpr int kMlpW3 = kMlpB2 + kMlpHidden;
+constexpr int kMlpB3 = kMlpW3 + kMlpOut * kMlpHidden;
+constexpr int kMlpParams = kMlpB3 + kMlpOut;
+void learned_features(hdg_index* idx, const float* d_queries, uint64_t q, const float* box, const uint32_t* cc,
+                      const uint32_t* qk, uint32_t k_max, float* feats, cudaStream_t st);
+void learned_infer(hdg_index* idx, const float* feats, uint64_t q, uint32_t* nprobe, uint8_t* sched, int allow_sched,
+                   uint32_t max_probe, float* z, cudaStream_t st);
+void mlp_init(hdg_index* idx, uint64_t seed);
+void mlp_set(hdg_index* idx, const float* host, size_t count);
+void mlp_get(hdg_index* idx, float* host, size_t count);
+void mlp_forward(hdg_index* idx, const float* d_x, uint64_t n, float* d_z, cudaStream_t st);
+double mlp_gradients(hdg_index* idx, const float* d_x, const float* d_y, uint64_t n, float* d_grad, cudaStream_t st);
+double mlp_train(hdg_index* idx, const float* d_x, const float* d_y, uint64_t n, uint32_t epochs, uint32_t batch,
+                 float lr, uint64_t seed, cudaStream_t st);
+// query features of a batch: the prologue (filter boxes, per-list counts) then k_features
+void query_features(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+                    uint32_t label_cols, const uint32_t* d_k, uint32_t k_max, float* d_feats, cudaStream_t st);
 void invalidate_graphs(hdg_index* idx);
 // waits for the last graph replay's status words; HDG_ERR_TIMEOUT (coarse GEMM wait
 // expired) or HDG_ERR_OOM (queries cut by the distance capacity) when they report one

@@ -68,6 +68,9 @@ struct Workspace {
     float* qnorm;            // [q] squared query norms
     void* qbf;               // [q x d] bf16 queries
     int* gemm_err;           // tensor-core wait expiry flag
+    float* feats;            // [q x 48] learned-schedule features
+    uint32_t* lq_ps;         // [q] lists to probe predicted by the learned schedule
+    uint8_t* lq_sched;       // [q] predicate-first flag predicted by the learned schedule
     // per-query parameters (nullptr: the batch-wide value)
     const uint32_t* qk;      // [q] k of each query (<= k_max)
     const uint32_t* qps;     // [q] lists probed (<= sub_lists)
@@ -1335,6 +1338,9 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.qnorm = (float*)take("qnorm", q * 4);
     w.qbf = take("qbf", q * idx->dev.d * 2);
     w.gemm_err = (int*)take("gemm_err", 16);
+    w.feats = (float*)take("features", q * kMlpFeatures * 4);
+    w.lq_ps = (uint32_t*)take("learned_nprobe", q * 4);
+    w.lq_sched = (uint8_t*)take("learned_schedule", q);
     w.dist = static_cast<float*>(idx->dist_buf.ptr);
     if (!base) idx->work.bytes = std::max(idx->work.bytes, off);  // size probe
     return w;
@@ -1568,6 +1574,16 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     CK_LAUNCH();
     launches++;
     tm.mark("prologue");
+    if (P.learned && !c.qps && !c.qsched) {
+        // the learned schedule: per-query lists to probe and predicate-first flag
+        HDG_REQUIRE(idx->mlp_ready, HDG_ERR_STATE, "LEARNED=1 but the index holds no trained model");
+        learned_features(idx, c.queries, q, w.box, w.cluster_counts, c.qk, k, w.feats, st);
+        learned_infer(idx, w.feats, q, w.lq_ps, w.lq_sched, mode != kPre, (uint32_t)Ps, nullptr, st);
+        w.qps = w.lq_ps;
+        w.qsched = mode != kPre ? w.lq_sched : nullptr;
+        launches += 2;
+        tm.mark("learned");
+    }
 
     const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
     const int sort_n2 = (int)next_pow2(std::max<uint32_t>((uint32_t)Pc * D.S_max, 2));
@@ -1715,7 +1731,7 @@ static void make_graph_key(const hdg_index* idx, const QueryCall& c, uint64_t* k
                             (uint64_t)c.dist, (uint64_t)c.ids, (uint64_t)c.qk, (uint64_t)c.qps, (uint64_t)c.qsched,
                             (uint64_t)idx->work.ptr, idx->work.bytes, (uint64_t)idx->dist_buf.ptr,
                             idx->dist_buf.bytes, P.n_list, P.sub_lists, P.exps0, P.lut_fp16, P.coarse_bf16,
-                            P.scan_cpt, P.scan_chunk, P.filter_dim, 0};
+                            P.scan_cpt, P.scan_chunk, P.filter_dim, P.learned};
     std::memcpy(key, v, sizeof(v));
 }
 
@@ -1787,6 +1803,27 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     CK(cudaStreamWaitEvent(st, g->ev_out, 0));
     g->last = *hit;
     g->pending = true;
+}
+
+void query_features(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
+                    uint32_t label_cols, const uint32_t* d_k, uint32_t k_max, float* d_feats, cudaStream_t st) {
+    HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
+    HDG_REQUIRE(q > 0 && q < (1ull << 31), HDG_ERR_INVALID_ARG, "query count out of range");
+    HDG_REQUIRE(d_queries && d_query_labels && d_feats, HDG_ERR_INVALID_ARG, "null pointer");
+    const IndexDev& D = idx->dev;
+    const int fd = (int)std::max<uint64_t>(1, idx->params.filter_dim);
+    HDG_REQUIRE(label_cols == (uint32_t)(D.l * fd), HDG_ERR_INVALID_ARG,
+                "query label columns must equal l * filter_dim");
+    const uint64_t kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
+    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) reserve_workspace(idx, q, kcand);
+    Workspace w = carve(idx, q, kcand, true);
+    const FilterDev f = filter_dev(idx);
+    const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
+    if (sm_pro > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_prologue, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_pro));
+    k_prologue<<<(unsigned)q, kThreads, sm_pro, st>>>(D, idx->grid, f, d_query_labels, (int)label_cols, w);
+    CK_LAUNCH();
+    learned_features(idx, d_queries, q, w.box, w.cluster_counts, d_k, k_max, d_feats, st);
 }
 
 void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,

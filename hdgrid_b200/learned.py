@@ -1,0 +1,124 @@
+"""Learned per-query schedule: labels from running the plain method, GPU training, evaluation.
+
+Labelling follows the method itself: every training query is run through the index at each
+probe count of ``PROBES`` under both schedules (0 = the index's own post-filter schedule,
+Super-Grid-IVF_PQ.cu:1151-1241; 1 = predicate-first scan with an exact re-rank), and is
+labelled with the cheapest setting -- fewest bytes scanned -- whose recall@k against the
+exact filtered kNN reaches ``target``; when none does, the setting with the best recall.
+The MLP (48 -> 128 -> 128 -> 2, BF16, trained by the library's own kernels) regresses
+log2(probe count) and classifies the schedule.  The plain schedule stays the fallback
+(LEARNED=0) and, with the brute-force kNN, the judge of the learned schedule's recall.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PROBES = (1, 2, 4, 8, 16, 32, 64, 128, 256)
+INV = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def per_query_recall(found: np.ndarray, gt: np.ndarray, ks: np.ndarray) -> np.ndarray:
+    """recall@k of each query (k from ks) with UINT64_MAX entries ignored; 1.0 when the
+    query has no valid ground truth."""
+    out = np.ones(found.shape[0])
+    for i in range(found.shape[0]):
+        k = int(ks[i])
+        g = gt[i, :k]
+        g = set(g[g != INV].tolist())
+        if g:
+            f = found[i, :k]
+            out[i] = len(g.intersection(f[f != INV].tolist())) / len(g)
+    return out
+
+
+def micro_recall(found, gt, ks) -> float:
+    hits = tot = 0
+    for i in range(found.shape[0]):
+        k = int(ks[i])
+        g = gt[i, :k]
+        g = set(g[g != INV].tolist())
+        f = found[i, :k]
+        hits += len(g.intersection(f[f != INV].tolist()))
+        tot += len(g)
+    return hits / tot if tot else 1.0
+
+
+class Batch:
+    """Device-resident query batch plus the output buffers of width k_max."""
+
+    def __init__(self, base, queries, query_labels, ks, k_max=100):
+        import torch
+        import hdgrid_b200 as hg
+        dev = base.device
+        self.q = torch.as_tensor(queries, device=dev).contiguous()
+        self.ql = torch.as_tensor(query_labels, device=dev).contiguous()
+        self.ks = np.asarray(ks, dtype=np.uint32)
+        self.k = torch.from_numpy(self.ks).to(dev)
+        self.k_max = k_max
+        self.dist = torch.empty((self.q.shape[0], k_max), dtype=torch.float32, device=dev)
+        self.ids = torch.empty((self.q.shape[0], k_max), dtype=torch.int64, device=dev)
+        self.qin = hg.query_input_t(base, self.q, self.ql)
+        self.qout = hg.query_output_t(self.dist, self.ids)
+
+    def run(self, idx, n_probe=None, schedule=None):
+        """Query through hdg_query_ex; returns (ids [q x k_max] u64, scanned candidates [q])."""
+        import torch
+        idx.query_ex(self.qin, self.qout, k=self.k, n_probe=n_probe, schedule=schedule)
+        torch.cuda.synchronize()
+        cand = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].copy()
+        return self.ids.cpu().numpy().view(np.uint64).copy(), cand
+
+
+def scan_bytes(cand: np.ndarray, schedule: int, m: int, l: int) -> np.ndarray:
+    """Bytes the ADC scan reads: M code bytes per candidate, plus 4*l label bytes when the
+    predicate runs inside the scan."""
+    return cand.astype(np.float64) * (m + (4 * l if schedule else 0))
+
+
+def label_queries(idx, batch: Batch, gt: np.ndarray, probes=PROBES, target: float = 0.95, schedules=(0, 1)):
+    """Per-query labels y [q x 2] = (log2 probe count, schedule) and the recall / cost tables."""
+    import torch
+    info = idx.info()
+    m, l = info["M"], info["l"]
+    nq = batch.q.shape[0]
+    dev = batch.q.device
+    rec = np.zeros((len(schedules), len(probes), nq))
+    cost = np.zeros((len(schedules), len(probes), nq))
+    for si, s in enumerate(schedules):
+        sch = torch.full((nq,), s, dtype=torch.uint8, device=dev)
+        for pi, p in enumerate(probes):
+            npb = torch.full((nq,), p, dtype=torch.uint32, device=dev)
+            ids, cand = batch.run(idx, n_probe=npb, schedule=sch)
+            rec[si, pi] = per_query_recall(ids, gt, batch.ks)
+            cost[si, pi] = scan_bytes(cand, s, m, l)
+    y = np.zeros((nq, 2), np.float32)
+    for i in range(nq):
+        ok = rec[:, :, i] >= target
+        if ok.any():
+            c = np.where(ok, cost[:, :, i], np.inf)
+            si, pi = np.unravel_index(np.argmin(c), c.shape)
+        else:
+            best = rec[:, :, i].max()
+            c = np.where(rec[:, :, i] >= best - 1e-12, cost[:, :, i], np.inf)
+            si, pi = np.unravel_index(np.argmin(c), c.shape)
+        y[i, 0] = np.log2(probes[pi])
+        y[i, 1] = schedules[si]
+    return y, {"recall": rec, "cost": cost}
+
+
+def train(idx, feats, y, epochs=60, batch=512, lr=2e-3, seed=1, init=True) -> float:
+    """Trains the index's MLP on (features, labels) with the library's GPU kernels."""
+    import torch
+    dev = feats.device
+    yt = torch.as_tensor(y, dtype=torch.float32, device=dev).contiguous()
+    if init:
+        idx.mlp_init(seed)
+    return idx.mlp_train(feats, yt, epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+
+def predicted_settings(idx, feats, max_probe: int):
+    """Per-query (probe count, schedule) the trained network gives, as the query path
+    derives them (round(2^z0) clamped to [1, max_probe], z1 > 0)."""
+    z = idx.mlp_forward(feats).cpu().numpy()
+    p = np.clip(np.rint(np.exp2(np.clip(z[:, 0], 0, 20))), 1, max_probe).astype(np.uint32)
+    return p, (z[:, 1] > 0).astype(np.uint8)

@@ -81,6 +81,8 @@ typedef struct hdg_params {
                              * [4096, 262144]; 0 = 32768) -- the list/query split of the scan */
     uint64_t query_graph;   /* QUERY_GRAPH: 1 = hdg_query replays a captured CUDA graph per
                              * (pointers, q, k); status of a replay via hdg_query_status */
+    uint64_t learned;       /* LEARNED: 1 = per-query lists to probe and predicate-first flag
+                             * from the index's trained MLP (hdg_mlp_*); 0 = plain schedule */
 } hdg_params;
 
 /* filter.conf contents (config_utils.h:112-172).  interval_map is the flat
@@ -148,6 +150,35 @@ hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q,
                         const float* d_query_labels, uint32_t label_cols, const float* d_data,
                         uint32_t k_max, const uint32_t* d_k, const uint32_t* d_nprobe,
                         const uint8_t* d_schedule, float* d_dist, uint64_t* d_ids, void* stream);
+
+/* ---- learned per-query schedule (no reference counterpart) ------------------------------
+ * A BF16 MLP, 48 features -> 128 -> 128 -> 2 (ReLU), whose outputs are z0 = log2(lists to
+ * probe) and z1 = logit of the predicate-first flag.  With LEARNED=1 and a model loaded,
+ * hdg_query / hdg_query_ex (without their own n_probe / schedule arrays) take each query's
+ * probe count round(2^z0) clamped to [1, sub_lists] and schedule (z1 > 0) from it; it
+ * replaces the batch-wide n_list / sub_lists of super_grid::index::query
+ * (Super-Grid-IVF_PQ.cu:1034-1042, 849-901) per query.  Weights are one f32 vector:
+ * W1 [128 x 48], b1 [128], W2 [128 x 128], b2 [128], W3 [2 x 128], b3 [2]. */
+
+/* The 48 features of each query ([q x 48] f32 device output); d_k may be NULL (k_max). */
+hdg_status hdg_query_features(hdg_index* index, const float* d_queries, uint64_t q,
+                              const float* d_query_labels, uint32_t label_cols, const uint32_t* d_k,
+                              uint32_t k_max, float* d_features, void* stream);
+uint64_t hdg_mlp_param_count(void);
+hdg_status hdg_mlp_init(hdg_index* index, uint64_t seed);  /* He-uniform weights, zero biases */
+hdg_status hdg_mlp_set_weights(hdg_index* index, const float* host, uint64_t count);
+hdg_status hdg_mlp_get_weights(hdg_index* index, float* host, uint64_t count);
+/* d_z [n x 2] = network outputs for d_x [n x 48] (device pointers). */
+hdg_status hdg_mlp_forward(hdg_index* index, const float* d_x, uint64_t n, float* d_z, void* stream);
+/* Gradient of the mean loss (z0 - y0)^2 + BCE(sigmoid(z1), y1) over the n rows, w.r.t. all
+ * parameters, into d_grad [hdg_mlp_param_count()] (device); loss (may be NULL) gets the loss. */
+hdg_status hdg_mlp_gradients(hdg_index* index, const float* d_x, const float* d_y, uint64_t n,
+                             float* d_grad, double* loss, void* stream);
+/* Adam (beta 0.9 / 0.999) over shuffled mini-batches of the n rows for the given epochs;
+ * final_loss (may be NULL) gets the last epoch's mean batch loss. */
+hdg_status hdg_mlp_train(hdg_index* index, const float* d_x, const float* d_y, uint64_t n,
+                         uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
+                         double* final_loss, void* stream);
 
 /* Scalars of the last hdg_query: out[0] queries, [1] candidate budget n_cand as the
  * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget actually used (capped by the
