@@ -91,6 +91,136 @@ __device__ __forceinline__ uint64_t morton_encode(const int* coords, int dims, i
     return code;
 }
 
+// ---- Morton decode and the next in-box code (zorder.cu:17-34, 83-243) -----------------
+__device__ __forceinline__ void morton_decode(uint64_t code, int* coords, int dims, int max_bits, int valid_map) {
+    const int active = __popc(valid_map);
+    for (int i = 0; i < dims; ++i) coords[i] = 0;
+    for (int b = 0; b < max_bits; ++b) {
+        int j = 0;
+        for (int i = 0; i < dims; ++i) {
+            if (!((valid_map >> i) & 1)) continue;
+            const int shift = (max_bits - 1 - b) * active + (active - 1 - j);
+            coords[i] |= (int)((code >> shift) & 1) << (max_bits - 1 - b);
+            j++;
+        }
+    }
+}
+
+// box: [lo, hi] cell pairs of every dim (masked dims included, as the reference checks them)
+__device__ __forceinline__ bool cells_in_box(const int* c, const int* box, int dims) {
+    for (int i = 0; i < dims; ++i)
+        if (c[i] < box[2 * i] || c[i] > box[2 * i + 1]) return false;
+    return true;
+}
+
+__device__ __forceinline__ int with_low_bits(int target, int source, int k) {
+    const uint64_t m = (1ull << k) - 1;
+    return (int)(((uint64_t)(int64_t)target & ~m) | ((uint64_t)(int64_t)source & m));
+}
+
+// The smallest code the reference's getNextZValueBaseline (zorder.cu:83-243) jumps to from
+// cur: cur + 1 when that decodes inside the box; otherwise the lowest violating bit of
+// cur + 1 is carried per its left/right-violation rules.  Returns false when no jump
+// exists.  The steps, including which bits count as "safe", are the reference's; the
+// result decides which candidate sub-ranges exist, so it has to match bit for bit.
+__device__ inline bool next_code_in_box(uint64_t cur, const int* box, int dims, int max_bits, int valid_map,
+                                        uint64_t* next) {
+    const uint64_t nisp = cur + 1;
+    int c[kMaxDims];
+    morton_decode(nisp, c, dims, max_bits, valid_map);
+    if (cells_in_box(c, box, dims)) {
+        *next = nisp;
+        return true;
+    }
+    const int active = __popc(valid_map);
+    int flag[kMaxDims], out_step[kMaxDims], save_min[kMaxDims], save_max[kMaxDims], vdim[kMaxDims];
+    int j = 0;
+    for (int i = 0; i < dims; ++i) {
+        flag[i] = 0;
+        if (!((valid_map >> i) & 1)) continue;
+        vdim[j++] = i;
+        out_step[i] = save_min[i] = save_max[i] = max_bits;
+        for (int s = 0; s < max_bits; ++s) {  // first differing bit against the low corner
+            const int sh = max_bits - 1 - s;
+            const int lb = (box[2 * i] >> sh) & 1, cb = (c[i] >> sh) & 1;
+            if (cb < lb) {
+                flag[i] = -1;
+                out_step[i] = s;
+                break;
+            }
+            if (cb > lb) break;
+        }
+        if (flag[i] == 0) {
+            for (int s = 0; s < max_bits; ++s) {  // ... and against the high corner
+                const int sh = max_bits - 1 - s;
+                const int hb = (box[2 * i + 1] >> sh) & 1, cb = (c[i] >> sh) & 1;
+                if (cb > hb) {
+                    flag[i] = 1;
+                    out_step[i] = s;
+                    break;
+                }
+                if (cb < hb) break;
+            }
+        }
+        if (flag[i] != -1) {
+            for (int s = 0; s < max_bits; ++s) {
+                const int sh = max_bits - 1 - s;
+                if (((c[i] >> sh) & 1) > ((box[2 * i] >> sh) & 1)) {
+                    save_min[i] = s;
+                    break;
+                }
+            }
+        }
+        if (flag[i] != 1) {
+            for (int s = 0; s < max_bits; ++s) {
+                const int sh = max_bits - 1 - s;
+                if (((c[i] >> sh) & 1) < ((box[2 * i + 1] >> sh) & 1)) {
+                    save_max[i] = s;
+                    break;
+                }
+            }
+        }
+    }
+    int change = 0;
+    j = 0;
+    for (int i = 0; i < dims; ++i) {
+        if (!((valid_map >> i) & 1)) continue;
+        if (out_step[i] < max_bits) change = max(change, (max_bits - 1 - out_step[i]) * active + (active - 1 - j));
+        j++;
+    }
+    int d = vdim[active - 1 - (change % active)];
+    if (flag[d] == 1) {
+        int found = -1;
+        for (int bp = change + 1; bp < max_bits * active; ++bp) {
+            const int a = active - 1 - (bp % active);
+            if (bp <= (max_bits - 1 - save_max[vdim[a]]) * active + (active - 1 - a) && ((nisp >> bp) & 1ull) == 0) {
+                found = bp;
+                break;
+            }
+        }
+        if (found < 0) return false;
+        change = found;
+        d = vdim[active - 1 - (change % active)];
+        save_min[d] = max_bits - 1 - (change / active);
+        flag[d] = 0;
+    }
+    const int blocks = change / active;
+    j = 0;
+    for (int i = 0; i < dims; ++i) {
+        if (!((valid_map >> i) & 1)) continue;
+        if (flag[i] >= 0) {
+            const int bits = blocks + (vdim[j] > d ? 1 : 0);
+            c[i] = change <= (max_bits - 1 - save_min[i]) * active + (active - 1 - j) ? with_low_bits(c[i], 0, bits)
+                                                                                    : with_low_bits(c[i], box[2 * i], bits);
+        } else {
+            c[i] = box[2 * i];
+        }
+        j++;
+    }
+    *next = morton_encode(c, dims, max_bits, valid_map) | (1ull << change);
+    return true;
+}
+
 // ---- distances --------------------------------------------------------------------
 // Exact f32 L2 in the reference's order (refine.cu:71-88 with d <= 512): each squared
 // difference rounded to f32, then summed sequentially in dimension order.

@@ -79,6 +79,8 @@ struct Workspace {
     int mode;                // batch schedule: 0 pre-filter (exps0 <= 1), 1 post-filter, 2 single dim
     uint32_t exps0;
     uint32_t chunk;          // candidates per scan work item
+    int is_split;            // IS_SPLIT: trimmed Morton sub-ranges per probed list
+    int nsplit;              // sub-ranges per probed list (n_split when is_split, else 1)
     uint64_t cap;            // distance-buffer capacity in candidates
 };
 
@@ -275,6 +277,47 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* __restrict__
     return lo;
 }
 
+// One sub-range of a probed list's Morton interval [lo, hi) when is_split = 1.
+// get_query_end_points_kernel (zorder.cu:596-654) cuts the interval into
+// min(len, n_split) near-equal parts; zorder_range_query_kernel (:474-594) then moves each
+// part's start forward by up to three next-in-box jumps and drops the part when a jump fails
+// or lands past the part's last code.  (The reference reads the probed list as
+// candidates[c] instead of candidates[q * n + c], :500; the list of this query is used.)
+// Empty parts get start kInvalid.
+__device__ void split_subrange(const uint64_t* __restrict__ z, uint32_t off, uint32_t lo, uint32_t hi, int s,
+                               int ns, const int* box, const GridMeta& g, uint32_t* start, uint32_t* len) {
+    const uint32_t n = hi - lo;
+    const uint32_t nsp = min(n, (uint32_t)ns);
+    if (n == 0 || (uint32_t)s >= nsp) {
+        *start = kInvalid;
+        *len = 0;
+        return;
+    }
+    const uint32_t qn = n / nsp, r = n % nsp;
+    uint32_t a = off + lo + (uint32_t)s * qn + min((uint32_t)s, r);
+    const uint32_t b = a + qn + ((uint32_t)s < r ? 1u : 0u);
+    const uint64_t zmax = z[b - 1];
+    uint64_t cur = z[a];
+    bool valid = true;
+    for (int jump = 0; jump < 3; jump++) {
+        const uint32_t idx = a + lower_bound_u64(z + a, b - a, cur);
+        if (idx >= b) break;
+        a = idx;
+        int c[kMaxDims];
+        morton_decode(z[idx], c, g.morton_dims, g.morton_max_bits, g.morton_valid_map);
+        if (cells_in_box(c, box, g.morton_dims)) break;
+        uint64_t nz = 0;
+        if (!next_code_in_box(z[idx], box, g.morton_dims, g.morton_max_bits, g.morton_valid_map, &nz) || nz >= zmax) {
+            valid = false;
+            break;
+        }
+        cur = nz;
+    }
+    *start = a;
+    *len = valid ? b - a : 0;
+}
+
+
 // Band [lo, hi] around the exact f32 distance of query qi to centroid col (clusters first,
 // then lists) from the tensor-core dot product S: |(|q|^2 + |c|^2 - 2 q.c) - exact| is below
 // 2 * 2^-8 |q||c| for BF16-rounded inputs, plus f32 rounding of the norms and sums; the band
@@ -288,7 +331,7 @@ __device__ __forceinline__ void approx_band(const IndexDev& D, const Workspace& 
     *hi = a + e;
 }
 
-__global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __restrict__ queries,
+__global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, const float* __restrict__ queries,
                                                      int Pc, int Ps, int sort_n1, int sort_n2,
                                                      Workspace w) {
     extern __shared__ uint64_t s_keys[];  // [max(sort_n1, sort_n2)] then query vector
@@ -420,21 +463,37 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, const float* __
     block_bitonic_sort(s_keys, sort_n3);
     const uint64_t zlo = w.zrange[qi * 2], zhi = w.zrange[qi * 2 + 1];
     uint32_t my_cand = 0, my_exact = 0;
+    const int ns = w.nsplit;
+    int box[2 * kMaxDims];
+    if (w.is_split)
+        for (int i = 0; i < 2 * g.l; i++) box[i] = w.cells[qi * 2 * g.l + i];
     for (int i = t; i < Ps; i += blockDim.x) {
-        uint32_t list = kInvalid, start = 0, len = 0;
+        uint32_t list = kInvalid, start = 0, len = 0, off = 0, lo = 0, hi = 0;
         if (i < nps) {
             list = (uint32_t)s_keys[i];
-            const uint32_t off = D.list_off[list], size = D.list_off[list + 1] - off;
-            const uint32_t lo = lower_bound_u64(D.zcodes + off, size, zlo);
-            const uint32_t hi = lower_bound_u64(D.zcodes + off, size, zhi + 1);
+            off = D.list_off[list];
+            const uint32_t size = D.list_off[list + 1] - off;
+            lo = lower_bound_u64(D.zcodes + off, size, zlo);
+            hi = lower_bound_u64(D.zcodes + off, size, zhi + 1);
             start = off + lo;
             len = hi - lo;
-            my_cand += len;
             my_exact += w.list_counts[qi * D.n_lists + list];
         }
         w.probe_lists[qi * Ps + i] = list;
-        w.range_start[qi * Ps + i] = start;
-        w.range_len[qi * Ps + i] = len;
+        const uint64_t r0 = (qi * Ps + i) * (uint64_t)ns;
+        if (!w.is_split) {
+            w.range_start[r0] = start;
+            w.range_len[r0] = len;
+            my_cand += len;
+        } else {
+            for (int sp = 0; sp < ns; sp++) {
+                uint32_t st = kInvalid, ln = 0;
+                if (i < nps) split_subrange(D.zcodes, off, lo, hi, sp, ns, box, g, &st, &ln);
+                w.range_start[r0 + sp] = st;
+                w.range_len[r0 + sp] = ln;
+                my_cand += ln;
+            }
+        }
     }
     atomicAdd(&s_red[0], my_cand);
     atomicAdd(&s_red[1], my_exact);
@@ -1319,8 +1378,11 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.cluster_counts = (uint32_t*)take("cluster_counts", q * C * 4);
     w.probe_clusters = (uint32_t*)take("probe_clusters", q * Pc * 4);
     w.probe_lists = (uint32_t*)take("probe_lists", q * Ps * 4);
-    w.range_start = (uint32_t*)take("range_start", q * Ps * 4);
-    w.range_len = (uint32_t*)take("range_len", q * Ps * 4);
+    const uint64_t ns = P.is_split ? std::max<uint64_t>(1, P.n_split) : 1;
+    w.range_start = (uint32_t*)take("range_start", q * Ps * ns * 4);
+    w.range_len = (uint32_t*)take("range_len", q * Ps * ns * 4);
+    w.is_split = P.is_split ? 1 : 0;
+    w.nsplit = (int)ns;
     w.qstat = (uint32_t*)take("qstat", q * 4 * 4);
     w.scal = (uint64_t*)take("scalars", 8 * 8);
     w.qoff = (uint64_t*)take("qoff", (q + 1) * 8);
@@ -1604,7 +1666,7 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     } else {
         w.S = nullptr;
     }
-    k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, c.queries, Pc, Ps, sort_n1, sort_n2, w);
+    k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, idx->grid, c.queries, Pc, Ps, sort_n1, sort_n2, w);
     CK_LAUNCH();
     launches++;
     tm.mark("coarse");
@@ -1650,7 +1712,9 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     }
 
     const int pre = mode == kPre ? 1 : 0;
-    const size_t sm_tab = sizeof(uint32_t) * (2 * Ps + 1);
+    // candidate ranges per query: one per probed list, or n_split per list when is_split
+    const int R = Ps * w.nsplit;
+    const size_t sm_tab = sizeof(uint32_t) * (2 * R + 1);
     if (!sync_sizing || sc[3] > 0) {
         if (fast) {
             const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
@@ -1658,7 +1722,7 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
-                kern<<<blocks, nt, sm, st>>>(D, c.queries, Ps, pre, l, q, w);
+                kern<<<blocks, nt, sm, st>>>(D, c.queries, R, pre, l, q, w);
             };
             // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
             const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
@@ -1680,7 +1744,7 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             CK(cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             const int blocks = sm_count() * occupancy_blocks(k_scan_generic, 512, sm);
-            k_scan_generic<<<blocks, 512, sm, st>>>(D, (int)G, Ps, pre, l, q, w);
+            k_scan_generic<<<blocks, 512, sm, st>>>(D, (int)G, R, pre, l, q, w);
         }
         CK_LAUNCH();
         launches++;
@@ -1691,7 +1755,7 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     const size_t sm_sel = sizeof(uint32_t) * kBins + sizeof(uint64_t) * kBCap +
                           (sorted_out ? sizeof(uint64_t) * next_pow2(std::max<uint32_t>(k, 2)) : 0) + sm_tab + 16;
     CK(cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_sel));
-    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, Ps, (int)k, sorted_out, w, c.dist, c.ids, (int)k);
+    k_select<<<(unsigned)q, kSelThreads, sm_sel, st>>>(D, R, (int)k, sorted_out, w, c.dist, c.ids, (int)k);
     CK_LAUNCH();
     launches++;
     tm.mark("select");
@@ -1731,7 +1795,7 @@ static void make_graph_key(const hdg_index* idx, const QueryCall& c, uint64_t* k
                             (uint64_t)c.dist, (uint64_t)c.ids, (uint64_t)c.qk, (uint64_t)c.qps, (uint64_t)c.qsched,
                             (uint64_t)idx->work.ptr, idx->work.bytes, (uint64_t)idx->dist_buf.ptr,
                             idx->dist_buf.bytes, P.n_list, P.sub_lists, P.exps0, P.lut_fp16, P.coarse_bf16,
-                            P.scan_cpt, P.scan_chunk, P.filter_dim, P.learned};
+                            P.scan_cpt, P.scan_chunk, P.filter_dim, P.learned | (P.is_split << 8) | (P.n_split << 16)};
     std::memcpy(key, v, sizeof(v));
 }
 

@@ -124,13 +124,17 @@ def config3(scale: float = 1.0, n_queries: int = 10_000, **conf):
     return ws
 
 
-def config4(scale: float = 1.0, n_queries: int = 100_000, **conf):
+def config4(scale: float = 1.0, n_queries: int = 100_000, query_seed: int = SEED_QUERY,
+            filter_seed: int = SEED_FILTER, with_base: bool = True, **conf):
+    """query_seed / filter_seed select an independent query stream of the same distribution
+    (the learned schedule trains on one and is evaluated on the standard one);
+    with_base=False skips the base set and its labels (None)."""
     n = max(8000, int(10_000_000 * scale))
-    base = mixture(n, 128, 1024, SEED_BASE)
-    queries = mixture(n_queries, 128, 1024, SEED_QUERY)
+    base = mixture(n, 128, 1024, SEED_BASE) if with_base else None
+    queries = mixture(n_queries, 128, 1024, query_seed)
     lrng = np.random.default_rng(SEED_LABEL)
-    labels = lrng.integers(0, 1_000_000, size=(n, 4)).astype(np.float32)
-    frng = np.random.default_rng(SEED_FILTER)
+    labels = lrng.integers(0, 1_000_000, size=(n, 4)).astype(np.float32) if with_base else None
+    frng = np.random.default_rng(filter_seed)
     sel = np.exp(frng.uniform(np.log(0.0001), np.log(0.9), size=n_queries))
     ql = np.zeros((n_queries, 8), np.float32)
     ql[:, 1::2] = 1_000_000
@@ -150,6 +154,16 @@ def config4(scale: float = 1.0, n_queries: int = 100_000, **conf):
     c.update(conf)
     return dict(name="config4", base=base, labels=labels, queries=queries, query_labels=ql,
                 hdgrid_conf=hdgrid_conf(**c), filter_conf=filt, k=int(c["topk"]), selectivity=sel, ks=ks)
+
+
+def config5(scale: float = 1.0, n_queries: int = 50_000, **conf):
+    """The learned variant: config4's data and queries with the index set up for per-query
+    probe counts up to 256 lists (n_list 64 clusters of 8 lists) and exps0 16."""
+    c = dict(n_list=64, sub_lists=256, exps0=16)
+    c.update(conf)
+    ws = config4(scale=scale, n_queries=n_queries, **c)
+    ws["name"] = "config5"
+    return ws
 
 
 def recall(found_ids: np.ndarray, gt_ids: np.ndarray) -> float:

@@ -17,30 +17,34 @@ PROBES = (1, 2, 4, 8, 16, 32, 64, 128, 256)
 INV = np.uint64(0xFFFFFFFFFFFFFFFF)
 
 
+def _hits(found: np.ndarray, gt: np.ndarray, ks: np.ndarray):
+    """Per query: |found[:k] & gt[:k]| and |valid gt[:k]| (UINT64_MAX entries ignored; the
+    ids of one result row are distinct)."""
+    n, w = gt.shape
+    col = np.arange(w)[None, :]
+    hits = np.zeros(n, np.int64)
+    tot = np.zeros(n, np.int64)
+    for a in range(0, n, 2048):
+        b = min(n, a + 2048)
+        keep = col < ks[a:b, None].astype(np.int64)
+        g = np.where(keep, gt[a:b], INV)
+        f = np.where(keep[:, :found.shape[1]], found[a:b, :w], INV - np.uint64(1))
+        valid = g != INV
+        hits[a:b] = ((f[:, :, None] == g[:, None, :]) & valid[:, None, :]).any(2).sum(1)
+        tot[a:b] = valid.sum(1)
+    return hits, tot
+
+
 def per_query_recall(found: np.ndarray, gt: np.ndarray, ks: np.ndarray) -> np.ndarray:
-    """recall@k of each query (k from ks) with UINT64_MAX entries ignored; 1.0 when the
-    query has no valid ground truth."""
-    out = np.ones(found.shape[0])
-    for i in range(found.shape[0]):
-        k = int(ks[i])
-        g = gt[i, :k]
-        g = set(g[g != INV].tolist())
-        if g:
-            f = found[i, :k]
-            out[i] = len(g.intersection(f[f != INV].tolist())) / len(g)
-    return out
+    """recall@k of each query (k from ks); 1.0 when the query has no valid ground truth."""
+    h, t = _hits(found, gt, ks)
+    return np.where(t > 0, h / np.maximum(t, 1), 1.0)
 
 
 def micro_recall(found, gt, ks) -> float:
-    hits = tot = 0
-    for i in range(found.shape[0]):
-        k = int(ks[i])
-        g = gt[i, :k]
-        g = set(g[g != INV].tolist())
-        f = found[i, :k]
-        hits += len(g.intersection(f[f != INV].tolist()))
-        tot += len(g)
-    return hits / tot if tot else 1.0
+    """sum of hits / sum of valid ground-truth ids (the reference's recall denominator)."""
+    h, t = _hits(found, gt, ks)
+    return float(h.sum() / t.sum()) if t.sum() else 1.0
 
 
 class Batch:

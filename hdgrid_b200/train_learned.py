@@ -1,0 +1,131 @@
+"""Train the learned per-query schedule for the 10M x 128 workload and evaluate it.
+
+    python -m hdgrid_b200.train_learned [--scale 1.0] [--train 200000] [--heldout 50000]
+        [--out hdgrid_b200/learned_weights/config5.npy]
+
+Builds the config5 index (config4's data: 10M x 128, 4 label dims, range filters), labels
+``--train`` queries of an independent query stream (query seed 2002, filter seed 2004) by
+running the plain method at every probe count under both schedules, trains the BF16 MLP
+on the GPU, and evaluates on ``--heldout`` queries of the standard stream: recall@k
+against the exact filtered kNN and bytes scanned, for the plain schedule at every uniform
+probe count and for the learned schedule.  Writes the weights (.npy, f32) and a JSON
+report next to them.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+
+def _gt(hg, base, labels, q, ql, filter_conf, k, step=10_000):
+    import torch
+    out = np.empty((q.shape[0], k), np.uint64)
+    for a in range(0, q.shape[0], step):
+        b = min(q.shape[0], a + step)
+        rng = torch.empty((b - a, 2 * labels.shape[1]), device=base.device)
+        hg.recover_filters(filter_conf, ql[a:b].contiguous(), rng)
+        gd = torch.empty((b - a, k), device=base.device)
+        gi = torch.empty((b - a, k), dtype=torch.int64, device=base.device)
+        hg.bruteforce_knn(base, labels, q[a:b].contiguous(), rng, k, gd, gi)
+        out[a:b] = gi.cpu().numpy().view(np.uint64)
+    return out
+
+
+def main():
+    import torch
+    import hdgrid_b200 as hg
+    from hdgrid_b200 import datasets
+    from hdgrid_b200 import learned as L
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--train", type=int, default=200_000)
+    ap.add_argument("--heldout", type=int, default=50_000)
+    ap.add_argument("--target", type=float, default=0.97, help="per-query recall a label must reach")
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--step", type=int, default=10_000, help="queries per labelling / evaluation batch")
+    ap.add_argument("--out", default=str(Path(__file__).resolve().parent / "learned_weights" / "config5.npy"))
+    args = ap.parse_args()
+    dev = torch.device("cuda:0")
+    t0 = time.time()
+    ev = datasets.config5(scale=args.scale, n_queries=args.heldout, break_down=0)
+    tr = datasets.config4(scale=args.scale, n_queries=args.train, query_seed=2002, filter_seed=2004,
+                          with_base=False)
+    idx = hg.SuperGridIndex.from_text(ev["hdgrid_conf"], ev["filter_conf"])
+    base = torch.from_numpy(ev["base"]).to(dev)
+    labels = torch.from_numpy(ev["labels"]).to(dev)
+    idx.build(hg.build_input_t(base, labels))
+    torch.cuda.synchronize()
+    log = {"build_s": round(time.time() - t0, 1)}
+    print(json.dumps(log), flush=True)
+
+    qtr = torch.from_numpy(tr["queries"]).to(dev)
+    qltr = torch.from_numpy(tr["query_labels"]).to(dev)
+    kstr = tr["ks"].astype(np.uint32)
+    t1 = time.time()
+    gt_tr = _gt(hg, base, labels, qtr, qltr, ev["filter_conf"], 100)
+    log["gt_train_s"] = round(time.time() - t1, 1)
+    ys, feats = [], []
+    t1 = time.time()
+    for a in range(0, qtr.shape[0], args.step):
+        b = min(qtr.shape[0], a + args.step)
+        batch = L.Batch(base, qtr[a:b], qltr[a:b], kstr[a:b])
+        y, _ = L.label_queries(idx, batch, gt_tr[a:b], target=args.target)
+        ys.append(y)
+        feats.append(idx.query_features(batch.q, batch.ql, 100, k=batch.k))
+    y = np.concatenate(ys)
+    f = torch.cat(feats).contiguous()
+    log["label_s"] = round(time.time() - t1, 1)
+    log["label_pre_share"] = float(y[:, 1].mean())
+    log["label_probe_hist"] = np.bincount(y[:, 0].astype(int), minlength=9).tolist()
+    t1 = time.time()
+    loss = L.train(idx, f, y, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=1)
+    log["train_s"] = round(time.time() - t1, 1)
+    log["train_loss"] = loss
+    print(json.dumps(log), flush=True)
+
+    # held-out evaluation
+    qev = torch.from_numpy(ev["queries"]).to(dev)
+    qlev = torch.from_numpy(ev["query_labels"]).to(dev)
+    ksev = ev["ks"].astype(np.uint32)
+    gt_ev = _gt(hg, base, labels, qev, qlev, ev["filter_conf"], 100)
+    info = idx.info()
+    plain = {p: [0, 0, 0.0] for p in L.PROBES}
+    learned = [0, 0, 0.0]
+    for a in range(0, qev.shape[0], args.step):
+        b = min(qev.shape[0], a + args.step)
+        batch = L.Batch(base, qev[a:b], qlev[a:b], ksev[a:b])
+        for p in L.PROBES:
+            idx.set_param("sub_lists", p)
+            ids, cand = batch.run(idx)
+            h, t = L._hits(ids, gt_ev[a:b], batch.ks)
+            plain[p][0] += int(h.sum())
+            plain[p][1] += int(t.sum())
+            plain[p][2] += float(L.scan_bytes(cand, 0, info["M"], info["l"]).sum())
+        idx.set_param("sub_lists", 256)
+        fe = idx.query_features(batch.q, batch.ql, 100, k=batch.k)
+        pp, ff = L.predicted_settings(idx, fe, 256)
+        idx.set_param("learned", 1)
+        ids, cand = batch.run(idx)
+        idx.set_param("learned", 0)
+        h, t = L._hits(ids, gt_ev[a:b], batch.ks)
+        learned[0] += int(h.sum())
+        learned[1] += int(t.sum())
+        learned[2] += float((cand * np.where(ff == 1, info["M"] + 4 * info["l"], info["M"])).sum())
+    report = dict(log, heldout=args.heldout, train=args.train,
+                  plain=[{"sub_lists": p, "recall": v[0] / max(v[1], 1), "scan_bytes": v[2]} for p, v in plain.items()],
+                  learned={"recall": learned[0] / max(learned[1], 1), "scan_bytes": learned[2]})
+    out = Path(args.out)
+    out.parent.mkdir(parents=True, exist_ok=True)
+    np.save(out, idx.mlp_weights())
+    out.with_name(out.stem + "_report.json").write_text(json.dumps(report, indent=1))
+    print(json.dumps(report), flush=True)
+
+
+if __name__ == "__main__":
+    main()

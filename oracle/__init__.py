@@ -169,11 +169,11 @@ class OracleIndex:
         self._h = LIB.ora_open(str(path).encode())
         if not self._h:
             raise IOError(LIB.ora_last_error().decode())
-        info = np.zeros(15, np.uint64)
+        info = np.zeros(17, np.uint64)
         LIB.ora_info(self._h, _p(info))
         (self.n, self.d, self.l, self.M, self.M_pad, self.n_lists, self.clusters, self.tot_cells, self.max_bits,
          self.valid_map, self.topk, self.filter_dim, self.exps0, self.n_list,
-         self.sub_lists) = (int(x) for x in info)
+         self.sub_lists, self.is_split, self.n_split) = (int(x) for x in info)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -213,7 +213,8 @@ class OracleIndex:
             t = dict(box=np.zeros((q, 2 * l), np.float32), cells=np.zeros((q, 2 * l), np.int32),
                      zrange=np.zeros((q, 2), np.uint64), list_counts=np.zeros((q, L), np.uint32),
                      probe_clusters=np.zeros((q, n_list), np.uint32), probe_lists=np.zeros((q, sub_lists), np.uint32),
-                     range_start=np.zeros((q, sub_lists), np.uint32), range_len=np.zeros((q, sub_lists), np.uint32),
+                     range_start=np.zeros((q, sub_lists * self.n_split), np.uint32),
+                     range_len=np.zeros((q, sub_lists * self.n_split), np.uint32),
                      scalars=np.zeros(4, np.float64))
             tr = _Trace(*(t[n].ctypes.data for n, _ in _Trace._fields_))
         opt = [None if a is None else _p(a) for a in (qk, n_probe, schedule)]

@@ -136,6 +136,119 @@ uint64_t morton(const int* c, int dims, int max_bits, int valid_map) {
     return code;
 }
 
+// Inverse of morton(): coords of every dim (masked dims 0), zorder.cu:17-34.
+void unmorton(uint64_t code, int* c, int dims, int max_bits, int valid_map) {
+    int active = 0;
+    for (int i = 0; i < dims; i++) active += (valid_map >> i) & 1;
+    for (int i = 0; i < dims; i++) c[i] = 0;
+    for (int b = 0; b < max_bits; b++) {
+        int j = 0;
+        for (int i = 0; i < dims; i++) {
+            if (!((valid_map >> i) & 1)) continue;
+            const int shift = (max_bits - 1 - b) * active + (active - 1 - j);
+            c[i] |= (int)((code >> shift) & 1) << (max_bits - 1 - b);
+            j++;
+        }
+    }
+}
+
+bool in_cell_box(const int* c, const int* box, int dims) {
+    for (int i = 0; i < dims; i++)
+        if (c[i] < box[2 * i] || c[i] > box[2 * i + 1]) return false;
+    return true;
+}
+
+// bit s (0 = most significant of max_bits) of v
+inline int bit_at(int v, int s, int max_bits) { return (v >> (max_bits - 1 - s)) & 1; }
+
+// getNextZValueBaseline (zorder.cu:83-243): the code the reference jumps to from cur.
+bool next_in_box(uint64_t cur, const int* box, int dims, int max_bits, int valid_map, uint64_t* next) {
+    const uint64_t nisp = cur + 1;
+    int c[kMaxDims];
+    unmorton(nisp, c, dims, max_bits, valid_map);
+    if (in_cell_box(c, box, dims)) {
+        *next = nisp;
+        return true;
+    }
+    std::vector<int> act;  // active (unmasked) dims in order
+    for (int i = 0; i < dims; i++)
+        if ((valid_map >> i) & 1) act.push_back(i);
+    const int A = (int)act.size();
+    int flag[kMaxDims] = {0}, step[kMaxDims], smin[kMaxDims], smax[kMaxDims];
+    for (int i : act) {
+        step[i] = smin[i] = smax[i] = max_bits;
+        const int lo = box[2 * i], hi = box[2 * i + 1];
+        for (int s = 0; s < max_bits; s++) {
+            const int cb = bit_at(c[i], s, max_bits), lb = bit_at(lo, s, max_bits);
+            if (cb != lb) {
+                if (cb < lb) {
+                    flag[i] = -1;
+                    step[i] = s;
+                }
+                break;
+            }
+        }
+        if (flag[i] == 0)
+            for (int s = 0; s < max_bits; s++) {
+                const int cb = bit_at(c[i], s, max_bits), hb = bit_at(hi, s, max_bits);
+                if (cb != hb) {
+                    if (cb > hb) {
+                        flag[i] = 1;
+                        step[i] = s;
+                    }
+                    break;
+                }
+            }
+        if (flag[i] != -1)
+            for (int s = 0; s < max_bits; s++)
+                if (bit_at(c[i], s, max_bits) > bit_at(lo, s, max_bits)) {
+                    smin[i] = s;
+                    break;
+                }
+        if (flag[i] != 1)
+            for (int s = 0; s < max_bits; s++)
+                if (bit_at(c[i], s, max_bits) < bit_at(hi, s, max_bits)) {
+                    smax[i] = s;
+                    break;
+                }
+    }
+    // bit position (LSB = 0) of active dim j at step s
+    auto pos = [&](int s, int j) { return (max_bits - 1 - s) * A + (A - 1 - j); };
+    int change = 0;
+    for (int j = 0; j < A; j++)
+        if (step[act[j]] < max_bits) change = std::max(change, pos(step[act[j]], j));
+    int d = act[A - 1 - change % A];
+    if (flag[d] == 1) {
+        int found = -1;
+        for (int bp = change + 1; bp < max_bits * A; bp++) {
+            const int j = A - 1 - bp % A;
+            if (bp <= pos(smax[act[j]], j) && ((nisp >> bp) & 1) == 0) {
+                found = bp;
+                break;
+            }
+        }
+        if (found < 0) return false;
+        change = found;
+        d = act[A - 1 - change % A];
+        smin[d] = max_bits - 1 - change / A;
+        flag[d] = 0;
+    }
+    const int blocks = change / A;
+    for (int j = 0; j < A; j++) {
+        const int i = act[j];
+        if (flag[i] < 0) {
+            c[i] = box[2 * i];
+            continue;
+        }
+        const int k = blocks + (i > d ? 1 : 0);
+        const uint64_t m = (1ull << k) - 1;
+        const uint64_t src = change <= pos(smin[i], j) ? 0 : (uint64_t)(int64_t)box[2 * i];
+        c[i] = (int)(((uint64_t)(int64_t)c[i] & ~m) | (src & m));
+    }
+    *next = morton(c, dims, max_bits, valid_map) | (1ull << change);
+    return true;
+}
+
 // Cell coords of one point (get_grid_ids_kernel, Super-Grid-IVF_PQ.cu:28-52).
 void point_cell(const Grid& g, const float* lab, int* coords) {
     for (int i = 0; i < g.l; i++) {
@@ -172,6 +285,8 @@ struct Index {
     uint64_t n_list() const { return params[8]; }
     uint64_t sub_lists() const { return params[9]; }
     uint64_t lut_fp16() const { return params[20]; }
+    uint64_t n_split() const { return params[10]; }
+    uint64_t is_split() const { return params[12]; }
 };
 
 template <typename T>
@@ -436,7 +551,8 @@ void ora_info(void* h, uint64_t* out) {
     const Index& ix = *static_cast<Index*>(h);
     const uint64_t v[] = {ix.n, ix.d, ix.l, ix.M, ix.M_pad, ix.L, ix.C, ix.g.tot_cells,
                           (uint64_t)ix.g.max_bits, (uint64_t)ix.g.valid_map, ix.topk(), ix.filter_dim(),
-                          ix.exps0(), std::max<uint64_t>(1, ix.n_list()), std::max<uint64_t>(1, ix.sub_lists())};
+                          ix.exps0(), std::max<uint64_t>(1, ix.n_list()), std::max<uint64_t>(1, ix.sub_lists()),
+                          ix.is_split(), ix.is_split() ? std::max<uint64_t>(1, ix.n_split()) : 1};
     std::memcpy(out, v, sizeof(v));
 }
 
@@ -523,6 +639,9 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
     const int Pc = (int)std::max<uint64_t>(1, ix.n_list()), Ps = (int)std::max<uint64_t>(1, ix.sub_lists());
     const uint64_t exps0 = ix.exps0();
     const int mode = exps0 <= 1 ? 0 : (l > 1 ? 1 : 2);  // pre-filter / post-filter / l==1
+    const bool split = ix.is_split() != 0;
+    const int ns = split ? (int)std::max<uint64_t>(1, ix.n_split()) : 1;
+    const int R = Ps * ns;  // candidate ranges per query
     if (threads > 0) omp_set_num_threads(threads);
     struct QState {
         float box[2 * kMaxDims];
@@ -581,8 +700,8 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
         const int nps = std::min<int>(psq, (int)sl.size());
         // the chosen lists in list-id (= pool) order; RAFT select_k returns them unsorted
         std::sort(sl.begin(), sl.begin() + nps, [](const auto& a, const auto& b) { return a.second < b.second; });
-        s.start.assign(Ps, 0);
-        s.len.assign(Ps, 0);
+        s.start.assign((size_t)R, split ? 0xffffffffu : 0u);
+        s.len.assign((size_t)R, 0);
         for (int i = 0; i < nps; i++) {
             const uint32_t j = sl[i].second;
             const uint64_t* zb = &ix.zcodes[ix.list_off[j]];
@@ -590,10 +709,45 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
             // get_query_end_points_no_split_kernel (zorder.cu:656-685)
             const uint32_t a = (uint32_t)(std::lower_bound(zb, ze, zlo) - zb);
             const uint32_t b = (uint32_t)(std::lower_bound(zb, ze, zhi + 1) - zb);
-            s.start[i] = ix.list_off[j] + a;
-            s.len[i] = b - a;
-            s.cand += b - a;
             s.exact += lc[j];
+            if (!split) {
+                s.start[i] = ix.list_off[j] + a;
+                s.len[i] = b - a;
+                s.cand += b - a;
+                continue;
+            }
+            // is_split: near-equal parts (get_query_end_points_kernel, zorder.cu:596-654), each
+            // start moved by up to three next-in-box jumps, the part dropped when a jump fails or
+            // passes its last code (zorder_range_query_kernel, :474-594, indexing this query's
+            // probed list rather than candidates[c] of :500)
+            const uint32_t n = b - a;
+            const uint32_t parts = std::min<uint32_t>(n, (uint32_t)ns);
+            for (uint32_t sp = 0; sp < parts; sp++) {
+                const uint32_t qn = n / parts, rem = n % parts;
+                uint32_t lo = ix.list_off[j] + a + sp * qn + std::min(sp, rem);
+                const uint32_t hi = lo + qn + (sp < rem ? 1 : 0);
+                const uint64_t* z = ix.zcodes.data();
+                const uint64_t zmax = z[hi - 1];
+                uint64_t cur = z[lo];
+                bool ok = true;
+                for (int jump = 0; jump < 3; jump++) {
+                    const uint32_t at = (uint32_t)(std::lower_bound(z + lo, z + hi, cur) - z);
+                    if (at >= hi) break;
+                    lo = at;
+                    int c[kMaxDims];
+                    unmorton(z[at], c, g.mdims, g.max_bits, g.valid_map);
+                    if (in_cell_box(c, cells, g.mdims)) break;
+                    uint64_t nz = 0;
+                    if (!next_in_box(z[at], cells, g.mdims, g.max_bits, g.valid_map, &nz) || nz >= zmax) {
+                        ok = false;
+                        break;
+                    }
+                    cur = nz;
+                }
+                s.start[(size_t)i * ns + sp] = lo;
+                s.len[(size_t)i * ns + sp] = ok ? hi - lo : 0;
+                s.cand += ok ? hi - lo : 0;
+            }
         }
         if (tr) {
             if (tr->box) std::memcpy(tr->box + qi * 2 * l, s.box, sizeof(float) * 2 * l);
@@ -605,10 +759,11 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
             if (tr->list_counts) std::memcpy(tr->list_counts + qi * L, lc.data(), sizeof(uint32_t) * L);
             if (tr->probe_clusters)
                 for (int i = 0; i < Pc; i++) tr->probe_clusters[qi * Pc + i] = i < npc ? cl[i].second : 0xffffffffu;
-            for (int i = 0; i < Ps; i++) {
+            for (int i = 0; i < Ps; i++)
                 if (tr->probe_lists) tr->probe_lists[qi * Ps + i] = i < nps ? sl[i].second : 0xffffffffu;
-                if (tr->range_start) tr->range_start[qi * Ps + i] = s.start[i];
-                if (tr->range_len) tr->range_len[qi * Ps + i] = s.len[i];
+            for (int r = 0; r < R; r++) {
+                if (tr->range_start) tr->range_start[qi * R + r] = s.start[r];
+                if (tr->range_len) tr->range_len[qi * R + r] = s.len[r];
             }
         }
     }
@@ -702,7 +857,7 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
         const bool pre = mode == 0 || sched1;
         std::vector<std::pair<float, uint32_t>> cand;
         uint32_t pos = 0;
-        for (int r = 0; r < Ps; r++)
+        for (int r = 0; r < R; r++)
             for (uint32_t p = s.start[r]; p < s.start[r] + s.len[r]; p++, pos++) {
                 if (pre && !pred(p)) continue;  // query_prefilter (prefiltering.cu:36-51)
                 cand.push_back({adc(p, pos), p});

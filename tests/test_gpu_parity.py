@@ -200,6 +200,32 @@ def test_parity_prefilter_generic_exact(cuda):
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
 
 
+@pytest.mark.parametrize("n_split", [1, 8])
+def test_parity_is_split_range_filters(cuda, n_split):
+    # is_split = 1: each probed list's Morton interval cut into n_split parts whose starts
+    # move by up to three next-in-box jumps (parts with no reachable in-box code dropped);
+    # every part's (start, len) must equal the oracle's
+    ws = datasets.config4(scale=0.002, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=4096, is_split=1, n_split=n_split)
+    idx, r = _parity(ws, cuda)
+    assert idx.last_query_stats()["coarse_total"] > 0
+
+
+def test_parity_is_split_postfilter_three_dims(cuda):
+    ws = datasets.config2(scale=0.01, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000, is_split=1, n_split=16)
+    idx, _ = _parity(ws, cuda)
+    split_total = idx.last_query_stats()["coarse_total"]
+    idx.set_param("is_split", 0)
+    query_gpu(idx, _base_of(ws, cuda), ws, ws["k"], cuda)
+    assert split_total <= idx.last_query_stats()["coarse_total"]
+
+
+def _base_of(ws, dev):
+    import torch
+    return torch.from_numpy(ws["base"]).to(dev)
+
+
 def test_select_handles_large_budget(cuda):
     # a candidate budget far above the old shared-memory top-K limit (exps0 = 40 -> 4000+)
     ws = datasets.config2(scale=0.01, n_queries=100, clusters=16, sub_clusters=4, n_list=16, sub_lists=64,
