@@ -158,8 +158,8 @@ def config4(scale: float = 1.0, n_queries: int = 100_000, query_seed: int = SEED
 
 def config5(scale: float = 1.0, n_queries: int = 50_000, **conf):
     """The learned variant: config4's data and queries with the index set up for per-query
-    probe counts up to 256 lists (n_list 64 clusters of 8 lists) and exps0 16."""
-    c = dict(n_list=64, sub_lists=256, exps0=16)
+    probe counts up to 1024 lists (n_list 128 clusters of 8 lists) and exps0 32."""
+    c = dict(n_list=128, sub_lists=1024, exps0=32)
     c.update(conf)
     ws = config4(scale=scale, n_queries=n_queries, **c)
     ws["name"] = "config5"

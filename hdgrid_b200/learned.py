@@ -13,7 +13,9 @@ from __future__ import annotations
 
 import numpy as np
 
-PROBES = (1, 2, 4, 8, 16, 32, 64, 128, 256)
+PROBES = (1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024)
+# index of b3[0] (the bias of the log2 probe-count output) in the parameter vector
+B3_PROBE = 128 * 48 + 128 + 128 * 128 + 128 + 2 * 128
 INV = np.uint64(0xFFFFFFFFFFFFFFFF)
 
 
@@ -88,14 +90,20 @@ def label_queries(idx, batch: Batch, gt: np.ndarray, probes=PROBES, target: floa
     dev = batch.q.device
     rec = np.zeros((len(schedules), len(probes), nq))
     cost = np.zeros((len(schedules), len(probes), nq))
+    hits = np.zeros((len(schedules), len(probes), nq), np.int64)
+    tot = np.zeros(nq, np.int64)
     for si, s in enumerate(schedules):
         sch = torch.full((nq,), s, dtype=torch.uint8, device=dev)
         for pi, p in enumerate(probes):
             npb = torch.full((nq,), p, dtype=torch.uint32, device=dev)
             ids, cand = batch.run(idx, n_probe=npb, schedule=sch)
-            rec[si, pi] = per_query_recall(ids, gt, batch.ks)
+            h, tot = _hits(ids, gt, batch.ks)
+            hits[si, pi] = h
+            rec[si, pi] = np.where(tot > 0, h / np.maximum(tot, 1), 1.0)
             cost[si, pi] = scan_bytes(cand, s, m, l)
     y = np.zeros((nq, 2), np.float32)
+    chosen_hits = np.zeros(nq, np.int64)
+    chosen_cost = np.zeros(nq)
     for i in range(nq):
         ok = rec[:, :, i] >= target
         if ok.any():
@@ -107,7 +115,11 @@ def label_queries(idx, batch: Batch, gt: np.ndarray, probes=PROBES, target: floa
             si, pi = np.unravel_index(np.argmin(c), c.shape)
         y[i, 0] = np.log2(probes[pi])
         y[i, 1] = schedules[si]
-    return y, {"recall": rec, "cost": cost}
+        chosen_hits[i] = hits[si, pi, i]
+        chosen_cost[i] = cost[si, pi, i]
+    # what a network reproducing every label exactly would reach
+    return y, {"recall": rec, "cost": cost, "label_recall": float(chosen_hits.sum() / max(tot.sum(), 1)),
+               "label_bytes": float(chosen_cost.sum()), "hits": int(chosen_hits.sum()), "total": int(tot.sum())}
 
 
 def train(idx, feats, y, epochs=60, batch=512, lr=2e-3, seed=1, init=True) -> float:
@@ -118,6 +130,33 @@ def train(idx, feats, y, epochs=60, batch=512, lr=2e-3, seed=1, init=True) -> fl
     if init:
         idx.mlp_init(seed)
     return idx.mlp_train(feats, yt, epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+
+def calibrate(idx, batch: Batch, gt: np.ndarray, target: float = 0.955, max_probe: int = 1024,
+              steps=(0.0, 0.25, 0.5, 0.75, 1.0, 1.25, 1.5, 2.0, 2.5, 3.0)) -> dict:
+    """Shifts the probe-count output by the smallest offset (log2 units) whose micro recall on
+    a validation batch reaches ``target``, written into the output bias b3[0]; the largest
+    offset when none does.  Returns the offset and the validation recall of each tried."""
+    import torch
+    w0 = idx.mlp_weights()
+    feats = idx.query_features(batch.q, batch.ql, batch.k_max, k=batch.k)
+    seen = {}
+    chosen = steps[-1]
+    for off in steps:
+        w = w0.copy()
+        w[B3_PROBE] += off
+        idx.set_mlp_weights(w)
+        p, f = predicted_settings(idx, feats, max_probe)
+        ids, _ = batch.run(idx, n_probe=torch.from_numpy(p).to(batch.q.device),
+                           schedule=torch.from_numpy(f).to(batch.q.device))
+        seen[off] = micro_recall(ids, gt, batch.ks)
+        if seen[off] >= target:
+            chosen = off
+            break
+    w = w0.copy()
+    w[B3_PROBE] += chosen
+    idx.set_mlp_weights(w)
+    return {"offset": chosen, "validation_recall": seen}
 
 
 def predicted_settings(idx, feats, max_probe: int):

@@ -6,10 +6,11 @@
 Builds the config5 index (config4's data: 10M x 128, 4 label dims, range filters), labels
 ``--train`` queries of an independent query stream (query seed 2002, filter seed 2004) by
 running the plain method at every probe count under both schedules, trains the BF16 MLP
-on the GPU, and evaluates on ``--heldout`` queries of the standard stream: recall@k
-against the exact filtered kNN and bytes scanned, for the plain schedule at every uniform
-probe count and for the learned schedule.  Writes the weights (.npy, f32) and a JSON
-report next to them.
+on the GPU, calibrates the probe-count output on ``--val`` further queries of that stream
+(the smallest log2 offset reaching recall 0.955), and evaluates on ``--heldout`` queries of
+the standard stream: recall@k against the exact filtered kNN, bytes scanned and device
+time, for the plain schedule at every uniform probe count and for the learned schedule.
+Writes the weights (.npy, f32) and a JSON report next to them.
 """
 from __future__ import annotations
 
@@ -44,8 +45,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--train", type=int, default=200_000)
     ap.add_argument("--heldout", type=int, default=50_000)
-    ap.add_argument("--target", type=float, default=0.97, help="per-query recall a label must reach")
-    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--val", type=int, default=10_000)
+    ap.add_argument("--target", type=float, default=0.98, help="per-query recall a label must reach")
+    ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--step", type=int, default=10_000, help="queries per labelling / evaluation batch")
@@ -54,7 +56,7 @@ def main():
     dev = torch.device("cuda:0")
     t0 = time.time()
     ev = datasets.config5(scale=args.scale, n_queries=args.heldout, break_down=0)
-    tr = datasets.config4(scale=args.scale, n_queries=args.train, query_seed=2002, filter_seed=2004,
+    tr = datasets.config4(scale=args.scale, n_queries=args.train + args.val, query_seed=2002, filter_seed=2004,
                           with_base=False)
     idx = hg.SuperGridIndex.from_text(ev["hdgrid_conf"], ev["filter_conf"])
     base = torch.from_numpy(ev["base"]).to(dev)
@@ -72,21 +74,27 @@ def main():
     log["gt_train_s"] = round(time.time() - t1, 1)
     ys, feats = [], []
     t1 = time.time()
-    for a in range(0, qtr.shape[0], args.step):
-        b = min(qtr.shape[0], a + args.step)
+    hits = tot = 0
+    for a in range(0, args.train, args.step):
+        b = min(args.train, a + args.step)
         batch = L.Batch(base, qtr[a:b], qltr[a:b], kstr[a:b])
-        y, _ = L.label_queries(idx, batch, gt_tr[a:b], target=args.target)
+        y, inf = L.label_queries(idx, batch, gt_tr[a:b], target=args.target)
+        hits += inf["hits"]
+        tot += inf["total"]
         ys.append(y)
         feats.append(idx.query_features(batch.q, batch.ql, 100, k=batch.k))
     y = np.concatenate(ys)
     f = torch.cat(feats).contiguous()
     log["label_s"] = round(time.time() - t1, 1)
     log["label_pre_share"] = float(y[:, 1].mean())
-    log["label_probe_hist"] = np.bincount(y[:, 0].astype(int), minlength=9).tolist()
+    log["label_probe_hist"] = np.bincount(y[:, 0].astype(int), minlength=len(L.PROBES)).tolist()
+    log["label_recall_bound"] = hits / max(tot, 1)
     t1 = time.time()
     loss = L.train(idx, f, y, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=1)
     log["train_s"] = round(time.time() - t1, 1)
     log["train_loss"] = loss
+    vb = L.Batch(base, qtr[args.train:], qltr[args.train:], kstr[args.train:])
+    log["calibration"] = L.calibrate(idx, vb, gt_tr[args.train:], max_probe=max(L.PROBES))
     print(json.dumps(log), flush=True)
 
     # held-out evaluation
@@ -95,8 +103,17 @@ def main():
     ksev = ev["ks"].astype(np.uint32)
     gt_ev = _gt(hg, base, labels, qev, qlev, ev["filter_conf"], 100)
     info = idx.info()
-    plain = {p: [0, 0, 0.0] for p in L.PROBES}
-    learned = [0, 0, 0.0]
+    plain = {p: [0, 0, 0.0, 0.0] for p in L.PROBES}
+    learned = [0, 0, 0.0, 0.0]
+
+    def timed(batch, **kw):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.run(idx, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
     for a in range(0, qev.shape[0], args.step):
         b = min(qev.shape[0], a + args.step)
         batch = L.Batch(base, qev[a:b], qlev[a:b], ksev[a:b])
@@ -107,19 +124,24 @@ def main():
             plain[p][0] += int(h.sum())
             plain[p][1] += int(t.sum())
             plain[p][2] += float(L.scan_bytes(cand, 0, info["M"], info["l"]).sum())
-        idx.set_param("sub_lists", 256)
+            plain[p][3] += timed(batch)
+        idx.set_param("sub_lists", max(L.PROBES))
         fe = idx.query_features(batch.q, batch.ql, 100, k=batch.k)
-        pp, ff = L.predicted_settings(idx, fe, 256)
+        pp, ff = L.predicted_settings(idx, fe, max(L.PROBES))
         idx.set_param("learned", 1)
         ids, cand = batch.run(idx)
+        learned[3] += timed(batch)
         idx.set_param("learned", 0)
         h, t = L._hits(ids, gt_ev[a:b], batch.ks)
         learned[0] += int(h.sum())
         learned[1] += int(t.sum())
         learned[2] += float((cand * np.where(ff == 1, info["M"] + 4 * info["l"], info["M"])).sum())
+    n = qev.shape[0]
     report = dict(log, heldout=args.heldout, train=args.train,
-                  plain=[{"sub_lists": p, "recall": v[0] / max(v[1], 1), "scan_bytes": v[2]} for p, v in plain.items()],
-                  learned={"recall": learned[0] / max(learned[1], 1), "scan_bytes": learned[2]})
+                  plain=[{"sub_lists": p, "recall": v[0] / max(v[1], 1), "scan_bytes": v[2], "qps": n / (v[3] / 1e3)}
+                         for p, v in plain.items()],
+                  learned={"recall": learned[0] / max(learned[1], 1), "scan_bytes": learned[2],
+                           "qps": n / (learned[3] / 1e3)})
     out = Path(args.out)
     out.parent.mkdir(parents=True, exist_ok=True)
     np.save(out, idx.mlp_weights())

@@ -11,6 +11,7 @@ from oracle import mlp_oracle as mo
 from tests.helpers import build_gpu
 
 pytestmark = pytest.mark.gpu
+PROBES = (1, 2, 4, 8, 16, 32, 64, 128, 256)  # this index probes at most 256 of its 512 lists
 
 
 def _index():
@@ -93,7 +94,7 @@ def learned_setup():
     tr, te = slice(0, 6000), slice(6000, 8000)
     btr = L.Batch(base, q[tr], ql[tr], ks[tr])
     bte = L.Batch(base, q[te], ql[te], ks[te])
-    y, _ = L.label_queries(idx, btr, gt[tr])
+    y, _ = L.label_queries(idx, btr, gt[tr], probes=PROBES)
     ftr = idx.query_features(btr.q, btr.ql, 100, k=btr.k)
     fte = idx.query_features(bte.q, bte.ql, 100, k=bte.k)
     loss = L.train(idx, ftr, y, epochs=80, batch=256, lr=2e-3, seed=1)
@@ -126,7 +127,7 @@ def test_learned_schedule_gains_over_plain(cuda, learned_setup):
     import torch
     plain, uniform_pre = [], []
     ones = torch.ones(b.q.shape[0], dtype=torch.uint8, device=cuda)
-    for p in L.PROBES:
+    for p in PROBES:
         idx.set_param("sub_lists", p)
         ids, cand = b.run(idx)  # the reference schedule at a uniform probe count
         plain.append((p, L.micro_recall(ids, gt, b.ks), float(L.scan_bytes(cand, 0, info["M"], info["l"]).sum())))
