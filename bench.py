@@ -53,6 +53,8 @@ def workload(name: str, scale: float, n_queries: int = 0):
         return datasets.config3(scale=scale, n_queries=nq, break_down=1)
     if name == "config4":
         return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1)
+    if name == "config5":
+        return datasets.config5(scale=scale, n_queries=n_queries or 10_000, break_down=1)
     raise SystemExit(f"unknown config {name}")
 
 
@@ -182,14 +184,16 @@ def run_reference(args):
 
 
 def metric_name(ws):
-    return "filtered QPS @recall@100>=0.95, 1 B200 (plain HDGrid path); ADC scan HBM GB/s"
+    path = "learned per-query schedule" if ws["name"] == "config5" else "plain HDGrid path"
+    return f"filtered QPS @recall@100>=0.95, 1 B200 ({path}); ADC scan HBM GB/s"
 
 
 def workload_config(ws, args):
     import hdgrid_b200 as hg
     p = hg.parse_config(ws["hdgrid_conf"])
     return {"workload": f"{ws['name']}: {ws['base'].shape[0]}x{ws['base'].shape[1]} base, "
-                        f"{ws['labels'].shape[1]} label dims, {ws['queries'].shape[0]} queries, k={ws['k']}",
+                        f"{ws['labels'].shape[1]} label dims, {ws['queries'].shape[0]} queries, "
+                        + (f"k={ws['k']}" if ws.get("ks") is None else "k per query in {10, 100}"),
             "n_lists": int(p["clusters"] * p["sub_clusters"]), "clusters": int(p["clusters"]),
             "n_list": int(p["n_list"]), "sub_lists": int(p["sub_lists"]), "pq_dim": int(p["pq_dim"]),
             "exps0": int(p["exps0"]), "max_grids": int(p["max_grids"]), "lut": "fp16" if p["lut_fp16"] else "f32",
@@ -241,13 +245,28 @@ def run_hdgrid(args):
     idx.build(hg.build_input_t(base, labels))
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
+    if ws["name"] == "config5":
+        # the learned per-query schedule, trained by hdgrid_b200/train_learned.py
+        wpath = ROOT / "hdgrid_b200" / "learned_weights" / "config5.npy"
+        if not wpath.exists():
+            raise SystemExit(f"{wpath} missing: run python -m hdgrid_b200.train_learned first")
+        idx.set_mlp_weights(np.load(wpath))
+        idx.set_param("learned", 1)
     q = torch.from_numpy(ws["queries"]).to(dev)
     ql = torch.from_numpy(ws["query_labels"]).to(dev)
     nq = q.shape[0]
     idx.reserve(nq)
+    ks = ws.get("ks")
+    qk = torch.from_numpy(ks.astype(np.uint32)).to(dev) if ks is not None else None
     dist = torch.empty((nq, k), device=dev)
     ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
     qin, qout = hg.query_input_t(base, q, ql), hg.query_output_t(dist, ids)
+
+    def do_query():  # per-query k (k drawn from {10, 100}) where the workload has one
+        if qk is not None:
+            idx.query_ex(qin, qout, k=qk)
+        else:
+            idx.query(qin, qout)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     stream = torch.cuda.current_stream()
 
@@ -260,14 +279,24 @@ def run_hdgrid(args):
     hg.bruteforce_knn(base, labels, q, ranges, k, gt_d, gt_i)
 
     for _ in range(args.warmup):
-        idx.query(qin, qout)
+        do_query()
     torch.cuda.synchronize()
     from hdgrid_b200 import datasets
+    from hdgrid_b200 import learned as L
     ids_np = ids.cpu().numpy().view(np.uint64)
-    rec = datasets.recall(ids_np, gt_i.cpu().numpy().view(np.uint64))
+    gt_np = gt_i.cpu().numpy().view(np.uint64)
+    rec = L.micro_recall(ids_np, gt_np, ks) if ks is not None else datasets.recall(ids_np, gt_np)
     launches_per_step = int(idx.last_query_stats()["launches"])
     max_rel = max_relative_error(ws, dist.cpu().numpy(), ids_np, args.err_sample)
-    cand = int(np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64).sum())
+    cand_q = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64)
+    cand = int(cand_q.sum())
+    info0, p0 = idx.info(), hg.parse_config(ws["hdgrid_conf"])
+    # algorithmic scan bytes: M code bytes per candidate, plus 4*l label bytes for every
+    # candidate whose query evaluates the predicate inside the scan
+    pre_q = np.full(nq, p0["exps0"] <= 1)
+    if ws["name"] == "config5":
+        pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
+    scan_bytes = float((cand_q * (info0["M"] + 4 * info0["l"] * pre_q)).sum())
 
     barrier(world)
     torch.cuda.synchronize()
@@ -277,13 +306,14 @@ def run_hdgrid(args):
         for s in range(args.steps):
             flush.fill_(float(s))
             ev[s][0].record(stream)
-            idx.query(qin, qout)
+            do_query()
             ev[s][1].record(stream)
             st = idx.stage_times()
             scan_ms.append(st.get("scan", float("nan")))
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
+    stage_ms = idx.stage_times()  # of the last timed step
     barrier(world)
 
     # end to end through the public API with host buffers
@@ -291,6 +321,7 @@ def run_hdgrid(args):
     ql_h = torch.from_numpy(ws["query_labels"]).pin_memory()
     d_h = torch.empty((nq, k), dtype=torch.float32).pin_memory()
     i_h = torch.empty((nq, k), dtype=torch.int64).pin_memory()
+    k_h = torch.from_numpy(ks.astype(np.uint32)).pin_memory() if ks is not None else None
     e2e_ms = []
     for s in range(args.steps):
         flush.fill_(float(s))
@@ -298,21 +329,45 @@ def run_hdgrid(args):
         t0 = time.perf_counter()
         q.copy_(q_h, non_blocking=True)
         ql.copy_(ql_h, non_blocking=True)
-        idx.query(qin, qout)
+        if k_h is not None:
+            qk.copy_(k_h, non_blocking=True)
+        do_query()
         d_h.copy_(dist, non_blocking=True)
         i_h.copy_(ids, non_blocking=True)
         torch.cuda.synchronize()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = max_over_ranks(sum(e2e_ms), world)
 
+    plain_ref = None
+    if ws["name"] == "config5":
+        # the plain schedule (LEARNED=0) on the same batch at uniform probe counts, for the
+        # learned-vs-plain comparison: recall and device-timed QPS of each
+        plain_ref = []
+        idx.set_param("learned", 0)
+        p5 = hg.parse_config(ws["hdgrid_conf"])
+        for sl in (16, 64, 128, 256):
+            idx.set_param("sub_lists", sl)
+            do_query()
+            torch.cuda.synchronize()
+            r = L.micro_recall(ids.cpu().numpy().view(np.uint64), gt_np, ks)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.fill_(1.0)
+            e0.record(stream)
+            do_query()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            plain_ref.append({"sub_lists": sl, "recall": r, "qps": nq / (e0.elapsed_time(e1) / 1e3)})
+        idx.set_param("sub_lists", int(p5["sub_lists"]))
+        idx.set_param("learned", 1)
+
     value = world * nq * args.steps / (total_ms / 1e3)
     peak, peak_kind = hbm_peak()
     info = idx.info()
     p = hg.parse_config(ws["hdgrid_conf"])
     lbl = ws["labels"].shape[1]
-    per_cand = info["M"] + (4 * lbl if p["exps0"] <= 1 else 0)
+    per_cand = scan_bytes / max(cand, 1)
     scan_avg = float(np.nanmean(scan_ms))
-    achieved = cand * per_cand / (scan_avg / 1e3) / 1e9
+    achieved = scan_bytes / (scan_avg / 1e3) / 1e9
     if rank != 0:
         return
     line = {
@@ -321,18 +376,20 @@ def run_hdgrid(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture, configs of the benchmark)",
         "config": workload_config(ws, args) | {"recall_at_k": rec, "build_s": round(t_build, 2),
                                                "candidates_per_step": cand,
-                                               "max_rel_dist_err_vs_fp64": max_rel},
+                                               "max_rel_dist_err_vs_fp64": max_rel}
+                  | ({"schedule": "learned (LEARNED=1)", "plain_schedule_same_batch": plain_ref}
+                     if plain_ref is not None else {}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": scan_traffic(ws, cand), "kernel": "k_scan_fast", "peak_kind": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg},
         "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
-                "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4),
+                "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4 + (k_h.numel() * 4 if k_h is not None else 0)),
                 "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},
         # kernels the library launched per query (prologue, [coarse GEMM x3], coarse, batch,
         # lut, scan, select, [refine]) times the timed steps
         "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
-        "stage_ms": idx.stage_times(),
+        "stage_ms": stage_ms,
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_bruteforce(ws, args.cpu_sample)

@@ -135,13 +135,14 @@ def train(idx, feats, y, epochs=60, batch=512, lr=2e-3, seed=1, init=True) -> fl
 def calibrate(idx, batch: Batch, gt: np.ndarray, target: float = 0.955, max_probe: int = 1024,
               steps=(0.0, 0.25, 0.5, 0.75, 1.0, 1.25, 1.5, 2.0, 2.5, 3.0)) -> dict:
     """Shifts the probe-count output by the smallest offset (log2 units) whose micro recall on
-    a validation batch reaches ``target``, written into the output bias b3[0]; the largest
-    offset when none does.  Returns the offset and the validation recall of each tried."""
+    a validation batch reaches ``target``, written into the output bias b3[0]; when none
+    does, the smallest offset within 0.0005 of the best recall seen.  Returns the offset and
+    the validation recall of each offset tried."""
     import torch
     w0 = idx.mlp_weights()
     feats = idx.query_features(batch.q, batch.ql, batch.k_max, k=batch.k)
     seen = {}
-    chosen = steps[-1]
+    chosen = None
     for off in steps:
         w = w0.copy()
         w[B3_PROBE] += off
@@ -153,6 +154,9 @@ def calibrate(idx, batch: Batch, gt: np.ndarray, target: float = 0.955, max_prob
         if seen[off] >= target:
             chosen = off
             break
+    if chosen is None:  # out of reach: the cheapest offset within 0.0005 of the best recall
+        best = max(seen.values())
+        chosen = min(o for o, r in seen.items() if r >= best - 5e-4)
     w = w0.copy()
     w[B3_PROBE] += chosen
     idx.set_mlp_weights(w)

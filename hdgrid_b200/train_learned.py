@@ -48,6 +48,7 @@ def main():
     ap.add_argument("--val", type=int, default=10_000)
     ap.add_argument("--target", type=float, default=0.98, help="per-query recall a label must reach")
     ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--exps0", type=int, default=0, help="refine ratio of the index (0 = config5's)")
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--step", type=int, default=10_000, help="queries per labelling / evaluation batch")
@@ -55,7 +56,8 @@ def main():
     args = ap.parse_args()
     dev = torch.device("cuda:0")
     t0 = time.time()
-    ev = datasets.config5(scale=args.scale, n_queries=args.heldout, break_down=0)
+    ev = datasets.config5(scale=args.scale, n_queries=args.heldout, break_down=0,
+                          **({"exps0": args.exps0} if args.exps0 else {}))
     tr = datasets.config4(scale=args.scale, n_queries=args.train + args.val, query_seed=2002, filter_seed=2004,
                           with_base=False)
     idx = hg.SuperGridIndex.from_text(ev["hdgrid_conf"], ev["filter_conf"])
