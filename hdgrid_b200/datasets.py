@@ -166,6 +166,39 @@ def config5(scale: float = 1.0, n_queries: int = 50_000, **conf):
     return ws
 
 
+def write_dataset_dir(ws: dict, path, neighbors=None) -> str:
+    """Writes a workload in the reference's dataset-directory format (what src/read_hfs5.py
+    produces and src/utils/io_utils.cu:3-28, 201-313 reads): `keys` and `dtypes`, one line per
+    key, and per key the raw row-major array plus `<key>_size` (int32 rows, cols).  Keys:
+    train_vec, train_label, test_vec, test_label and, when given, neighbors (int32, -1 for
+    missing).  Also writes HDGrid.conf (PATH pointing here) and filter.conf; returns the
+    HDGrid.conf path."""
+    import os
+    d = str(path).rstrip("/") + "/"
+    os.makedirs(d, exist_ok=True)
+    arrays = [("train_vec", ws["base"]), ("train_label", ws["labels"]), ("test_vec", ws["queries"]),
+              ("test_label", ws["query_labels"])]
+    if neighbors is not None:
+        nb = np.asarray(neighbors)
+        if nb.dtype == np.uint64:
+            nb = np.where(nb == np.uint64(0xFFFFFFFFFFFFFFFF), -1, nb.astype(np.int64))
+        arrays.append(("neighbors", nb.astype(np.int32)))
+    for key, a in arrays:
+        a = np.ascontiguousarray(a)
+        a.tofile(d + key)
+        np.array([a.shape[0], a.shape[1]], np.int32).tofile(d + key + "_size")
+    with open(d + "keys", "w") as f:
+        f.write("".join(k + "\n" for k, _ in arrays))
+    with open(d + "dtypes", "w") as f:
+        f.write("".join(str(np.asarray(a).dtype) + "\n" for _, a in arrays))
+    conf = "\n".join(line for line in ws["hdgrid_conf"].splitlines() if not line.lower().startswith("path"))
+    with open(d + "HDGrid.conf", "w") as f:
+        f.write(conf + f'\npath = "{d}"\n')
+    with open(d + "filter.conf", "w") as f:
+        f.write(ws["filter_conf"])
+    return d + "HDGrid.conf"
+
+
 def recall(found_ids: np.ndarray, gt_ids: np.ndarray) -> float:
     """|result ∩ GT| / |valid GT| with UINT64_MAX (or -1) GT entries ignored
     (src/verification/verification.cuh:97-153 without its app_reviews_points side file)."""
