@@ -67,14 +67,26 @@ __global__ void __launch_bounds__(256) k_features(IndexDev D, GridMeta g, const 
     unsigned long long tot = 0;
     unsigned nz = 0;
     for (int c = t; c < sort_n; c += blockDim.x) {
-        uint64_t key = ~0ull;
         if (c < C) {
-            key = ((uint64_t)float_key(seq_l2(s_q, D.centers + (uint64_t)c * d, d)) << 32) | (uint32_t)c;
             const uint32_t n = cc[qi * C + c];
             tot += n;
             nz += n > 0;
+        } else {
+            s_keys[c] = ~0ull;
         }
-        s_keys[c] = key;
+    }
+    // centroid distances, one warp per centroid: the lanes read a row with coalesced loads
+    // (the features only rank and log-scale these distances; no summation order is implied)
+    const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    for (int c = warp; c < C; c += nw) {
+        const float* row = D.centers + (uint64_t)c * d;
+        float sq = 0.f;
+        for (int i = lane; i < d; i += 32) {
+            const float df = s_q[i] - __ldg(row + i);
+            sq = fmaf(df, df, sq);
+        }
+        sq = warp_sum(sq);
+        if (lane == 0) s_keys[c] = ((uint64_t)float_key(sq) << 32) | (uint32_t)c;
     }
     atomicAdd(&s_tot, tot);
     atomicAdd(&s_nz, nz);
