@@ -100,6 +100,7 @@ def _load() -> C.CDLL:
         "hdg_recover_filters_noalloc": [C.POINTER(hdg_filter_spec), vp, u64, vp, vp],
         "hdg_bruteforce_knn": [vp, u64, u32, vp, u32, vp, u64, vp, u32, vp, vp, vp],
         "hdg_bf16_gemm": [vp, u64, vp, u64, u32, vp, u64, vp],
+        "hdg_merge_topk": [vp, vp, u64, u32, u32, vp, vp, vp, vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -470,3 +471,11 @@ def version() -> str:
 __all__ = ["Config", "config_factory", "index_factory", "SuperGridIndex", "build_input_t", "query_input_t",
            "query_output_t", "HDGError", "parse_config", "parse_filter", "pq_lut", "pq_adc", "label_mask",
            "recover_filters", "bruteforce_knn", "version", "EXPORTED", "LIB"]
+
+
+def merge_topk(dist, ids, k: int, offsets, out_dist, out_ids, stream=None) -> None:
+    """Merge of per-data-batch results (hdg_merge_topk): dist / ids [q x k * n_batches] CUDA
+    tensors (float32 / int64 holding u64 ids), offsets a CUDA int64 tensor of n_batches."""
+    nb = offsets.numel()
+    _check(LIB.hdg_merge_topk(_ptr(dist), _ptr(ids), dist.shape[0], k, nb, _ptr(offsets), _ptr(out_dist),
+                              _ptr(out_ids), _stream_ptr(stream)))

@@ -288,6 +288,16 @@ hdg_status hdg_mlp_train(hdg_index* index, const float* d_x, const float* d_y, u
     });
 }
 
+hdg_status hdg_merge_topk(const float* d_dist, const uint64_t* d_ids, uint64_t q, uint32_t k, uint32_t n_batches,
+                          const uint64_t* d_offsets, float* d_out_dist, uint64_t* d_out_ids, void* stream) {
+    return guarded([&] {
+        HDG_REQUIRE(d_dist && d_ids && d_offsets && d_out_dist && d_out_ids, HDG_ERR_INVALID_ARG, "null pointer");
+        if (q == 0) return;
+        merge_topk(d_dist, d_ids, q, k, n_batches, d_offsets, d_out_dist, d_out_ids,
+                   static_cast<cudaStream_t>(stream));
+    });
+}
+
 int hdg_last_query_stats(hdg_index* index, uint64_t* out, int cap) {
     if (!index || !out) return 0;
     guarded([&] { finish_async_query(index); });

@@ -312,3 +312,67 @@ void bruteforce_knn(const float* data, uint64_t n, uint32_t d, const float* labe
 }
 
 }  // namespace hdg
+
+namespace hdg {
+
+// ---- merge of per-data-batch results (merge_intermediate_result, src/core/merge_res.cu:18-56)
+// Row r of (dist, ids) holds n_batches blocks of k results, block b from an index built on
+// base rows [offset_b, ...): ids are shifted by offset_b (invalid ids stay invalid), the
+// k smallest (distance, id) of the row are kept, ascending.
+namespace {
+__global__ void k_merge_topk(const float* __restrict__ dist, const uint64_t* __restrict__ ids, uint32_t k,
+                             uint32_t nb, const uint64_t* __restrict__ offsets, int n2, float* __restrict__ out_dist,
+                             uint64_t* __restrict__ out_ids) {
+    extern __shared__ uint64_t s_key[];            // [n2] (distance key << 32 | slot)
+    uint64_t* s_id = s_key + n2;                    // [k * nb] shifted ids
+    const uint64_t r = blockIdx.x;
+    const uint32_t w = k * nb;
+    for (uint32_t i = threadIdx.x; i < (uint32_t)n2; i += blockDim.x) {
+        uint64_t key = ~0ull;
+        if (i < w) {
+            const uint64_t id = ids[r * w + i];
+            const bool ok = id != ~0ull;
+            const uint64_t sid = ok ? id + offsets[i / k] : ~0ull;
+            s_id[i] = sid;
+            // ties by the shifted id: the slot order of equal distances follows the id
+            key = ok ? ((uint64_t)float_key(dist[r * w + i]) << 32) | i : ~0ull;
+        }
+        s_key[i] = key;
+    }
+    __syncthreads();
+    block_bitonic_sort(s_key, n2);
+    // equal distance keys are ordered by slot; re-order each run of equal keys by id
+    if (threadIdx.x == 0) {
+        for (uint32_t i = 0; i + 1 < (uint32_t)min(n2, (int)w) && i < k; i++) {  // runs reaching the top k
+            uint32_t j = i + 1;
+            while (j < w && (s_key[j] >> 32) == (s_key[i] >> 32) && s_key[j] != ~0ull) j++;
+            for (uint32_t a = i + 1; a < j; a++)  // insertion sort on the (short) tie run
+                for (uint32_t b2 = a; b2 > i && s_id[(uint32_t)s_key[b2]] < s_id[(uint32_t)s_key[b2 - 1]]; b2--) {
+                    const uint64_t tmp = s_key[b2];
+                    s_key[b2] = s_key[b2 - 1];
+                    s_key[b2 - 1] = tmp;
+                }
+            i = j - 1;
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < k; i += blockDim.x) {
+        const uint64_t key = s_key[i];
+        const bool ok = key != ~0ull;
+        out_dist[r * k + i] = ok ? key_float((uint32_t)(key >> 32)) : INFINITY;
+        out_ids[r * k + i] = ok ? s_id[(uint32_t)key] : ~0ull;
+    }
+}
+}  // namespace
+
+void merge_topk(const float* dist, const uint64_t* ids, uint64_t q, uint32_t k, uint32_t nb, const uint64_t* offsets,
+                float* out_dist, uint64_t* out_ids, cudaStream_t st) {
+    HDG_REQUIRE(k >= 1 && nb >= 1 && (uint64_t)k * nb <= 8192, HDG_ERR_UNSUPPORTED, "k * n_batches must be <= 8192");
+    const int n2 = (int)next_pow2(std::max<uint32_t>(k * nb, 2));
+    const size_t sm = sizeof(uint64_t) * (n2 + (size_t)k * nb);
+    CK(cudaFuncSetAttribute(k_merge_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_merge_topk<<<(unsigned)q, 256, sm, st>>>(dist, ids, k, nb, offsets, n2, out_dist, out_ids);
+    CK_LAUNCH();
+}
+
+}  // namespace hdg

@@ -13,6 +13,11 @@
 //     their filter labels (filter_dim columns per label dim), neighbors the int32 ground truth;
 //   * with ENABLE_MULTI_GPU=1 every visible GPU holds a replica and takes an equal share of
 //     the queries (uniformly_divide); otherwise GPU 0 answers all;
+//   * when the base set is larger than MEM_BOUND bytes allow (d*4 + 64 bytes per point: the
+//     vector plus codes, labels, Morton code, id and build scratch), it is split into data
+//     batches: an index per batch answers every query and the per-batch top-k lists are
+//     merged on the GPU with ids shifted by the batch start (the reference's data-batch split
+//     and merge_intermediate_result, search-engine-auto-batch.cu:214-337, merge_res.cu:18-56);
 //   * results go to res/distances_<gpu> (f32) and res/neighbors_<gpu> (u64), topk per query,
 //     row-major, queries in order; then, when PATH/neighbors exists, the recall line.
 // Labels stored as int32 / int64 / float64 are converted to f32 on load (the reference copies
@@ -123,67 +128,103 @@ struct DeviceResult {
     std::vector<float> dist;
     std::vector<uint64_t> ids;
     double build_ms = 0, query_ms = 0;
+    uint64_t data_batches = 0;
     std::string error;
 };
 
-// One GPU: build its replica, answer queries [q0, q0 + nq) in batches, keep the results.
+uint64_t data_batch_rows(const hdg_params& P, uint64_t n, uint32_t d) {
+    const uint64_t per_row = (uint64_t)d * 4 + 64;
+    if (P.mem_bound == 0 || n * per_row <= P.mem_bound) return n;
+    return std::max<uint64_t>(1, P.mem_bound / per_row);
+}
+
+// One GPU: for each data batch build an index, answer queries [q0, q0 + nq) in query
+// batches, and merge the batch's top-k into the running results.
 void run_device(int dev, const std::string& algo, const std::string& conf, const std::string& filt,
-                const Array& base, const Array& blab, const Array& qv, const Array& qlab, uint64_t q0, uint64_t nq,
-                uint32_t topk, DeviceResult* out) {
+                const hdg_params& P, const Array& base, const Array& blab, const Array& qv, const Array& qlab,
+                uint64_t q0, uint64_t nq, uint32_t topk, DeviceResult* out) {
     try {
         cuda_check(cudaSetDevice(dev), "cudaSetDevice");
-        hdg_index* idx = nullptr;
-        check(hdg_create(algo.c_str(), conf.c_str(), filt.c_str(), &idx), "create");
         const uint64_t n = (uint64_t)base.rows;
         const uint32_t d = (uint32_t)base.cols, l = (uint32_t)blab.cols, lc = (uint32_t)qlab.cols;
-        float *d_base = nullptr, *d_lab = nullptr;
-        cuda_check(cudaMalloc(&d_base, n * d * 4), "cudaMalloc base");
-        cuda_check(cudaMalloc(&d_lab, n * l * 4), "cudaMalloc labels");
-        cuda_check(cudaMemcpy(d_base, base.f32.data(), n * d * 4, cudaMemcpyHostToDevice), "copy base");
-        cuda_check(cudaMemcpy(d_lab, blab.f32.data(), n * l * 4, cudaMemcpyHostToDevice), "copy labels");
-        cudaEvent_t e0, e1;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0);
-        check(hdg_build(idx, d_base, n, d, d_lab, l, nullptr), "build");
-        cudaEventRecord(e1);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        out->build_ms = ms;
+        const uint64_t dbatch = data_batch_rows(P, n, d);
         const uint64_t batch = std::min<uint64_t>(std::max<uint64_t>(nq, 1), 50000);
-        float *d_q = nullptr, *d_ql = nullptr, *d_dist = nullptr;
-        uint64_t* d_ids = nullptr;
+        float *d_base = nullptr, *d_lab = nullptr, *d_q = nullptr, *d_ql = nullptr, *d_dist = nullptr;
+        float *d_best_d = nullptr, *d_pair_d = nullptr;
+        uint64_t *d_ids = nullptr, *d_best_i = nullptr, *d_pair_i = nullptr, *d_off = nullptr;
+        const uint64_t nq1 = std::max<uint64_t>(nq, 1);
+        cuda_check(cudaMalloc(&d_base, dbatch * d * 4), "cudaMalloc base");
+        cuda_check(cudaMalloc(&d_lab, dbatch * l * 4), "cudaMalloc labels");
         cuda_check(cudaMalloc(&d_q, batch * d * 4), "cudaMalloc queries");
         cuda_check(cudaMalloc(&d_ql, batch * lc * 4), "cudaMalloc query labels");
         cuda_check(cudaMalloc(&d_dist, batch * topk * 4), "cudaMalloc distances");
         cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_ids), batch * topk * 8), "cudaMalloc ids");
-        check(hdg_reserve(idx, batch), "reserve");
-        out->dist.resize(nq * topk);
-        out->ids.resize(nq * topk);
-        for (uint64_t a = 0; a < nq; a += batch) {
-            const uint64_t b = std::min(nq, a + batch), m = b - a;
-            cuda_check(cudaMemcpy(d_q, qv.f32.data() + (q0 + a) * d, m * d * 4, cudaMemcpyHostToDevice), "copy q");
-            cuda_check(cudaMemcpy(d_ql, qlab.f32.data() + (q0 + a) * lc, m * lc * 4, cudaMemcpyHostToDevice),
-                       "copy query labels");
+        cuda_check(cudaMalloc(&d_best_d, nq1 * topk * 4), "cudaMalloc results");
+        cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_best_i), nq1 * topk * 8), "cudaMalloc results");
+        cuda_check(cudaMalloc(&d_pair_d, batch * topk * 2 * 4), "cudaMalloc merge");
+        cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_pair_i), batch * topk * 2 * 8), "cudaMalloc merge");
+        cuda_check(cudaMalloc(reinterpret_cast<void**>(&d_off), 2 * 8), "cudaMalloc offsets");
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float ms = 0;
+        for (uint64_t off = 0; off < n; off += dbatch) {
+            const uint64_t nb = std::min(dbatch, n - off);
+            hdg_index* idx = nullptr;
+            check(hdg_create(algo.c_str(), conf.c_str(), filt.c_str(), &idx), "create");
+            cuda_check(cudaMemcpy(d_base, base.f32.data() + off * d, nb * d * 4, cudaMemcpyHostToDevice), "copy base");
+            cuda_check(cudaMemcpy(d_lab, blab.f32.data() + off * l, nb * l * 4, cudaMemcpyHostToDevice), "copy labels");
             cudaEventRecord(e0);
-            check(hdg_query(idx, d_q, m, d_ql, lc, d_base, topk, d_dist, d_ids, nullptr), "query");
+            check(hdg_build(idx, d_base, nb, d, d_lab, l, nullptr), "build");
             cudaEventRecord(e1);
             cudaEventSynchronize(e1);
             cudaEventElapsedTime(&ms, e0, e1);
-            out->query_ms += ms;
-            cuda_check(cudaMemcpy(out->dist.data() + a * topk, d_dist, m * topk * 4, cudaMemcpyDeviceToHost), "copy d");
-            cuda_check(cudaMemcpy(out->ids.data() + a * topk, d_ids, m * topk * 8, cudaMemcpyDeviceToHost), "copy i");
+            out->build_ms += ms;
+            check(hdg_reserve(idx, batch), "reserve");
+            const uint64_t offs[2] = {0, off};
+            cuda_check(cudaMemcpy(d_off, offs, sizeof(offs), cudaMemcpyHostToDevice), "copy offsets");
+            for (uint64_t a = 0; a < nq; a += batch) {
+                const uint64_t m = std::min(nq, a + batch) - a;
+                cuda_check(cudaMemcpy(d_q, qv.f32.data() + (q0 + a) * d, m * d * 4, cudaMemcpyHostToDevice),
+                           "copy queries");
+                cuda_check(cudaMemcpy(d_ql, qlab.f32.data() + (q0 + a) * lc, m * lc * 4, cudaMemcpyHostToDevice),
+                           "copy query labels");
+                cudaEventRecord(e0);
+                check(hdg_query(idx, d_q, m, d_ql, lc, d_base, topk, d_dist, d_ids, nullptr), "query");
+                float* bd = d_best_d + a * topk;
+                uint64_t* bi = d_best_i + a * topk;
+                if (off == 0) {
+                    cuda_check(cudaMemcpyAsync(bd, d_dist, m * topk * 4, cudaMemcpyDeviceToDevice), "keep");
+                    cuda_check(cudaMemcpyAsync(bi, d_ids, m * topk * 8, cudaMemcpyDeviceToDevice), "keep");
+                } else {  // rows [running k | this batch's k], merged back into the running rows
+                    const size_t kd = (size_t)topk * 4, ki = (size_t)topk * 8;
+                    cuda_check(cudaMemcpy2DAsync(d_pair_d, 2 * kd, bd, kd, kd, m, cudaMemcpyDeviceToDevice), "pair");
+                    cuda_check(cudaMemcpy2DAsync(d_pair_d + topk, 2 * kd, d_dist, kd, kd, m,
+                                                 cudaMemcpyDeviceToDevice), "pair");
+                    cuda_check(cudaMemcpy2DAsync(d_pair_i, 2 * ki, bi, ki, ki, m, cudaMemcpyDeviceToDevice), "pair");
+                    cuda_check(cudaMemcpy2DAsync(d_pair_i + topk, 2 * ki, d_ids, ki, ki, m,
+                                                 cudaMemcpyDeviceToDevice), "pair");
+                    check(hdg_merge_topk(d_pair_d, d_pair_i, m, topk, 2, d_off, bd, bi, nullptr), "merge");
+                }
+                cudaEventRecord(e1);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1);
+                out->query_ms += ms;
+            }
+            hdg_destroy(idx);
+            out->data_batches++;
         }
-        cudaFree(d_q);
-        cudaFree(d_ql);
-        cudaFree(d_dist);
-        cudaFree(d_ids);
-        cudaFree(d_base);
-        cudaFree(d_lab);
+        out->dist.resize(nq * topk);
+        out->ids.resize(nq * topk);
+        if (nq) {
+            cuda_check(cudaMemcpy(out->dist.data(), d_best_d, nq * topk * 4, cudaMemcpyDeviceToHost), "copy d");
+            cuda_check(cudaMemcpy(out->ids.data(), d_best_i, nq * topk * 8, cudaMemcpyDeviceToHost), "copy i");
+        }
+        for (void* p : {(void*)d_base, (void*)d_lab, (void*)d_q, (void*)d_ql, (void*)d_dist, (void*)d_ids,
+                        (void*)d_best_d, (void*)d_best_i, (void*)d_pair_d, (void*)d_pair_i, (void*)d_off})
+            cudaFree(p);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        hdg_destroy(idx);
     } catch (const std::exception& ex) {
         out->error = ex.what();
     }
@@ -253,8 +294,8 @@ int main(int argc, char** argv) {
             const uint64_t per = nq / n_dev, rem = nq % n_dev;
             qn[i] = per + ((uint64_t)i < rem ? 1 : 0);
             q0[i] = (uint64_t)i * per + std::min<uint64_t>(i, rem);
-            workers.emplace_back(run_device, i, algo, conf, filt, std::cref(base), std::cref(blab), std::cref(qv),
-                                 std::cref(qlab), q0[i], qn[i], topk, &res[i]);
+            workers.emplace_back(run_device, i, algo, conf, filt, std::cref(P), std::cref(base), std::cref(blab),
+                                 std::cref(qv), std::cref(qlab), q0[i], qn[i], topk, &res[i]);
         }
         for (auto& w : workers) w.join();
         ::mkdir("res", 0755);
@@ -266,9 +307,10 @@ int main(int argc, char** argv) {
             fd.write(reinterpret_cast<const char*>(res[i].dist.data()), (std::streamsize)(res[i].dist.size() * 4));
             fi.write(reinterpret_cast<const char*>(res[i].ids.data()), (std::streamsize)(res[i].ids.size() * 8));
             if (!fd || !fi) throw std::runtime_error("Failed to flush query result!");
-            std::printf("device: %d build time: %.3f ms, query time: %.3f ms (%llu queries, %.0f QPS)\n", i,
-                        res[i].build_ms, res[i].query_ms, (unsigned long long)qn[i],
-                        res[i].query_ms > 0 ? qn[i] / (res[i].query_ms / 1e3) : 0.0);
+            std::printf("device: %d build time: %.3f ms, query time: %.3f ms (%llu queries, %.0f QPS, %llu data "
+                        "batches)\n", i, res[i].build_ms, res[i].query_ms, (unsigned long long)qn[i],
+                        res[i].query_ms > 0 ? qn[i] / (res[i].query_ms / 1e3) : 0.0,
+                        (unsigned long long)res[i].data_batches);
             all_ids.insert(all_ids.end(), res[i].ids.begin(), res[i].ids.end());
         }
         if (type.count("neighbors") && file_exists(dir + "neighbors")) {

@@ -285,6 +285,16 @@ hdg_status hdg_bruteforce_knn(const float* d_data, uint64_t n, uint32_t d,
                               uint64_t q, const float* d_ranges, uint32_t k,
                               float* d_dist, uint64_t* d_ids, void* stream);
 
+/* Merge of per-data-batch results, replacing merge_intermediate_result
+ * (src/core/merge_res.cu:18-56): row r of d_dist / d_ids [q x (k * n_batches)] holds
+ * n_batches blocks of k results, block b from an index built on base rows starting at
+ * d_offsets[b] (device array); ids are shifted by that offset (UINT64_MAX stays invalid) and
+ * the k smallest (distance, id) of the row are written ascending to d_out_dist / d_out_ids
+ * [q x k].  k * n_batches <= 8192. */
+hdg_status hdg_merge_topk(const float* d_dist, const uint64_t* d_ids, uint64_t q, uint32_t k,
+                          uint32_t n_batches, const uint64_t* d_offsets, float* d_out_dist,
+                          uint64_t* d_out_ids, void* stream);
+
 /* Thread-local message of the last failing call. */
 const char* hdg_last_error(void);
 const char* hdg_version(void);
