@@ -298,6 +298,20 @@ def run_hdgrid(args):
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
     scan_bytes = float((cand_q * (info0["M"] + 4 * info0["l"] * pre_q)).sum())
 
+    # the batched workloads (10M x 128) run as the persistent scan under a captured CUDA graph,
+    # with the scan's threads x candidates-per-thread and work-item size picked by the
+    # autotuner; a plain-path run first gives the per-stage times (events do not reach into
+    # a graph replay)
+    graph_mode = ws["name"] in ("config4", "config5")
+    tuned, plain_stages = None, None
+    if graph_mode:
+        tuned = idx.autotune(qin, qout)
+        do_query()
+        torch.cuda.synchronize()
+        plain_stages = idx.stage_times()
+        idx.set_param("query_graph", 1)
+        do_query()  # first call of the shape: plain run + capture
+        torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -314,6 +328,10 @@ def run_hdgrid(args):
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
     stage_ms = idx.stage_times()  # of the last timed step
+    if graph_mode:
+        idx.status()  # raises if a replay outgrew the captured distance capacity
+        stage_ms = plain_stages
+        scan_ms = [plain_stages.get("scan", float("nan"))]
     barrier(world)
 
     # end to end through the public API with host buffers
@@ -378,7 +396,8 @@ def run_hdgrid(args):
                                                "candidates_per_step": cand,
                                                "max_rel_dist_err_vs_fp64": max_rel}
                   | ({"schedule": "learned (LEARNED=1)", "plain_schedule_same_batch": plain_ref}
-                     if plain_ref is not None else {}),
+                     if plain_ref is not None else {})
+                  | ({"cuda_graph": True, "autotuned": tuned} if graph_mode else {}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": scan_traffic(ws, cand), "kernel": "k_scan_fast", "peak_kind": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg},

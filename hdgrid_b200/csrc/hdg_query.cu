@@ -1828,7 +1828,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         // first call of this shape: the plain path computes this call's results and sizes
         // the buffers; the captured graph serves the next calls
         enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
-        const uint64_t need = std::max<uint64_t>(idx->last_stats[3], 1) * 4 * 2;  // 2x this batch
+        const uint64_t need = std::max<uint64_t>(idx->last_stats[3], 1) * 4 * 5 / 4;  // 1.25x this batch
         if (idx->dist_buf.bytes < need) {
             invalidate_graphs(idx);
             idx->dist_buf.reset();

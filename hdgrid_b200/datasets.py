@@ -149,7 +149,9 @@ def config4(scale: float = 1.0, n_queries: int = 100_000, query_seed: int = SEED
             ql[i, 2 * dd + 1] = lo + width - 1
     ks = frng.choice([10, 100], size=n_queries)
     filt = "l = 4\n" + "".join(f"filter{i}:\n\ttype = 3\n" for i in range(4))
-    c = dict(clusters=512, sub_clusters=8, pq_dim=32, max_grids=65536, n_list=32, sub_lists=64, exps0=4, topk=100,
+    # n_list / sub_lists / exps0: where the plain schedule's recall stops rising on this
+    # workload (0.72 at 64 lists; more lists add cost, not recall)
+    c = dict(clusters=512, sub_clusters=8, pq_dim=32, max_grids=65536, n_list=64, sub_lists=64, exps0=32, topk=100,
              filter_dim=2)
     c.update(conf)
     return dict(name="config4", base=base, labels=labels, queries=queries, query_labels=ql,

@@ -191,7 +191,7 @@ int hdg_last_query_stats(hdg_index* index, uint64_t* out, int cap);
 /* With QUERY_GRAPH=1 hdg_query returns once the captured graph is enqueued; this waits for
  * the last replay and returns its device status: HDG_OK, HDG_ERR_TIMEOUT (a tensor-core
  * wait of the coarse GEMM expired) or HDG_ERR_OOM (the batch had more candidates than the
- * distance buffer sized at capture -- twice the first batch of the shape -- and the
+ * distance buffer sized at capture -- 1.25x the first batch of the shape -- and the
  * queries past it returned no results).  HDG_OK when no replay is pending.  No reference
  * counterpart: the reference synchronises after every stage. */
 hdg_status hdg_query_status(hdg_index* index);
