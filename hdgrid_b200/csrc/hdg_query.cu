@@ -1075,12 +1075,15 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     block_exclusive_scan(s_pre, Ps + 1, s_warp);
     const uint32_t nfin = w.nfin[qi];
     const uint32_t need0 = min((uint32_t)K, nfin);
+    // emitted entries keep their candidate position; positions become pool slots once the
+    // selection is complete, in one divergence-free loop over the K entries (converting at
+    // emit time made nearly every warp of the pass run the range search for one lane)
     auto emit = [&](uint32_t e, float d) {
         const uint32_t pos = atomicAdd(&s_out, 1u);
         if (sorted_out)
             s_sel[pos] = ((uint64_t)float_key(d) << 32) | e;
         else
-            w.cand_pool[qi * w.kcand + pos] = pos_to_pool(s_pre, s_start, Ps, e);
+            w.cand_pool[qi * w.kcand + pos] = e;
     };
     auto inside = [&](float d, int nlv) {
         for (int l = 0; l < nlv; l++)
@@ -1233,6 +1236,8 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     __syncthreads();
     const uint32_t nsel = s_out;
     if (!sorted_out) {
+        uint32_t* pool = w.cand_pool + qi * w.kcand;
+        for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
         if (t == 0) w.cand_count[qi] = nsel;
         return;
     }
