@@ -810,10 +810,17 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         float* dst = w.dist + w.qoff[qq];
         const bool preq = pre || q_prefilter(w, qq);
         uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
+        // each warp takes a contiguous span of the item (a multiple of 32 * CPT positions,
+        // so position mod 32 stays the lane), so a lane's walk to its candidate's range
+        // crosses few range boundaries per step
+        constexpr uint32_t kStep = 32u * CPT;
+        const uint32_t span = ((e1 - e0 + NT / 32 - 1) / (NT / 32) + kStep - 1) / kStep * kStep;
+        const uint32_t wb = e0 + (uint32_t)(t >> 5) * span;
+        const uint32_t we = min(e1, wb + span);
         int r[CPT];
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
-            const uint32_t e = e0 + t + u * NT;
+            const uint32_t e = wb + lane + u * 32;
             int lo = 0, hi = Ps - 1;
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -824,14 +831,14 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         }
         const uint4* planes = reinterpret_cast<const uint4*>(D.codes);
         const uint64_t n_pts = D.n;
-        for (uint32_t eb = e0 + t; eb < e1; eb += NT * CPT) {
+        for (uint32_t eb = wb + lane; eb < we; eb += kStep) {
             const uint4* cp[CPT];
             bool live[CPT];
             float sum[CPT], sum1[CPT];  // even / odd steps, added at the end
 #pragma unroll
             for (int u = 0; u < CPT; u++) {
-                const uint32_t e = eb + u * NT;
-                live[u] = e < e1;
+                const uint32_t e = eb + u * 32;
+                live[u] = e < we;
                 sum[u] = INFINITY;
                 uint32_t row = 0;  // dead / filtered candidates read row 0 (in bounds), result discarded
                 if (live[u]) {
@@ -882,7 +889,7 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
             for (int u = 0; u < CPT; u++) {
                 sum[u] += sum1[u];
                 if (!live[u]) continue;
-                const uint32_t e = eb + u * NT;
+                const uint32_t e = eb + u * 32;
                 if (sum[u] < INFINITY) {
                     const uint32_t key = float_key(sum[u]);
                     kmin = min(kmin, key);
