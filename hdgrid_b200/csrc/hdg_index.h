@@ -24,6 +24,8 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -98,6 +100,22 @@ struct DeviceBuffer {
 struct GraphState;                 // captured query graphs (hdg_query.cu)
 void release_graphs(GraphState* g);
 
+// Query state of one stream: the workspace, the distance buffer and the captured graphs.
+// Calls on different streams use different contexts and may run concurrently; calls on one
+// stream take `mu` in turn.
+struct QueryCtx {
+    DeviceBuffer work;              // per-query workspace
+    DeviceBuffer dist_buf;          // one f32 ADC distance per scanned candidate
+    uint64_t work_queries = 0;
+    std::map<std::string, std::pair<size_t, size_t>> layout;  // name -> (offset, bytes)
+    GraphState* graphs = nullptr;   // QUERY_GRAPH=1: graphs keyed by pointers and sizes
+    std::mutex mu;
+    QueryCtx() = default;
+    QueryCtx(const QueryCtx&) = delete;
+    QueryCtx& operator=(const QueryCtx&) = delete;
+    ~QueryCtx() { release_graphs(graphs); }
+};
+
 }  // namespace hdg
 
 struct hdg_index {
@@ -109,10 +127,11 @@ struct hdg_index {
     hdg::IndexDev dev{};
     hdg::DeviceBuffer arena;       // all index arrays
     hdg::DeviceBuffer map_buf;     // filter interval map
-    hdg::DeviceBuffer work;        // per-query workspace
-    hdg::DeviceBuffer dist_buf;    // one f32 ADC distance per scanned candidate
-    uint64_t work_queries = 0;
-    std::map<std::string, std::pair<size_t, size_t>> work_layout;  // name -> (offset, bytes)
+    // query contexts by stream (the last one used serves hdg_debug_fetch)
+    std::map<void*, std::unique_ptr<hdg::QueryCtx>> ctxs;
+    hdg::QueryCtx* last_ctx = nullptr;
+    std::mutex ctx_mu;             // guards ctxs and last_ctx
+    std::mutex stats_mu;           // guards the last-query stats and stage times
     int device = 0;
     // stage timing (break_down=1)
     std::vector<std::string> stage_names;
@@ -121,9 +140,6 @@ struct hdg_index {
     uint64_t last_q = 0, last_ncand = 0;
     uint64_t last_stats[10] = {0};
     float last_beta = 0.f;
-    // CUDA-graph query path (QUERY_GRAPH=1): graphs keyed by the call's pointers and sizes,
-    // the replay stream and the pinned status words of the last replay
-    hdg::GraphState* graphs = nullptr;
     // learned per-query schedule: f32 master | Adam m | Adam v | gradient | bf16 weights
     hdg::DeviceBuffer mlp;
     bool mlp_ready = false;
@@ -131,5 +147,5 @@ struct hdg_index {
     hdg_index() = default;
     hdg_index(const hdg_index&) = delete;
     hdg_index& operator=(const hdg_index&) = delete;
-    ~hdg_index() { hdg::release_graphs(graphs); }
+    ~hdg_index() = default;
 };

@@ -1369,17 +1369,17 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
 // ------------------------------------------------------------------------------------
 static uint32_t lut_groups(const IndexDev& D) { return (D.M + 31) / 32; }
 
-static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) {
+static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand, bool record) {
     const hdg_params& P = idx->params;
     const uint64_t l = idx->dev.l, L = idx->dev.n_lists, C = idx->dev.C;
     const uint64_t Pc = std::max<uint64_t>(1, P.n_list), Ps = std::max<uint64_t>(1, P.sub_lists);
     const uint64_t G = lut_groups(idx->dev);
     size_t off = 0;
-    char* base = static_cast<char*>(idx->work.ptr);
+    char* base = static_cast<char*>(cx.work.ptr);
     auto take = [&](const char* name, size_t bytes) -> void* {
         const size_t o = off;
         off += align_up(bytes ? bytes : 1, 256);
-        if (record) idx->work_layout[name] = {o, bytes};
+        if (record) cx.layout[name] = {o, bytes};
         return base ? base + o : nullptr;
     };
     Workspace w{};
@@ -1415,31 +1415,46 @@ static Workspace carve(hdg_index* idx, uint64_t q, uint64_t kcand, bool record) 
     w.feats = (float*)take("features", q * kMlpFeatures * 4);
     w.lq_ps = (uint32_t*)take("learned_nprobe", q * 4);
     w.lq_sched = (uint8_t*)take("learned_schedule", q);
-    w.dist = static_cast<float*>(idx->dist_buf.ptr);
-    if (!base) idx->work.bytes = std::max(idx->work.bytes, off);  // size probe
+    w.dist = static_cast<float*>(cx.dist_buf.ptr);
+    if (!base) cx.work.bytes = std::max(cx.work.bytes, off);  // size probe
     return w;
 }
 
-static size_t workspace_bytes(hdg_index* idx, uint64_t q, uint64_t kcand) {
-    void* saved = idx->work.ptr;
-    idx->work.ptr = nullptr;
-    const size_t before = idx->work.bytes;
-    idx->work.bytes = 0;
-    carve(idx, q, kcand, false);
-    const size_t need = idx->work.bytes;
-    idx->work.ptr = saved;
-    idx->work.bytes = before;
+static size_t workspace_bytes(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand) {
+    void* saved = cx.work.ptr;
+    cx.work.ptr = nullptr;
+    const size_t before = cx.work.bytes;
+    cx.work.bytes = 0;
+    carve(idx, cx, q, kcand, false);
+    const size_t need = cx.work.bytes;
+    cx.work.ptr = saved;
+    cx.work.bytes = before;
     return need;
 }
 
-void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand) {
+static void reserve_ctx(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand) {
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
     if (kcand == 0) kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
-    const size_t need = workspace_bytes(idx, q, kcand);
-    if (idx->work.ptr && idx->work.bytes >= need) return;
-    idx->work.reset();
-    idx->work.ensure(need);
-    idx->work_queries = q;
+    const size_t need = workspace_bytes(idx, cx, q, kcand);
+    if (cx.work.ptr && cx.work.bytes >= need) return;
+    cx.work.reset();
+    cx.work.ensure(need);
+    cx.work_queries = q;
+}
+
+// The query context of a stream (created on first use); it becomes the last one used.
+static QueryCtx& query_ctx(hdg_index* idx, cudaStream_t st) {
+    std::lock_guard<std::mutex> g(idx->ctx_mu);
+    auto& slot = idx->ctxs[static_cast<void*>(st)];
+    if (!slot) slot.reset(new QueryCtx());
+    idx->last_ctx = slot.get();
+    return *slot;
+}
+
+void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand, cudaStream_t st) {
+    QueryCtx& cx = query_ctx(idx, st);
+    std::lock_guard<std::mutex> g(cx.mu);
+    reserve_ctx(idx, cx, q, kcand);
 }
 
 FilterDev filter_dev(const hdg_index* idx) {
@@ -1483,6 +1498,7 @@ struct StageTimer {
     void finish() {
         if (!on) return;
         CK(cudaEventSynchronize(ev.back()));
+        std::lock_guard<std::mutex> g(idx->stats_mu);
         idx->stage_names.clear();
         idx->stage_ms.clear();
         for (size_t i = 1; i < ev.size(); i++) {
@@ -1557,18 +1573,27 @@ void release_graphs(GraphState* g) {
     delete g;
 }
 
-void invalidate_graphs(hdg_index* idx) {
-    if (!idx->graphs) return;
-    if (idx->graphs->pending) cudaEventSynchronize(idx->graphs->ev_out);
-    for (auto& e : idx->graphs->entries)
+static void invalidate_ctx_graphs(QueryCtx& cx) {
+    if (!cx.graphs) return;
+    if (cx.graphs->pending) cudaEventSynchronize(cx.graphs->ev_out);
+    for (auto& e : cx.graphs->entries)
         if (e.exec) cudaGraphExecDestroy(e.exec);
-    idx->graphs->entries.clear();
-    idx->graphs->pending = false;
+    cx.graphs->entries.clear();
+    cx.graphs->pending = false;
+}
+
+void invalidate_graphs(hdg_index* idx) {
+    std::lock_guard<std::mutex> g(idx->ctx_mu);
+    for (auto& kv : idx->ctxs) {
+        std::lock_guard<std::mutex> gc(kv.second->mu);
+        invalidate_ctx_graphs(*kv.second);
+    }
 }
 
 // The stats of a query from its batch scalars (scal of k_batch).
 static void fill_stats(hdg_index* idx, uint64_t q, uint32_t k, int mode, uint64_t exps0, const uint64_t* sc,
                        uint64_t launches) {
+    std::lock_guard<std::mutex> g(idx->stats_mu);
     const uint64_t coarse = sc[0], real = sc[1], max_row = sc[2];
     const uint32_t bb = (uint32_t)sc[4];
     float beta;
@@ -1599,8 +1624,8 @@ static void fill_stats(hdg_index* idx, uint64_t q, uint32_t k, int mode, uint64_
 // distance buffer and fills the stats (the plain path).  Otherwise nothing waits on the
 // host (the CUDA-graph path): the distance buffer keeps its capacity, queries past it are
 // cut by k_batch, and the scalars and the GEMM status word are copied to pinned memory.
-static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, bool sync_sizing,
-                          uint64_t* pinned, uint64_t* launches_out, int* mode_out) {
+static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cudaStream_t st, bool sync_sizing,
+                          uint64_t* pinned, uint64_t* launches_out, int* mode_out, uint64_t* coarse_out = nullptr) {
     const uint64_t q = c.q;
     const uint32_t k = c.k;
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
@@ -1624,11 +1649,11 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     HDG_REQUIRE(mode != kPre || !c.qsched, HDG_ERR_INVALID_ARG,
                 "per-query schedules need exps0 > 1 (the pre-filter schedule has no re-rank)");
     const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
-    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) {
+    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q, kcand)) {
         HDG_REQUIRE(sync_sizing, HDG_ERR_STATE, "workspace too small for a captured query");
-        reserve_workspace(idx, q, kcand);
+        reserve_ctx(idx, cx, q, kcand);
     }
-    Workspace w = carve(idx, q, kcand, true);
+    Workspace w = carve(idx, cx, q, kcand, true);
     w.qk = c.qk;
     w.qps = c.qps;
     w.qsched = c.qsched;
@@ -1636,7 +1661,7 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     w.mode = mode;
     w.exps0 = (uint32_t)std::min<uint64_t>(exps0, 1u << 20);
     w.chunk = P.scan_chunk ? (uint32_t)P.scan_chunk : kChunk;
-    w.cap = sync_sizing ? ~0ull : idx->dist_buf.bytes / 4;
+    w.cap = sync_sizing ? ~0ull : cx.dist_buf.bytes / 4;
     const FilterDev f = filter_dev(idx);
     StageTimer tm(idx, st, sync_sizing && P.break_down != 0);
 
@@ -1695,15 +1720,16 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
         CK(cudaStreamSynchronize(st));
         HDG_REQUIRE(gemm_err == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
         const uint64_t coarse = sc[0];
-        if (idx->dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
-            invalidate_graphs(idx);  // their distance pointer dies with the old buffer
-            idx->dist_buf.reset();
-            idx->dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
+        if (coarse_out) *coarse_out = coarse;
+        if (cx.dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
+            invalidate_ctx_graphs(cx);  // their distance pointer dies with the old buffer
+            cx.dist_buf.reset();
+            cx.dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
         }
     } else {
-        HDG_REQUIRE(idx->dist_buf.ptr, HDG_ERR_STATE, "no distance buffer for a captured query");
+        HDG_REQUIRE(cx.dist_buf.ptr, HDG_ERR_STATE, "no distance buffer for a captured query");
     }
-    w.dist = static_cast<float*>(idx->dist_buf.ptr);
+    w.dist = static_cast<float*>(cx.dist_buf.ptr);
     tm.mark("budget");
 
     const uint32_t G = lut_groups(D);
@@ -1790,8 +1816,8 @@ static void enqueue_query(hdg_index* idx, const QueryCall& c, cudaStream_t st, b
     tm.finish();
 }
 
-hdg_status finish_async_query(hdg_index* idx) {
-    GraphState* g = idx->graphs;
+static hdg_status finish_ctx(hdg_index* idx, QueryCtx& cx) {
+    GraphState* g = cx.graphs;
     if (!g || !g->pending) return HDG_OK;
     CK(cudaEventSynchronize(g->ev_out));
     g->pending = false;
@@ -1801,12 +1827,27 @@ hdg_status finish_async_query(hdg_index* idx) {
     return HDG_OK;
 }
 
-static void make_graph_key(const hdg_index* idx, const QueryCall& c, uint64_t* key) {
+hdg_status finish_async_query(hdg_index* idx) {
+    std::vector<QueryCtx*> all;
+    {
+        std::lock_guard<std::mutex> g(idx->ctx_mu);
+        for (auto& kv : idx->ctxs) all.push_back(kv.second.get());
+    }
+    hdg_status worst = HDG_OK;
+    for (QueryCtx* cx : all) {
+        std::lock_guard<std::mutex> g(cx->mu);
+        const hdg_status s = finish_ctx(idx, *cx);
+        if (worst == HDG_OK) worst = s;
+    }
+    return worst;
+}
+
+static void make_graph_key(const hdg_index* idx, const QueryCtx& cx, const QueryCall& c, uint64_t* key) {
     const hdg_params& P = idx->params;
     const uint64_t v[24] = {(uint64_t)c.queries, c.q, (uint64_t)c.qlabels, c.label_cols, (uint64_t)c.data, c.k,
                             (uint64_t)c.dist, (uint64_t)c.ids, (uint64_t)c.qk, (uint64_t)c.qps, (uint64_t)c.qsched,
-                            (uint64_t)idx->work.ptr, idx->work.bytes, (uint64_t)idx->dist_buf.ptr,
-                            idx->dist_buf.bytes, P.n_list, P.sub_lists, P.exps0, P.lut_fp16, P.coarse_bf16,
+                            (uint64_t)cx.work.ptr, cx.work.bytes, (uint64_t)cx.dist_buf.ptr,
+                            cx.dist_buf.bytes, P.n_list, P.sub_lists, P.exps0, P.lut_fp16, P.coarse_bf16,
                             P.scan_cpt, P.scan_chunk, P.filter_dim, P.learned | (P.is_split << 8) | (P.n_split << 16)};
     std::memcpy(key, v, sizeof(v));
 }
@@ -1815,45 +1856,48 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
                cudaStream_t st, const uint32_t* d_k, const uint32_t* d_nprobe, const uint8_t* d_sched) {
     const QueryCall c{d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids, d_k, d_nprobe, d_sched};
+    QueryCtx& cx = query_ctx(idx, st);
+    std::lock_guard<std::mutex> lock(cx.mu);  // one query at a time per stream
     if (idx->params.query_graph == 0) {
-        finish_async_query(idx);
-        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
+        finish_ctx(idx, cx);
+        enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr);
         return;
     }
-    if (!idx->graphs) {
+    if (!cx.graphs) {
         GraphState* g = new GraphState();
-        idx->graphs = g;
+        cx.graphs = g;
         CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming));
         CK(cudaMallocHost(reinterpret_cast<void**>(&g->pinned), 16 * sizeof(uint64_t)));
         std::memset(g->pinned, 0, 16 * sizeof(uint64_t));
     }
-    GraphState* g = idx->graphs;
-    finish_async_query(idx);  // the pinned status words are reused by this replay
+    GraphState* g = cx.graphs;
+    finish_ctx(idx, cx);  // the pinned status words are reused by this replay
     uint64_t key[24];
-    make_graph_key(idx, c, key);
+    make_graph_key(idx, cx, c, key);
     GraphEntry* hit = nullptr;
     for (auto& e : g->entries)
         if (std::memcmp(e.key, key, sizeof(key)) == 0) hit = &e;
     if (!hit) {
         // first call of this shape: the plain path computes this call's results and sizes
         // the buffers; the captured graph serves the next calls
-        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
-        const uint64_t need = std::max<uint64_t>(idx->last_stats[3], 1) * 4 * 5 / 4;  // 1.25x this batch
-        if (idx->dist_buf.bytes < need) {
-            invalidate_graphs(idx);
-            idx->dist_buf.reset();
-            idx->dist_buf.ensure(need);
+        uint64_t coarse = 0;
+        enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr, &coarse);
+        const uint64_t need = std::max<uint64_t>(coarse, 1) * 4 * 5 / 4;  // 1.25x this batch
+        if (cx.dist_buf.bytes < need) {
+            invalidate_ctx_graphs(cx);
+            cx.dist_buf.reset();
+            cx.dist_buf.ensure(need);
         }
-        make_graph_key(idx, c, key);
+        make_graph_key(idx, cx, c, key);
         CK(cudaStreamSynchronize(st));
         GraphEntry e;
         std::memcpy(e.key, key, sizeof(key));
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed));
         try {
-            enqueue_query(idx, c, g->stream, false, g->pinned, &e.launches, &e.mode);
+            enqueue_query(idx, cx, c, g->stream, false, g->pinned, &e.launches, &e.mode);
         } catch (...) {
             cudaStreamEndCapture(g->stream, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -1891,8 +1935,10 @@ void query_features(hdg_index* idx, const float* d_queries, uint64_t q, const fl
     HDG_REQUIRE(label_cols == (uint32_t)(D.l * fd), HDG_ERR_INVALID_ARG,
                 "query label columns must equal l * filter_dim");
     const uint64_t kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
-    if (!idx->work.ptr || idx->work.bytes < workspace_bytes(idx, q, kcand)) reserve_workspace(idx, q, kcand);
-    Workspace w = carve(idx, q, kcand, true);
+    QueryCtx& cx = query_ctx(idx, st);
+    std::lock_guard<std::mutex> lock(cx.mu);
+    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q, kcand)) reserve_ctx(idx, cx, q, kcand);
+    Workspace w = carve(idx, cx, q, kcand, true);
     const FilterDev f = filter_dev(idx);
     const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
     if (sm_pro > 48 * 1024)
@@ -1912,8 +1958,10 @@ void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const fl
     const QueryCall c{d_queries, q, d_query_labels, label_cols, d_data, k, d_dist, d_ids, nullptr, nullptr, nullptr};
     float best = INFINITY;
     uint64_t best_cpt = 1, best_chunk = kChunk;
+    QueryCtx& cx = query_ctx(idx, st);
+    std::unique_lock<std::mutex> lock(cx.mu);
     try {
-        enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);  // warm-up, buffers sized
+        enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr);  // warm-up, buffers sized
         const uint64_t cpts[3] = {1, 2, 4};
         const uint64_t chunks[4] = {8192, 16384, 32768, 65536};
         for (uint64_t cpt : cpts)
@@ -1922,8 +1970,9 @@ void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const fl
                 P.scan_chunk = ch;
                 float t = INFINITY;
                 for (int rep = 0; rep < 2; rep++) {  // the faster of two runs
-                    enqueue_query(idx, c, st, true, nullptr, nullptr, nullptr);
+                    enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr);
                     float s = 0.f;
+                    std::lock_guard<std::mutex> gs(idx->stats_mu);
                     for (size_t i = 0; i < idx->stage_names.size(); i++)
                         if (idx->stage_names[i] == "scan") s = idx->stage_ms[i];
                     t = std::min(t, s);
@@ -1943,6 +1992,7 @@ void autotune_query(hdg_index* idx, const float* d_queries, uint64_t q, const fl
     P.scan_chunk = best_chunk;
     P.break_down = saved_bd;
     P.query_graph = saved_graph;
+    lock.unlock();
     invalidate_graphs(idx);
     if (best_ms) *best_ms = best;
 }

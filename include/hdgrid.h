@@ -125,8 +125,11 @@ hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value);
 hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t d,
                      const float* d_labels, uint32_t l, void* stream);
 
-/* Pre-size the query workspace for batches of up to max_queries, so that later
- * hdg_query calls on such batches allocate nothing. */
+/* Pre-size the query workspace of calls on the NULL stream for batches of up to
+ * max_queries, so that later hdg_query calls on such batches allocate nothing (calls on
+ * another stream size their own workspace on their first call).  Queries on different
+ * streams use different workspaces and may run concurrently from different host threads;
+ * calls on one stream run one after another. */
 hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries);
 
 /* d_queries [q x d] f32; d_query_labels [q x label_cols] f32 with label_cols = l*filter_dim;

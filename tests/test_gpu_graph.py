@@ -106,3 +106,44 @@ def test_autotune_keeps_results_and_picks_a_variant(cuda):
     torch.cuda.synchronize()
     assert torch.equal(ids, ref_i)
     assert torch.equal(dist.view(torch.int32), ref_d.view(torch.int32))
+
+
+def test_concurrent_queries_on_two_streams(cuda):
+    """Two host threads query one index on two streams at once: each stream has its own
+    workspace, so every answer equals the one the same batch gets alone."""
+    import threading
+    import torch
+    ws = datasets.config2(scale=0.01, n_queries=256, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                          max_grids=20_000)
+    k = ws["k"]
+    idx, base, _ = build_gpu(ws, cuda)
+    a = _io(ws, base, k, cuda)
+    b = _io(ws, base, k, cuda)
+    b[0].copy_(torch.flip(a[0], [0]))
+    b[1].copy_(torch.flip(a[1], [0]))
+    refs = []
+    for io in (a, b):
+        idx.query(io[4], io[5])
+        torch.cuda.synchronize()
+        refs.append((io[2].clone(), io[3].clone()))
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    errors = []
+
+    def worker(io, st, ref):
+        try:
+            for _ in range(6):
+                with torch.cuda.stream(st):
+                    io[2].fill_(-1.0)
+                idx.query(io[4], io[5], stream=st)
+                st.synchronize()
+                if not (torch.equal(io[3], ref[1]) and torch.equal(io[2].view(torch.int32), ref[0].view(torch.int32))):
+                    errors.append("mismatch")
+        except Exception as ex:  # reported below
+            errors.append(repr(ex))
+
+    threads = [threading.Thread(target=worker, args=(io, st, ref)) for io, st, ref in zip((a, b), streams, refs)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
