@@ -1267,10 +1267,10 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
 // ------------------------------------------------------------------------------------
 // k_refine: post-filter predicate, exact f32 L2, top-k
 // ------------------------------------------------------------------------------------
-// Candidates are taken in chunks of blockDim: the predicate survivors of a chunk are
-// compacted, each gets its exact distance from one warp, and the keys (distance, id) go
-// through a threshold buffer of pow2(k + blockDim) entries that is sorted and truncated
-// to k when it fills.
+// The predicate survivors of the query's candidates are compacted first; then every warp
+// computes exact distances of survivor rows in rounds, and the keys (distance, id) below the
+// running k-th go to a buffer of pow2(k + 4 * blockDim) entries that is sorted and cut to k
+// between rounds.
 __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __restrict__ queries,
                                                      const float* __restrict__ data, int cap, int apply_pred,
                                                      int lbl, Workspace w, float* __restrict__ out_dist,
@@ -1278,10 +1278,9 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);           // [cap]
     float* s_q = reinterpret_cast<float*>(s_keys + cap);             // [d]
-    __shared__ uint32_t s_chunk[kThreads];
     __shared__ float s_box[2 * kMaxDims];
     __shared__ int s_wsum[kThreads / 32];
-    __shared__ int s_cnt;
+    __shared__ int s_cnt, s_ns;
     __shared__ uint64_t s_th;
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = kThreads / 32;
@@ -1290,18 +1289,22 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
     if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
     if (t == 0) {
         s_cnt = 0;
+        s_ns = 0;
         s_th = ~0ull;
     }
     __syncthreads();
     const int nc = (int)w.cand_count[qi];
     const int kq = (int)q_k(w, qi);
     const bool pred_q = apply_pred && q_sched(w, qi) == 0;  // predicate-first queries already passed it
+    uint32_t* list = w.cand_pool + qi * w.kcand;
+    // 1. the predicate survivors, compacted in place as original ids (each chunk is read
+    //    before the barrier and written at or below its own start)
     for (int base = 0; base < nc; base += kThreads) {
         const int e = base + t;
         bool keep = false;
         uint32_t pool = kInvalid;
         if (e < nc) {
-            pool = w.cand_pool[qi * w.kcand + e];
+            pool = list[e];
             keep = pool != kInvalid;
             if (keep && pred_q) {
                 const float* lab = D.labels + (uint64_t)pool * lbl;
@@ -1314,35 +1317,45 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) s_wsum[warp] = __popc(bal);
         __syncthreads();
-        int before = 0, tot = 0;
+        int before = s_ns, tot = 0;
         for (int i = 0; i < nw; i++) {
             before += i < warp ? s_wsum[i] : 0;
             tot += s_wsum[i];
         }
-        if (keep) s_chunk[before + __popc(bal & ((1u << lane) - 1))] = pool;
+        if (keep) list[before + __popc(bal & ((1u << lane) - 1))] = D.ids[pool];
         __syncthreads();
-        for (int i = warp; i < tot; i += nw) {
-            const uint32_t id = D.ids[s_chunk[i]];
+        if (t == 0) s_ns += tot;
+    }
+    __syncthreads();
+    const int ns = s_ns;
+    // 2. exact distances in rounds of cap - kq rows: every warp takes rows of the round, the
+    //    keys (distance, id) below the running k-th go to the buffer, which is sorted and cut
+    //    to kq after each round
+    const int per_round = max(cap - kq, 1);
+    for (int r0 = 0; r0 < ns; r0 += per_round) {
+        const int r1 = min(ns, r0 + per_round);
+        for (int i = r0 + warp; i < r1; i += nw) {
+            const uint32_t id = list[i];
             const float* row = data + (uint64_t)id * d;
-            float s = 0.f;
+            float sq = 0.f;
             for (int j = lane; j < d; j += 32) {
                 const float df = s_q[j] - __ldg(row + j);
-                s = fmaf(df, df, s);
+                sq = fmaf(df, df, sq);
             }
-            s = warp_sum(s);
-            const uint64_t key = ((uint64_t)float_key(s) << 32) | id;
+            sq = warp_sum(sq);
+            const uint64_t key = ((uint64_t)float_key(sq) << 32) | id;
             if (lane == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
         }
         __syncthreads();
         const int c = s_cnt;
         __syncthreads();
-        if (c > cap - kThreads) {
+        if (r1 < ns && c > kq) {  // more rows follow: keep the kq best
             for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
             __syncthreads();
             block_bitonic_sort(s_keys, cap);
             if (t == 0) {
-                s_cnt = min(c, kq);
-                if (c >= kq) s_th = s_keys[kq - 1];
+                s_cnt = kq;
+                s_th = s_keys[kq - 1];
             }
             __syncthreads();
         }
@@ -1798,7 +1811,7 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     launches++;
     tm.mark("select");
     if (mode != kPre) {
-        const int rcap = (int)next_pow2(k + kThreads);
+        const int rcap = (int)next_pow2(k + 4 * kThreads);  // rounds of rcap - k exact distances
         const size_t sm_ref = sizeof(uint64_t) * rcap + sizeof(float) * D.d + 16;
         CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ref));
         k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, c.queries, c.data, rcap, mode == kPost ? 1 : 0, l, w,
