@@ -201,7 +201,7 @@ def _check_algorithm(algorithm: str) -> None:
     if a == "super-grid":
         return
     if a in ("pq", "prefilter", "sorting", "parafilter", "ivf-ivf_pq", "grid-ivf_pq", "cagra-post", "ivfpq-post"):
-        raise HDGError(6, f"algorithm '{algorithm}' is not part of this build (only super-grid)")
+        raise HDGError(6, f"algorithm '{algorithm}' is not implemented by this library (only super-grid)")
     raise HDGError(1, f"Unknown index type: {algorithm}")
 
 

@@ -61,7 +61,7 @@ static void check_algorithm(const char* algorithm) {
     for (const char* k : known)
         if (a == k)
             fail(HDG_ERR_UNSUPPORTED, std::string("algorithm '") + algorithm +
-                                          "' is not part of this build (only super-grid)");
+                                          "' is not implemented by this library (only super-grid)");
     fail(HDG_ERR_INVALID_ARG, std::string("Unknown index type: ") + algorithm);
 }
 

@@ -7,7 +7,7 @@ labelled with the cheapest setting -- fewest bytes scanned -- whose recall@k aga
 exact filtered kNN reaches ``target``; when none does, the setting with the best recall.
 The MLP (48 -> 128 -> 128 -> 2, BF16, trained by the library's own kernels) regresses
 log2(probe count) and classifies the schedule.  The plain schedule stays the fallback
-(LEARNED=0) and, with the brute-force kNN, the judge of the learned schedule's recall.
+(LEARNED=0) and, with the brute-force kNN, the yardstick of the learned schedule's recall.
 """
 from __future__ import annotations
 

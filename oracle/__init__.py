@@ -2,7 +2,8 @@
 
 ctypes bindings to liboracle.so (oracle/hdg_oracle.cpp), a plain C++ restatement of the
 reference's query schedule plus an FP64 filtered brute-force kNN.  Only tests/,
-__graft_entry__.smoke() and bench.py's CPU-baseline leg use it, always as the checker.
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use it, to check results, never
+to produce them.
 """
 from __future__ import annotations
 

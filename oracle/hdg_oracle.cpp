@@ -1,7 +1,8 @@
 // HDGrid oracle -- TEST INFRASTRUCTURE ONLY.
 //
 // A plain C++ (OpenMP, no CUDA) restatement of the HDGrid "super-grid" filtered query path,
-// used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.
+// used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg to check results,
+// never to produce them.
 // Nothing in the product links or calls this library.
 //
 // Each function cites the reference file:line it restates (paths inside the HDGrid project).
