@@ -121,13 +121,21 @@ def barrier(world):
         torch.distributed.barrier()
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank's value, all-reduced with MAX (a collective that
+    every rank calls in the same order)."""
     import torch
     if world == 1:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(world: int, nq: int, steps: int, total_ms: float) -> float:
+    """Whole-job queries per second: every rank answers its own full replica batch of nq
+    queries per step (weak scaling), timed as the slowest rank."""
+    return world * nq * steps / (total_ms / 1e3)
 
 
 def cpu_baseline_bruteforce(ws, n_sample: int):
@@ -378,7 +386,7 @@ def run_hdgrid(args):
         idx.set_param("sub_lists", int(p5["sub_lists"]))
         idx.set_param("learned", 1)
 
-    value = world * nq * args.steps / (total_ms / 1e3)
+    value = replica_value(world, nq, args.steps, total_ms)
     peak, peak_kind = hbm_peak()
     info = idx.info()
     p = hg.parse_config(ws["hdgrid_conf"])
