@@ -3,14 +3,16 @@
 // (src/core/refine.cu:36-75) for the ranking step of k_coarse; the chosen set is still
 // decided by exact FP32 distances re-checked inside a provable error band.
 //
-// One CTA = 128 queries x 128 centroids, 128 threads.  K runs in chunks of 64: all threads
-// copy the chunk of A (queries) and B (centroids) into shared memory in the K-major
-// "no swizzle" canonical UMMA layout (8-row x 16-byte core matrices; K chunks of 8 elements
-// LBO bytes apart, 8-row groups SBO bytes apart), one elected thread issues four
-// tcgen05.mma (M=128, N=128, K=16) and a tcgen05.commit to an mbarrier, everyone waits on
-// it.  The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31
-// = rows of the tile) and writes S.  Every wait is bounded: on expiry the kernel records an
-// error in *err and stops instead of hanging.
+// One CTA = 128 queries x 128 centroids, 128 threads.  K runs in chunks of 64 through two
+// shared-memory stages: all threads copy chunk kc+1 of A (queries) and B (centroids) with
+// cp.async (16 bytes, zero-filled past the matrix edges) into the K-major "no swizzle"
+// canonical UMMA layout (8-row x 16-byte core matrices; K chunks of 8 elements LBO bytes
+// apart, 8-row groups SBO bytes apart) while the tensor core runs chunk kc: one elected
+// thread issues four tcgen05.mma (M=128, N=128, K=16) per chunk and a tcgen05.commit to the
+// stage's mbarrier, which is waited on only before that stage is refilled.  The epilogue
+// reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows of the
+// tile) and writes S.  Every wait is bounded: on expiry the kernel records an error in *err,
+// lets its own copies land and stops instead of hanging.
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -21,7 +23,7 @@ namespace hdg {
 
 constexpr int GM = 128, GN = 128, GK = 64;  // tile
 constexpr int kGemmThreads = 128;
-constexpr uint32_t kRegion = 48 * 1024;        // operand region per matrix (slack for descriptor reads)
+constexpr uint32_t kStage = 16 * 1024;         // one 128 x 64 bf16 chunk in the canonical layout
 constexpr uint32_t kLBO = (GM / 8) * 128;      // bytes between the two 8-element K chunks
 constexpr uint32_t kSBO = 128;                 // bytes between 8-row groups
 constexpr long long kSpinLimit = 1ll << 26;
@@ -67,19 +69,24 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 }
 
 // out[r][n] = sum_k A[r][k] * B[n][k]; A [rows x d] bf16, B [cols x d] bf16, out row stride ldo.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// out[r][n] = sum_k A[r][k] * B[n][k]; A [rows x d] bf16, B [cols x d] bf16, out row stride ldo.
 __global__ void __launch_bounds__(kGemmThreads) k_umma_dot(const __nv_bfloat16* __restrict__ A, uint64_t rows,
                                                            const __nv_bfloat16* __restrict__ B, uint64_t cols,
                                                            int d, float* __restrict__ out, uint64_t ldo,
                                                            int* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* sA = smem;
-    unsigned char* sB = smem + kRegion;
-    __shared__ __align__(8) uint64_t s_bar;
+    extern __shared__ __align__(1024) unsigned char smem[];  // stage s: A at 2s*kStage, B at (2s+1)*kStage
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const uint64_t r0 = (uint64_t)blockIdx.x * GM, c0 = (uint64_t)blockIdx.y * GN;
-    const uint32_t bar = smem_u32(&s_bar);
+    const uint32_t sbase = smem_u32(smem);
+    const uint32_t bar[2] = {smem_u32(&s_bar[0]), smem_u32(&s_bar[1])};
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(GN));
@@ -87,39 +94,53 @@ __global__ void __launch_bounds__(kGemmThreads) k_umma_dot(const __nv_bfloat16* 
     }
     if (t == 0) {
         s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar[0]), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar[1]), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    // zero the operand regions once: rows beyond the matrix edge stay zero
-    for (uint32_t i = t * 16; i < 2 * kRegion; i += kGemmThreads * 16)
-        *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
+    // chunk kc -> stage s: every 16-byte piece of the 128 x 64 tiles of A and B
+    auto load = [&](int kc, int st) {
+        const int k0 = kc * GK;
+        const uint32_t sa = sbase + (uint32_t)(2 * st) * kStage, sb = sa + kStage;
+        for (int p = t; p < GM * (GK / 8); p += kGemmThreads) {
+            const int row = p >> 3, kk = (p & 7) * 8;
+            const bool kin = k0 + kk < d;
+            const bool va = kin && r0 + row < rows, vb = kin && c0 + row < cols;
+            cp_async16(sa + canon_off(row, kk), va ? (const void*)(A + (r0 + row) * d + k0 + kk) : (const void*)A, va);
+            cp_async16(sb + canon_off(row, kk), vb ? (const void*)(B + (c0 + row) * d + k0 + kk) : (const void*)B, vb);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
-    uint32_t phase = 0;
+    uint32_t phase[2] = {0u, 0u};
     const int nchunks = (d + GK - 1) / GK;
+    load(0, 0);
     for (int kc = 0; kc < nchunks; kc++) {
-        const int k0 = kc * GK;
-        // copy 16-byte pieces: piece p -> (row = p / 8, kk = (p % 8) * 8)
-        for (int p = t; p < GM * (GK / 8); p += kGemmThreads) {
-            const int row = p >> 3, kk = (p & 7) * 8;
-            uint4 va = make_uint4(0, 0, 0, 0), vb = make_uint4(0, 0, 0, 0);
-            if (k0 + kk < d) {
-                if (r0 + row < rows) va = *reinterpret_cast<const uint4*>(A + (r0 + row) * d + k0 + kk);
-                if (c0 + row < cols) vb = *reinterpret_cast<const uint4*>(B + (c0 + row) * d + k0 + kk);
+        const int st = kc & 1;
+        if (kc + 1 < nchunks) {
+            const int s1 = st ^ 1;
+            if (kc >= 1) {  // stage s1 was read by chunk kc - 1's MMAs
+                if (!mbar_wait(bar[s1], phase[s1])) s_fail = 1;
+                phase[s1] ^= 1u;
             }
-            *reinterpret_cast<uint4*>(sA + canon_off(row, kk)) = va;
-            *reinterpret_cast<uint4*>(sB + canon_off(row, kk)) = vb;
+            load(kc + 1, s1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (s_fail) break;
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t sa = sbase + (uint32_t)(2 * st) * kStage, sb = sa + kStage;
 #pragma unroll
             for (int ks = 0; ks < GK / 16; ks++) {
-                const uint64_t da = umma_desc(smem_u32(sA) + ks * 2 * kLBO);
-                const uint64_t db = umma_desc(smem_u32(sB) + ks * 2 * kLBO);
+                const uint64_t da = umma_desc(sa + ks * 2 * kLBO);
+                const uint64_t db = umma_desc(sb + ks * 2 * kLBO);
                 const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
@@ -127,14 +148,17 @@ __global__ void __launch_bounds__(kGemmThreads) k_umma_dot(const __nv_bfloat16* 
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
                     "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar[st])
                          : "memory");
         }
-        if (!mbar_wait(bar, phase)) s_fail = 1;
-        phase ^= 1u;
-        __syncthreads();
-        if (s_fail) break;
     }
+    // the last commit covers every earlier MMA of this thread
+    if (!s_fail) {
+        const int st = (nchunks - 1) & 1;
+        if (!mbar_wait(bar[st], phase[st])) s_fail = 1;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!s_fail) {
         const uint64_t row = r0 + warp * 32 + lane;
@@ -176,7 +200,7 @@ __global__ void k_f32_to_bf16_rows(const float* __restrict__ x, uint64_t n, __nv
     if (lane == 0 && norms) norms[r] = s;
 }
 
-size_t umma_smem_bytes() { return 2 * kRegion; }
+size_t umma_smem_bytes() { return 4 * kStage; }
 
 // S [rows x cols] (row stride ldo) = A . B^T in BF16 with FP32 accumulation.
 void umma_dot(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
