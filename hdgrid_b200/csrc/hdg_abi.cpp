@@ -322,14 +322,23 @@ hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_
         HDG_REQUIRE(index && name, HDG_ERR_INVALID_ARG, "null argument");
         const hdg::QueryCtx* cx = index->last_ctx;
         HDG_REQUIRE(cx, HDG_ERR_STATE, "no query has run on this index");
-        auto it = cx->layout.find(name);
-        HDG_REQUIRE(it != cx->layout.end(), HDG_ERR_INVALID_ARG, std::string("no workspace buffer named ") + name);
-        const size_t off = it->second.first, sz = it->second.second;
+        const char* src = nullptr;
+        size_t sz = 0;
+        if (std::string(name) == "distances") {  // the ADC distance buffer (qoff gives the rows)
+            src = static_cast<const char*>(cx->dist_buf.ptr);
+            sz = cx->dist_buf.bytes;
+        } else {
+            auto it = cx->layout.find(name);
+            HDG_REQUIRE(it != cx->layout.end(), HDG_ERR_INVALID_ARG,
+                        std::string("no workspace buffer named ") + name);
+            src = static_cast<const char*>(cx->work.ptr) + it->second.first;
+            sz = it->second.second;
+        }
         if (bytes_needed) *bytes_needed = sz;
         if (!host_dst) return;
         HDG_REQUIRE(bytes >= sz, HDG_ERR_INVALID_ARG, "destination too small");
         CK(cudaDeviceSynchronize());
-        CK(cudaMemcpy(host_dst, static_cast<const char*>(cx->work.ptr) + off, sz, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(host_dst, src, sz, cudaMemcpyDeviceToHost));
     });
 }
 

@@ -217,7 +217,9 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
 
 /* Copy a named intermediate buffer of the last query to host memory (parity tests).
  * Names: "box", "cells", "zrange", "list_counts", "cluster_counts", "probe_clusters",
- * "probe_lists", "range_start", "range_len", "cand_pool", "cand_count", "scalars". */
+ * "probe_lists", "range_start", "range_len", "cand_pool", "cand_count", "scalars", "qoff",
+ * "qstat", and "distances" (the f32 ADC distance of every scanned candidate, query rows at
+ * the "qoff" offsets). */
 hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,
                            size_t bytes, size_t* bytes_needed);
 
