@@ -277,6 +277,28 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* __restrict__
     return lo;
 }
 
+// lower_bound of two keys in the same sorted array, the two searches interleaved so their
+// dependent loads overlap (each result equals lower_bound_u64's)
+__device__ __forceinline__ void lower_bound_u64_x2(const uint64_t* __restrict__ a, uint32_t n, uint64_t k1,
+                                                   uint64_t k2, uint32_t* r1, uint32_t* r2) {
+    uint32_t lo1 = 0, hi1 = n, lo2 = 0, hi2 = n;
+    while (lo1 < hi1 || lo2 < hi2) {
+        const uint32_t m1 = (lo1 + hi1) >> 1, m2 = (lo2 + hi2) >> 1;
+        const bool b1 = lo1 < hi1, b2 = lo2 < hi2;
+        const uint64_t v1 = b1 ? a[m1] : 0, v2 = b2 ? a[m2] : 0;
+        if (b1) {
+            if (v1 < k1) lo1 = m1 + 1;
+            else hi1 = m1;
+        }
+        if (b2) {
+            if (v2 < k2) lo2 = m2 + 1;
+            else hi2 = m2;
+        }
+    }
+    *r1 = lo1;
+    *r2 = lo2;
+}
+
 // One sub-range of a probed list's Morton interval [lo, hi) when is_split = 1.
 // get_query_end_points_kernel (zorder.cu:596-654) cuts the interval into
 // min(len, n_split) near-equal parts; zorder_range_query_kernel (:474-594) then moves each
@@ -457,10 +479,14 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     block_bitonic_sort(s_keys, sort_n2);
     const int nps = min(Psq, s_nvalid);
     // the probed lists in list-id (= pool) order, so candidate positions follow pool order
-    const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
-    for (int i = t; i < sort_n3; i += blockDim.x) s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
-    __syncthreads();
-    block_bitonic_sort(s_keys, sort_n3);
+    // (with every list taken the keys carry no distance and are in list-id order already)
+    if (!all_l) {
+        const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
+        for (int i = t; i < sort_n3; i += blockDim.x)
+            s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
+        __syncthreads();
+        block_bitonic_sort(s_keys, sort_n3);
+    }
     const uint64_t zlo = w.zrange[qi * 2], zhi = w.zrange[qi * 2 + 1];
     uint32_t my_cand = 0, my_exact = 0;
     const int ns = w.nsplit;
@@ -473,8 +499,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
             list = (uint32_t)s_keys[i];
             off = D.list_off[list];
             const uint32_t size = D.list_off[list + 1] - off;
-            lo = lower_bound_u64(D.zcodes + off, size, zlo);
-            hi = lower_bound_u64(D.zcodes + off, size, zhi + 1);
+            lower_bound_u64_x2(D.zcodes + off, size, zlo, zhi + 1, &lo, &hi);
             start = off + lo;
             len = hi - lo;
             my_exact += w.list_counts[qi * D.n_lists + list];
