@@ -277,26 +277,65 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* __restrict__
     return lo;
 }
 
-// lower_bound of two keys in the same sorted array, the two searches interleaved so their
-// dependent loads overlap (each result equals lower_bound_u64's)
-__device__ __forceinline__ void lower_bound_u64_x2(const uint64_t* __restrict__ a, uint32_t n, uint64_t k1,
-                                                   uint64_t k2, uint32_t* r1, uint32_t* r2) {
-    uint32_t lo1 = 0, hi1 = n, lo2 = 0, hi2 = n;
-    while (lo1 < hi1 || lo2 < hi2) {
-        const uint32_t m1 = (lo1 + hi1) >> 1, m2 = (lo2 + hi2) >> 1;
-        const bool b1 = lo1 < hi1, b2 = lo2 < hi2;
-        const uint64_t v1 = b1 ? a[m1] : 0, v2 = b2 ? a[m2] : 0;
-        if (b1) {
-            if (v1 < k1) lo1 = m1 + 1;
-            else hi1 = m1;
-        }
-        if (b2) {
-            if (v2 < k2) lo2 = m2 + 1;
-            else hi2 = m2;
-        }
+// N lower_bounds (key k[i] in the sorted a[i][0, n[i])) with their searches interleaved so the
+// dependent loads overlap; each result equals lower_bound_u64's
+template <int N>
+__device__ __forceinline__ void lower_bound_u64_multi(const uint64_t* const (&a)[N], const uint32_t (&n)[N],
+                                                      const uint64_t (&k)[N], uint32_t (&r)[N]) {
+    uint32_t lo[N], hi[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        lo[i] = 0;
+        hi[i] = n[i];
     }
-    *r1 = lo1;
-    *r2 = lo2;
+    for (;;) {
+        bool any = false;
+        uint64_t v[N];
+        uint32_t m[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            m[i] = (lo[i] + hi[i]) >> 1;
+            v[i] = lo[i] < hi[i] ? a[i][m[i]] : 0;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (lo[i] < hi[i]) {
+                if (v[i] < k[i]) lo[i] = m[i] + 1;
+                else hi[i] = m[i];
+            }
+            any |= lo[i] < hi[i];
+        }
+        if (!any) break;
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) r[i] = lo[i];
+}
+
+// Stable in-place compaction of the keys that are not ~0 to the front of keys[0, n) (the
+// rest set to ~0); all threads of the block.  s_wc: 32 words of shared scratch.
+__device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32_t* s_wc) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    uint32_t base = 0;
+    for (int r = 0; r < n; r += blockDim.x) {
+        const int e = r + t;
+        const uint64_t v = e < n ? keys[e] : ~0ull;
+        const bool f = v != ~0ull;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) s_wc[warp] = __popc(bal);
+        __syncthreads();  // every read of this round is done before any write
+        uint32_t off = 0, tot = 0;
+        for (int i = 0; i < nw; i++) {
+            const uint32_t c = s_wc[i];
+            off += i < warp ? c : 0u;
+            tot += c;
+        }
+        // the destination is below r + blockDim.x: no later round's key is overwritten
+        if (f) keys[base + off + __popc(bal & ((1u << lane) - 1u))] = v;
+        __syncthreads();
+        base += tot;
+    }
+    for (int e = (int)base + t; e < n; e += blockDim.x) keys[e] = ~0ull;
+    __syncthreads();
 }
 
 // One sub-range of a probed list's Morton interval [lo, hi) when is_split = 1.
@@ -360,6 +399,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     float* s_q = reinterpret_cast<float*>(s_keys + max(sort_n1, sort_n2));
     __shared__ uint32_t s_chosen[1024];
     __shared__ uint32_t s_red[2];
+    __shared__ uint32_t s_wc[32];
     __shared__ int s_nvalid;
     __shared__ float s_bound;
     const uint64_t qi = blockIdx.x;
@@ -412,7 +452,9 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
         s_keys[c] = key;
     }
     __syncthreads();
-    block_bitonic_sort(s_keys, sort_n1);
+    // with every non-empty cluster taken the keys hold no distance: cluster order, compacted
+    if (all_c) block_compact_keys(s_keys, sort_n1, s_wc);
+    else block_bitonic_sort(s_keys, sort_n1);
     const int npc = min(Pc, s_nvalid);
     for (int i = t; i < Pc; i += blockDim.x) {
         const uint32_t c = i < npc ? (uint32_t)s_keys[i] : kInvalid;
@@ -476,7 +518,10 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
         s_keys[e] = key;
     }
     __syncthreads();
-    block_bitonic_sort(s_keys, sort_n2);
+    // every list taken and every cluster taken (chosen clusters in cluster order): the keys are
+    // already in list-id order and only need compacting; otherwise the sort orders them
+    if (all_l && all_c) block_compact_keys(s_keys, sort_n2, s_wc);
+    else block_bitonic_sort(s_keys, sort_n2);
     const int nps = min(Psq, s_nvalid);
     // the probed lists in list-id (= pool) order, so candidate positions follow pool order
     // (with every list taken the keys carry no distance and are in list-id order already)
@@ -493,30 +538,53 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     int box[2 * kMaxDims];
     if (w.is_split)
         for (int i = 0; i < 2 * g.l; i++) box[i] = w.cells[qi * 2 * g.l + i];
-    for (int i = t; i < Ps; i += blockDim.x) {
-        uint32_t list = kInvalid, start = 0, len = 0, off = 0, lo = 0, hi = 0;
-        if (i < nps) {
-            list = (uint32_t)s_keys[i];
-            off = D.list_off[list];
-            const uint32_t size = D.list_off[list + 1] - off;
-            lower_bound_u64_x2(D.zcodes + off, size, zlo, zhi + 1, &lo, &hi);
-            start = off + lo;
-            len = hi - lo;
-            my_exact += w.list_counts[qi * D.n_lists + list];
+    // two probed lists per thread and step: their four Morton bound searches interleaved
+    for (int i0 = t; i0 < Ps; i0 += 2 * blockDim.x) {
+        const uint64_t* arr[4];
+        uint32_t nn[4], rr[4], list[2], off[2];
+        uint64_t kk[4];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = i0 + u * (int)blockDim.x;
+            uint32_t size = 0;
+            list[u] = kInvalid;
+            off[u] = 0;
+            if (i < nps) {
+                list[u] = (uint32_t)s_keys[i];
+                off[u] = D.list_off[list[u]];
+                size = D.list_off[list[u] + 1] - off[u];
+            }
+            arr[2 * u] = arr[2 * u + 1] = D.zcodes + off[u];
+            nn[2 * u] = nn[2 * u + 1] = size;
+            kk[2 * u] = zlo;
+            kk[2 * u + 1] = zhi + 1;
         }
-        w.probe_lists[qi * Ps + i] = list;
-        const uint64_t r0 = (qi * Ps + i) * (uint64_t)ns;
-        if (!w.is_split) {
-            w.range_start[r0] = start;
-            w.range_len[r0] = len;
-            my_cand += len;
-        } else {
-            for (int sp = 0; sp < ns; sp++) {
-                uint32_t st = kInvalid, ln = 0;
-                if (i < nps) split_subrange(D.zcodes, off, lo, hi, sp, ns, box, g, &st, &ln);
-                w.range_start[r0 + sp] = st;
-                w.range_len[r0 + sp] = ln;
-                my_cand += ln;
+        lower_bound_u64_multi<4>(arr, nn, kk, rr);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = i0 + u * (int)blockDim.x;
+            if (i >= Ps) break;
+            const uint32_t lo = rr[2 * u], hi = rr[2 * u + 1];
+            uint32_t start = 0, len = 0;
+            if (i < nps) {
+                start = off[u] + lo;
+                len = hi - lo;
+                my_exact += w.list_counts[qi * D.n_lists + list[u]];
+            }
+            w.probe_lists[qi * Ps + i] = list[u];
+            const uint64_t r0 = (qi * Ps + i) * (uint64_t)ns;
+            if (!w.is_split) {
+                w.range_start[r0] = start;
+                w.range_len[r0] = len;
+                my_cand += len;
+            } else {
+                for (int sp = 0; sp < ns; sp++) {
+                    uint32_t st = kInvalid, ln = 0;
+                    if (i < nps) split_subrange(D.zcodes, off[u], lo, hi, sp, ns, box, g, &st, &ln);
+                    w.range_start[r0 + sp] = st;
+                    w.range_len[r0 + sp] = ln;
+                    my_cand += ln;
+                }
             }
         }
     }
