@@ -77,16 +77,32 @@ __global__ void __launch_bounds__(256) k_features(IndexDev D, GridMeta g, const 
     }
     // centroid distances, one warp per centroid: the lanes read a row with coalesced loads
     // (the features only rank and log-scale these distances; no summation order is implied)
+    // Four centroids per warp and step keep four independent row loads in flight; each
+    // centroid's sum is formed exactly as with one per step (per-lane FMA chain, warp sum).
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    for (int c = warp; c < C; c += nw) {
-        const float* row = D.centers + (uint64_t)c * d;
-        float sq = 0.f;
-        for (int i = lane; i < d; i += 32) {
-            const float df = s_q[i] - __ldg(row + i);
-            sq = fmaf(df, df, sq);
+    constexpr int kCU = 4;
+    for (int c0 = warp; c0 < C; c0 += kCU * nw) {
+        const float* row[kCU];
+        float sq[kCU];
+#pragma unroll
+        for (int u = 0; u < kCU; u++) {
+            row[u] = D.centers + (uint64_t)min(c0 + u * nw, C - 1) * d;
+            sq[u] = 0.f;
         }
-        sq = warp_sum(sq);
-        if (lane == 0) s_keys[c] = ((uint64_t)float_key(sq) << 32) | (uint32_t)c;
+        for (int i = lane; i < d; i += 32) {
+            const float qv = s_q[i];
+#pragma unroll
+            for (int u = 0; u < kCU; u++) {
+                const float df = qv - __ldg(row[u] + i);
+                sq[u] = fmaf(df, df, sq[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kCU; u++) {
+            const float v = warp_sum(sq[u]);
+            const int c = c0 + u * nw;
+            if (lane == 0 && c < C) s_keys[c] = ((uint64_t)float_key(v) << 32) | (uint32_t)c;
+        }
     }
     atomicAdd(&s_tot, tot);
     atomicAdd(&s_nz, nz);
