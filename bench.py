@@ -299,12 +299,15 @@ def run_hdgrid(args):
     cand_q = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64)
     cand = int(cand_q.sum())
     info0, p0 = idx.info(), hg.parse_config(ws["hdgrid_conf"])
-    # algorithmic scan bytes: M code bytes per candidate, plus 4*l label bytes for every
-    # candidate whose query evaluates the predicate inside the scan
+    # algorithmic scan bytes: M code bytes per candidate of a post-filter query; for a
+    # predicate-first query 4*l label bytes per candidate and M code bytes per candidate that
+    # passes the predicate (the ADC of the others is not needed)
     pre_q = np.full(nq, p0["exps0"] <= 1)
     if ws["name"] == "config5":
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
-    scan_bytes = float((cand_q * (info0["M"] + 4 * info0["l"] * pre_q)).sum())
+    pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
+    scan_bytes = float(np.where(pre_q, cand_q * (4 * info0["l"]) + pass_q * info0["M"], cand_q * info0["M"]).sum())
+    pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
 
     # the batched workloads (10M x 128) run as the persistent scan under a captured CUDA graph,
     # with the scan's threads x candidates-per-thread and work-item size picked by the
@@ -402,6 +405,7 @@ def run_hdgrid(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture, configs of the benchmark)",
         "config": workload_config(ws, args) | {"recall_at_k": rec, "build_s": round(t_build, 2),
                                                "candidates_per_step": cand,
+                                               "predicate_pass_share": pass_share,
                                                "max_rel_dist_err_vs_fp64": max_rel}
                   | ({"schedule": "learned (LEARNED=1)", "plain_schedule_same_batch": plain_ref}
                      if plain_ref is not None else {})

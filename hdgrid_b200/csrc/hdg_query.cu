@@ -817,6 +817,30 @@ struct ScanShared {
     int item, query;
 };
 
+// ADC of one candidate's 32-subspace group g in the fast path's lane-rotated order (the
+// same loads, rotation and lookups as the interleaved loop of k_scan_fast)
+__device__ __forceinline__ void adc_group1(const uint4* cp, uint64_t n_pts, int g, uint32_t R, uint32_t sh,
+                                           uint32_t lane4, const float* s_lut, float& s0, float& s1) {
+    const uint4 a = __ldg(cp + (2 * g) * n_pts), b = __ldg(cp + (2 * g + 1) * n_pts);
+    uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    rotate_words(wv, R);
+    uint32_t x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) x[i] = __funnelshift_r(wv[i], wv[(i + 1) & 7], sh);
+    const char* L = reinterpret_cast<const char*>(s_lut + g * (kCodes * 64));
+#pragma unroll
+    for (int st = 0; st < 32; st += 2) {
+        const uint32_t a0 = __byte_perm(x[st >> 2], lane4, 0x5504u | ((st & 3) << 4));
+        const uint32_t a1 = __byte_perm(x[st >> 2], lane4, 0x5504u | (((st + 1) & 3) << 4));
+        add_f32x2(s0, s1, reinterpret_cast<const float*>(L + a0)[st], reinterpret_cast<const float*>(L + a1)[st + 1]);
+    }
+}
+
+// Predicate-first candidates queued per lane before their ADC (fast path, one 32-subspace
+// group, one candidate per thread): the queue of each lane holds up to kPreQueue entries.
+constexpr int kPreQueue = 8;
+constexpr bool scan_compacts(int G, int CPT) { return G == 1 && CPT == 1; }
+
 __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int qq, uint32_t* s_pre,
                                                 uint32_t* s_start, uint32_t* s_warp) {
     for (int i = threadIdx.x; i < Ps; i += blockDim.x) {
@@ -833,11 +857,13 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
 // candidates; CPT candidates per thread are interleaved step by step so every thread keeps
 // CPT independent load->add chains in flight.
 template <int G, int NT, int CPT>
-__global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __restrict__ queries, int Ps,
+__global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast(IndexDev D, const float* __restrict__ queries, int Ps,
                                                      int pre, int lbl, uint64_t q, Workspace w) {
     extern __shared__ __align__(16) float s_lut[];  // [G][256][64]
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 64);  // [Ps + 1]
     uint32_t* s_start = s_pre + Ps + 1;                                       // [Ps]
+    // [NT/32][2][kPreQueue][32] queued (position, pool row) pairs, 16-byte aligned
+    uint32_t* s_queue = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_start + Ps) + 15) & ~uintptr_t(15));
     __shared__ ScanShared s;
     __shared__ uint32_t s_warp[32];
     __shared__ float s_box[2 * kMaxDims];
@@ -924,7 +950,72 @@ __global__ void __launch_bounds__(NT, 1) k_scan_fast(IndexDev D, const float* __
         }
         const uint4* planes = reinterpret_cast<const uint4*>(D.codes);
         const uint64_t n_pts = D.n;
-        for (uint32_t eb = wb + lane; eb < we; eb += kStep) {
+        bool compacted = false;
+        if constexpr (scan_compacts(G, CPT)) {
+            if (preq) {
+                // Predicate first, ADC for the survivors only.  A predicate step tests one
+                // position per lane (position mod 32 = lane, as in the loop below) and queues
+                // a survivor in that lane's queue; an ADC step takes one queued candidate per
+                // lane, so every sum is formed by the lane, and in the order, of the loop below.
+                // ADC steps run when every lane has a candidate queued, when a queue is full,
+                // and at the end of the span until the queues are empty.
+                uint32_t* qe = s_queue + (uint32_t)(t >> 5) * (2 * kPreQueue * 32);
+                uint32_t* qp = qe + kPreQueue * 32;
+                int qh = 0, qn = 0, rr = r[0];
+                uint32_t eb = wb;
+                for (;;) {
+                    const bool more = eb < we;  // warp-uniform
+                    const bool adc = __all_sync(0xffffffffu, qn > 0) || __any_sync(0xffffffffu, qn == kPreQueue) ||
+                                     (!more && __any_sync(0xffffffffu, qn > 0));
+                    if (adc) {
+                        const bool live = qn > 0;
+                        uint32_t e = 0, row = 0;  // an idle lane reads row 0 (in bounds), result discarded
+                        if (live) {
+                            e = qe[qh * 32 + lane];
+                            row = qp[qh * 32 + lane];
+                            qh = (qh + 1) & (kPreQueue - 1);
+                            qn--;
+                        }
+                        float s0 = 0.f, s1 = 0.f;
+                        adc_group1(planes + row, n_pts, 0, R, sh, lane4, s_lut, s0, s1);
+                        s0 += s1;
+                        if (live) {
+                            if (s0 < INFINITY) {
+                                const uint32_t key = float_key(s0);
+                                kmin = min(kmin, key);
+                                kmax = max(kmax, key);
+                                nf++;
+                            }
+                            dst[e] = s0;
+                        }
+                        continue;
+                    }
+                    if (!more) break;
+                    const uint32_t e = eb + lane;
+                    if (e < we) {
+                        while (s_pre[rr + 1] <= e) rr++;
+                        const uint32_t pool = s_start[rr] + (e - s_pre[rr]);
+                        const float* lab = D.labels + (uint64_t)pool * lbl;
+                        bool pass = true;
+                        for (int i = 0; i < lbl; i++) {
+                            const float v = lab[i];
+                            if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
+                        }
+                        if (pass) {  // qn < kPreQueue here: a full queue forced an ADC step first
+                            const int slot = (qh + qn) & (kPreQueue - 1);
+                            qe[slot * 32 + lane] = e;
+                            qp[slot * 32 + lane] = pool;
+                            qn++;
+                        } else {
+                            dst[e] = INFINITY;
+                        }
+                    }
+                    eb += 32;
+                }
+                compacted = true;
+            }
+        }
+        for (uint32_t eb = wb + lane; !compacted && eb < we; eb += kStep) {
             const uint4* cp[CPT];
             bool live[CPT];
             float sum[CPT], sum1[CPT];  // even / odd steps, added at the end
@@ -1912,15 +2003,18 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     const size_t sm_tab = sizeof(uint32_t) * (2 * R + 1);
     if (!sync_sizing || sc[3] > 0) {
         if (fast) {
-            const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
+            // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
+            const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
+            size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
+            // the compacting variant (one group, one candidate per thread, 512 threads) adds the
+            // per-lane survivor queues: 2 x kPreQueue words per thread, 16-byte aligned
+            if (scan_compacts((int)G, cpt)) sm += 16 + sizeof(uint32_t) * 2 * kPreQueue * 512;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
                 kern<<<blocks, nt, sm, st>>>(D, c.queries, R, pre, l, q, w);
             };
-            // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
-            const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
             if (G == 1) {
                 if (cpt == 1) launch(k_scan_fast<1, 512, 1>, 512);
                 else if (cpt == 2) launch(k_scan_fast<1, 512, 2>, 512);

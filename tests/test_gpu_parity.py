@@ -171,6 +171,19 @@ def test_parity_prefilter_rotated_adc(cuda):
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
 
 
+def test_parity_prefilter_compacted_scan(cuda):
+    # M = 32 (one subspace group): predicate-first queries run the compacting scan -- the
+    # survivors queue per lane and their ADC runs in full warps, each sum formed by the lane
+    # of its position -- so ids and ADC distances still equal the oracle's bit for bit
+    ws = datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
+                          max_grids=4096, exps0=1)
+    _, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
+    valid = r["g_ids"] != INV
+    assert valid.any()
+    assert np.array_equal(r["g_ids"], r["o_ids"])
+    assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+
+
 def test_parity_prefilter_rotated_adc_fp16_lut(cuda):
     # LUT_FP16=1: entries rounded to binary16 and widened back to f32 in shared memory; the
     # oracle rounds the same way, so ids and distances still match bit for bit
