@@ -62,6 +62,7 @@ struct Workspace {
     uint32_t* cand_pool;     // [q x kcand]
     uint32_t* cand_count;    // [q]
     uint64_t kcand;
+    int surv_list;           // 1: the compacting scan lists each predicate-first query's survivors
     float* dist;             // [sum of candidates]
     float* S;                // [q x (C + L)] tensor-core dot products (nullptr: exact path only)
     uint64_t ldS;
@@ -839,6 +840,7 @@ __device__ __forceinline__ void adc_group1(const uint4* cp, uint64_t n_pts, int 
 // Predicate-first candidates queued per lane before their ADC (fast path, one 32-subspace
 // group, one candidate per thread): the queue of each lane holds up to kPreQueue entries.
 constexpr int kPreQueue = 8;
+constexpr int kPreStep = 4;  // positions per lane in one predicate step (<= kPreQueue / 2)
 constexpr bool scan_compacts(int G, int CPT) { return G == 1 && CPT == 1; }
 
 __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int qq, uint32_t* s_pre,
@@ -957,15 +959,21 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                 // position per lane (position mod 32 = lane, as in the loop below) and queues
                 // a survivor in that lane's queue; an ADC step takes one queued candidate per
                 // lane, so every sum is formed by the lane, and in the order, of the loop below.
-                // ADC steps run when every lane has a candidate queued, when a queue is full,
-                // and at the end of the span until the queues are empty.
+                // ADC steps run when every lane has a candidate queued, when a queue might not
+                // take a whole predicate step, and at the end of the span until the queues
+                // are empty.
                 uint32_t* qe = s_queue + (uint32_t)(t >> 5) * (2 * kPreQueue * 32);
                 uint32_t* qp = qe + kPreQueue * 32;
                 int qh = 0, qn = 0, rr = r[0];
+                const bool lab4 = lbl == 4 && (reinterpret_cast<uintptr_t>(D.labels) & 15) == 0;
+                float bx[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) bx[i] = lab4 ? s_box[i] : 0.f;
                 uint32_t eb = wb;
                 for (;;) {
                     const bool more = eb < we;  // warp-uniform
-                    const bool adc = __all_sync(0xffffffffu, qn > 0) || __any_sync(0xffffffffu, qn == kPreQueue) ||
+                    const bool adc = __all_sync(0xffffffffu, qn > 0) ||
+                                     __any_sync(0xffffffffu, qn > kPreQueue - kPreStep) ||
                                      (!more && __any_sync(0xffffffffu, qn > 0));
                     if (adc) {
                         const bool live = qn > 0;
@@ -987,30 +995,63 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                                 nf++;
                             }
                             dst[e] = s0;
+                            // the survivor's position, for a select that takes every survivor
+                            const uint32_t slot = atomicAdd(&w.cand_count[qq], 1u);
+                            if (slot < w.kcand) w.cand_pool[(uint64_t)qq * w.kcand + slot] = e;
                         }
                         continue;
                     }
                     if (!more) break;
-                    const uint32_t e = eb + lane;
-                    if (e < we) {
-                        while (s_pre[rr + 1] <= e) rr++;
-                        const uint32_t pool = s_start[rr] + (e - s_pre[rr]);
-                        const float* lab = D.labels + (uint64_t)pool * lbl;
-                        bool pass = true;
-                        for (int i = 0; i < lbl; i++) {
-                            const float v = lab[i];
-                            if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
-                        }
-                        if (pass) {  // qn < kPreQueue here: a full queue forced an ADC step first
-                            const int slot = (qh + qn) & (kPreQueue - 1);
-                            qe[slot * 32 + lane] = e;
-                            qp[slot * 32 + lane] = pool;
-                            qn++;
-                        } else {
-                            dst[e] = INFINITY;
+                    // kPreStep positions per lane (e, e + 32, ...), their label loads in flight
+                    // together (one 16-byte load each with 4 aligned label dims)
+                    uint32_t pe[kPreStep], pp[kPreStep];
+                    bool pv[kPreStep], ps[kPreStep];
+#pragma unroll
+                    for (int j = 0; j < kPreStep; j++) {
+                        pe[j] = eb + lane + 32u * j;
+                        pv[j] = pe[j] < we;
+                        pp[j] = 0;
+                        if (pv[j]) {
+                            while (s_pre[rr + 1] <= pe[j]) rr++;
+                            pp[j] = s_start[rr] + (pe[j] - s_pre[rr]);
                         }
                     }
-                    eb += 32;
+                    if (lab4) {
+                        float4 v[kPreStep];
+#pragma unroll
+                        for (int j = 0; j < kPreStep; j++)
+                            v[j] = pv[j] ? __ldg(reinterpret_cast<const float4*>(D.labels) + pp[j])
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                        for (int j = 0; j < kPreStep; j++)
+                            ps[j] = pv[j] && !(v[j].x < bx[0] || v[j].x > bx[1]) && !(v[j].y < bx[2] || v[j].y > bx[3]) &&
+                                    !(v[j].z < bx[4] || v[j].z > bx[5]) && !(v[j].w < bx[6] || v[j].w > bx[7]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < kPreStep; j++) {
+                            ps[j] = pv[j];
+                            if (pv[j]) {
+                                const float* lab = D.labels + (uint64_t)pp[j] * lbl;
+                                for (int i = 0; i < lbl; i++) {
+                                    const float v = lab[i];
+                                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) ps[j] = false;
+                                }
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < kPreStep; j++) {
+                        if (!pv[j]) continue;
+                        if (ps[j]) {  // qn <= kPreQueue - kPreStep before this step: room for all
+                            const int slot = (qh + qn) & (kPreQueue - 1);
+                            qe[slot * 32 + lane] = pe[j];
+                            qp[slot * 32 + lane] = pp[j];
+                            qn++;
+                        } else {
+                            dst[pe[j]] = INFINITY;
+                        }
+                    }
+                    eb += 32u * kPreStep;
                 }
                 compacted = true;
             }
@@ -1281,7 +1322,15 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             if (sel_bin(d, s_lv[l].lo, s_lv[l].inv) != s_lv[l].bin) return false;
         return true;
     };
-    if (need0 > 0 && nfin <= (uint32_t)K) {
+    // A predicate-first query scanned by the compacting scan has its survivors' positions
+    // listed in its candidate slots already (cand_count of them, its finite count): when all
+    // are selected, the list is the selection and the distance row need not be read.
+    const bool listed = w.surv_list && !sorted_out && q_prefilter(w, qi) && w.cand_count[qi] == nfin &&
+                        nfin <= (uint32_t)K && nfin <= w.kcand;
+    if (listed) {
+        if (t == 0) s_out = nfin;
+        __syncthreads();
+    } else if (need0 > 0 && nfin <= (uint32_t)K) {
         // every finite candidate is selected
         for (uint32_t e = t; e < total; e += blockDim.x) {
             const float d = dist[e];
@@ -2009,6 +2058,7 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
             // the compacting variant (one group, one candidate per thread, 512 threads) adds the
             // per-lane survivor queues: 2 x kPreQueue words per thread, 16-byte aligned
             if (scan_compacts((int)G, cpt)) sm += 16 + sizeof(uint32_t) * 2 * kPreQueue * 512;
+            w.surv_list = scan_compacts((int)G, cpt) ? 1 : 0;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
