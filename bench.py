@@ -225,6 +225,15 @@ def max_relative_error(ws, dist, ids, n_sample):
     return worst
 
 
+def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int) -> float:
+    """Bytes the ADC scan of one batch must read: M code bytes per candidate of a post-filter
+    query; for a predicate-first query 4*l label bytes per candidate plus M code bytes per
+    candidate that passes the predicate (the others need no ADC)."""
+    cand_q = np.asarray(cand_q, np.float64)
+    pass_q = np.asarray(pass_q, np.float64)
+    return float(np.where(np.asarray(pre_q, bool), cand_q * (4 * l) + pass_q * M, cand_q * M).sum())
+
+
 def scan_traffic(ws, candidates):
     """DRAM bytes of one k_scan_fast launch: the per-candidate figure of the committed ncu
     summary for this workload (dram__bytes_read.sum + dram__bytes_write.sum over the
@@ -306,7 +315,7 @@ def run_hdgrid(args):
     if ws["name"] == "config5":
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
     pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
-    scan_bytes = float(np.where(pre_q, cand_q * (4 * info0["l"]) + pass_q * info0["M"], cand_q * info0["M"]).sum())
+    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info0["M"], info0["l"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
 
     # the batched workloads (10M x 128) run as the persistent scan under a captured CUDA graph,

@@ -1,5 +1,6 @@
-"""The multi-process plumbing of bench.py on CPU ranks (gloo, world size 2): barrier,
-max-over-ranks timing and the whole-job value of the replicas-only path."""
+"""bench.py's host logic on CPU: the multi-process plumbing on gloo ranks (world size 2:
+barrier, max-over-ranks timing, the whole-job value of the replicas-only path) and the
+scan's algorithmic byte count behind the roofline."""
 import os
 import socket
 import sys
@@ -49,3 +50,12 @@ def test_two_rank_max_timing_and_replica_value():
     for rank, total, value in res:
         assert total == 20.0
         assert value == pytest.approx(2 * 1000 * 5 / 0.020)
+
+
+def test_algorithmic_scan_bytes():
+    # post-filter query: M code bytes per candidate; predicate-first: 4*l label bytes per
+    # candidate plus M code bytes per survivor
+    sys.path.insert(0, str(ROOT))
+    import bench
+    got = bench.algorithmic_scan_bytes([1000, 2000, 0], [900, 10, 0], [False, True, True], M=32, l=4)
+    assert got == 1000 * 32 + (2000 * 16 + 10 * 32)
