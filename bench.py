@@ -1,16 +1,27 @@
 """Benchmark: filtered ANN QPS of the HDGrid query path on B200.
 
-    python bench.py [--gpus N --steps K --warmup W] [--config config2] [--impl hdgrid|reference]
+    python bench.py [--gpus N --steps K --warmup W] [--config config5] [--impl hdgrid|reference]
 
-A step is one hdg_query over the whole query batch of the workload (index resident in HBM,
-queries and labels already on the device for ``value``).  ``e2e`` repeats the step through
-the public API with pinned host buffers: H2D of queries + labels, query, D2H of the results.
+Default workload (config5): 10,000,000 x 128 base, 4 int label dims with range filters, a
+10,000-query batch of the standard stream (per-query selectivity log-uniform in
+[0.01 %, 90 %], k drawn from {10, 100}), answered by the learned per-query schedule (BF16
+MLP, hdgrid_b200/learned_weights/config5.npy) under a captured CUDA graph with the scan's
+launch shape picked by the autotuner.  A step is one query of the whole batch: ``value`` is
+device-timed QPS with the index resident and the queries on the device; ``e2e`` repeats the
+step through the public API with pinned host buffers, the H2D copies of queries, labels and
+k's and the D2H copies of the results inside the timed region.  The plain HDGrid path is
+measured on the same batch under both of the reference's schedules (the post-filter budget
+min(exps0 * k * beta, max_row_len) with an exact re-rank, and the pre-filter schedule of
+exps0 <= 1) at every probe count, and the learned schedule's QPS is compared with the
+fastest plain setting at equal recall (``learned_vs_plain``).
+
 The path does not shard (queries are independent, each GPU holds a full replica), so
 ``--gpus N`` runs N replicas, one process per GPU, with the barrier + max-over-ranks timing.
 
-``--impl reference`` times the CPU port of the same query schedule (oracle/, all host
-threads) on a bounded sample of the workload; the reference's own CUDA build does not
-compile offline (it fetches RAFT/RMM at configure time).
+``--impl reference`` times the CPU restatement of the reference's query schedule (oracle/,
+all host threads) on a bounded sample of the same batch; the reference's own CUDA build does
+not compile offline (it fetches RAFT/RMM at configure time).  Its index is built and saved by
+a child process, so the timed process loads no library of this package.
 """
 from __future__ import annotations
 
@@ -32,6 +43,8 @@ sys.path.insert(0, str(ROOT))
 
 MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM = 6650.0
+PLAIN_PROBES = (16, 32, 64, 128, 256, 512, 1024)  # uniform probe counts of the plain sweep
+TARGET_RECALL = 0.95
 
 
 def hbm_peak():
@@ -41,8 +54,32 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
-def workload(name: str, scale: float, n_queries: int = 0):
-    from hdgrid_b200 import datasets
+def _datasets():
+    """hdgrid_b200/datasets.py loaded by path: it needs numpy only, and importing the package
+    would load libhdgrid.so into the process (the CPU reference arm must not)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("hdg_datasets", ROOT / "hdgrid_b200" / "datasets.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def conf_values(text: str) -> dict:
+    """The `key = value` lines of an HDGrid.conf text, lower-case keys, integers where they parse."""
+    out = {}
+    for line in text.splitlines():
+        if "=" not in line:
+            continue
+        key, val = (x.strip() for x in line.split("=", 1))
+        try:
+            out[key.lower()] = int(val)
+        except ValueError:
+            out[key.lower()] = val
+    return out
+
+
+def workload(name: str, scale: float, n_queries: int = 0, with_base: bool = True):
+    datasets = _datasets()
     if name == "config1":
         return datasets.config1(scale=scale, n_queries=n_queries or 1000, break_down=1)
     if name == "config2":
@@ -52,9 +89,10 @@ def workload(name: str, scale: float, n_queries: int = 0):
         nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
         return datasets.config3(scale=scale, n_queries=nq, break_down=1)
     if name == "config4":
-        return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1)
+        return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1,
+                                with_base=with_base)
     if name == "config5":
-        return datasets.config5(scale=scale, n_queries=n_queries or 10_000, break_down=1)
+        return datasets.config5(scale=scale, n_queries=n_queries or 10_000, break_down=1, with_base=with_base)
     raise SystemExit(f"unknown config {name}")
 
 
@@ -155,56 +193,81 @@ def cpu_baseline_bruteforce(ws, n_sample: int):
                       f"for {n_sample} of the workload's queries"}
 
 
+def reference_probe(ws) -> int:
+    """Lists the CPU reference arm probes per query: the index's sub_lists, or for the learned
+    workload the plain schedule's setting of the 10M x 128 batch without the network (the
+    config4 operating point, 64 lists)."""
+    return 64 if ws["name"] == "config5" else int(conf_values(ws["hdgrid_conf"])["sub_lists"])
+
+
+def build_index_only(args):
+    """Child process of the reference arm: builds the workload's index on the GPU and saves it."""
+    import torch
+    import hdgrid_b200 as hg
+    ws = workload(args.config, args.scale, args.queries)
+    idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
+    base = torch.from_numpy(ws["base"]).cuda()
+    labels = torch.from_numpy(ws["labels"]).cuda()
+    idx.build(hg.build_input_t(base, labels))
+    torch.cuda.synchronize()
+    idx.save(args.build_index_only)
+
+
 def run_reference(args):
-    """--impl reference: the CPU port of the HDGrid query schedule on the host cores."""
+    """--impl reference: the CPU restatement of the HDGrid query schedule on the host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import torch
-    import hdgrid_b200 as hg
     import oracle
-    from tests.helpers import build_gpu
-    ws = workload(args.config, args.scale, args.queries)
-    idx, base, _ = build_gpu(ws, "cuda:0")
     d = tempfile.mkdtemp(prefix="hdg_ref_")
     path = os.path.join(d, "index.hdg")
-    idx.save(path)
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--build-index-only", path, "--config", args.config,
+           "--scale", str(args.scale), "--queries", str(args.queries)]
+    subprocess.run(cmd, check=True, env=dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("LOCAL_RANK", "0")))
+    ws = workload(args.config, args.scale, args.queries)
     ora = oracle.OracleIndex(path)
-    n_sample = args.ref_sample
+    n_sample = min(args.ref_sample, ws["queries"].shape[0])
     cores = os.cpu_count() or 1
     qs, ql = ws["queries"][:n_sample], ws["query_labels"][:n_sample]
+    ks = ws.get("ks")
+    probe = reference_probe(ws)
+    kw = dict(threads=cores, trace=False, prefix_counts=True,
+              n_probe=np.full(n_sample, probe, np.uint32),
+              qk=None if ks is None else ks[:n_sample].astype(np.uint32))
     for _ in range(max(0, min(args.warmup, 1))):
-        ora.query(qs, ql, ws["base"], ws["k"], threads=cores, trace=False)
+        ora.query(qs, ql, ws["base"], ws["k"], **kw)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        ora.query(qs, ql, ws["base"], ws["k"], threads=cores, trace=False)
+        ora.query(qs, ql, ws["base"], ws["k"], **kw)
         times.append(time.perf_counter() - t0)
     value = n_sample * len(times) / sum(times)
-    sample = f"{n_sample} of the {ws['name']} queries per step through the CPU port of the super-grid query"
+    sample = (f"{n_sample} of the {ws['name']} batch's queries per step through the CPU restatement of the "
+              f"reference's plain super-grid schedule ({probe} lists per query, per-list counts from the index's "
+              f"prefix counts)")
     line = {"impl": "reference", "metric": metric_name(ws), "value": value, "unit": "queries/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(ws, args),
+            "config": workload_config(ws, args) | {"reference_sample_queries": n_sample, "reference_probe": probe},
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def metric_name(ws):
-    path = "learned per-query schedule" if ws["name"] == "config5" else "plain HDGrid path"
-    return f"filtered QPS @recall@100>=0.95, 1 B200 ({path}); ADC scan HBM GB/s"
+    return ("filtered QPS @recall@100>=0.95, 1 B200, learned vs plain; ADC scan HBM GB/s" if ws["name"] == "config5"
+            else f"filtered QPS @recall@100>=0.95, 1 B200 (plain HDGrid path, {ws['name']}); ADC scan HBM GB/s")
 
 
 def workload_config(ws, args):
-    import hdgrid_b200 as hg
-    p = hg.parse_config(ws["hdgrid_conf"])
-    return {"workload": f"{ws['name']}: {ws['base'].shape[0]}x{ws['base'].shape[1]} base, "
-                        f"{ws['labels'].shape[1]} label dims, {ws['queries'].shape[0]} queries, "
+    p = conf_values(ws["hdgrid_conf"])
+    nb = ws["base"].shape if ws.get("base") is not None else None
+    return {"workload": f"{ws['name']}: {nb[0]}x{nb[1]} base, {ws['labels'].shape[1]} label dims, "
+                        f"{ws['queries'].shape[0]} queries, "
                         + (f"k={ws['k']}" if ws.get("ks") is None else "k per query in {10, 100}"),
             "n_lists": int(p["clusters"] * p["sub_clusters"]), "clusters": int(p["clusters"]),
             "n_list": int(p["n_list"]), "sub_lists": int(p["sub_lists"]), "pq_dim": int(p["pq_dim"]),
-            "exps0": int(p["exps0"]), "max_grids": int(p["max_grids"]), "lut": "fp16" if p["lut_fp16"] else "f32",
+            "exps0": int(p["exps0"]), "max_grids": int(p["max_grids"]), "lut": "fp16" if p.get("lut_fp16") else "f32",
             "l2_flush": "256 MiB buffer written between timed steps", "parallelism": f"replicas{args.gpus}"}
 
 
@@ -250,6 +313,8 @@ def scan_traffic(ws, candidates):
 def run_hdgrid(args):
     import torch
     import hdgrid_b200 as hg
+    from hdgrid_b200 import datasets
+    from hdgrid_b200 import learned as L
     rank, world, local = dist_setup(args)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -262,7 +327,8 @@ def run_hdgrid(args):
     idx.build(hg.build_input_t(base, labels))
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
-    if ws["name"] == "config5":
+    learned = ws["name"] == "config5"
+    if learned:
         # the learned per-query schedule, trained by hdgrid_b200/train_learned.py
         wpath = ROOT / "hdgrid_b200" / "learned_weights" / "config5.npy"
         if not wpath.exists():
@@ -288,71 +354,68 @@ def run_hdgrid(args):
     stream = torch.cuda.current_stream()
 
     # recall against the exact filtered kNN (GPU brute force, FP32)
-    spec = hg.filter_spec(ws["filter_conf"])
     ranges = torch.empty((nq, 2 * ws["labels"].shape[1]), device=dev)
     hg.recover_filters(ws["filter_conf"], ql, ranges)
     gt_d = torch.empty((nq, k), device=dev)
     gt_i = torch.empty((nq, k), dtype=torch.int64, device=dev)
     hg.bruteforce_knn(base, labels, q, ranges, k, gt_d, gt_i)
+    gt_np = gt_i.cpu().numpy().view(np.uint64)
+
+    def recall_of(found):
+        return L.micro_recall(found, gt_np, ks) if ks is not None else datasets.recall(found, gt_np)
 
     for _ in range(args.warmup):
         do_query()
     torch.cuda.synchronize()
-    from hdgrid_b200 import datasets
-    from hdgrid_b200 import learned as L
-    ids_np = ids.cpu().numpy().view(np.uint64)
-    gt_np = gt_i.cpu().numpy().view(np.uint64)
-    rec = L.micro_recall(ids_np, gt_np, ks) if ks is not None else datasets.recall(ids_np, gt_np)
-    launches_per_step = int(idx.last_query_stats()["launches"])
-    max_rel = max_relative_error(ws, dist.cpu().numpy(), ids_np, args.err_sample)
-    cand_q = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].astype(np.uint64)
-    cand = int(cand_q.sum())
-    info0, p0 = idx.info(), hg.parse_config(ws["hdgrid_conf"])
-    # algorithmic scan bytes: M code bytes per candidate of a post-filter query; for a
-    # predicate-first query 4*l label bytes per candidate and M code bytes per candidate that
-    # passes the predicate (the ADC of the others is not needed)
-    pre_q = np.full(nq, p0["exps0"] <= 1)
-    if ws["name"] == "config5":
-        pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
-    pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
-    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info0["M"], info0["l"])
-    pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
 
-    # the batched workloads (10M x 128) run as the persistent scan under a captured CUDA graph,
-    # with the scan's threads x candidates-per-thread and work-item size picked by the
-    # autotuner; a plain-path run first gives the per-stage times (events do not reach into
-    # a graph replay)
+    # the batched workloads (10M x 128) run under a captured CUDA graph, with the scan's
+    # threads x candidates-per-thread and work-item size picked by the autotuner; the graph
+    # carries event nodes between its stages, so every timed replay gives its stage times
     graph_mode = ws["name"] in ("config4", "config5")
-    tuned, plain_stages = None, None
+    tuned = None
     if graph_mode:
         tuned = idx.autotune(qin, qout)
-        do_query()
-        torch.cuda.synchronize()
-        plain_stages = idx.stage_times()
         idx.set_param("query_graph", 1)
         do_query()  # first call of the shape: plain run + capture
-        torch.cuda.synchronize()
+        idx.status()
+        for _ in range(max(1, args.warmup)):
+            do_query()
+        idx.status()
     barrier(world)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    scan_ms = []
+    stage_steps = []
     with ClockSampler(local) as clk:
         for s in range(args.steps):
             flush.fill_(float(s))
             ev[s][0].record(stream)
             do_query()
             ev[s][1].record(stream)
-            st = idx.stage_times()
-            scan_ms.append(st.get("scan", float("nan")))
+            idx.status()  # waits for this step's work, raises its device status (graph replays)
+            stage_steps.append(idx.stage_times())
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(sum(step_ms), world)
-    stage_ms = idx.stage_times()  # of the last timed step
-    if graph_mode:
-        idx.status()  # raises if a replay outgrew the captured distance capacity
-        stage_ms = plain_stages
-        scan_ms = [plain_stages.get("scan", float("nan"))]
+    stats = idx.last_query_stats()
+    stage_ms = {n: float(np.mean([st.get(n, np.nan) for st in stage_steps])) for n in stage_steps[-1]}
+    scan_avg = stage_ms.get("scan", float("nan"))
     barrier(world)
+
+    # results, recall and scan accounting of the timed batch (the last replay's buffers)
+    ids_np = ids.cpu().numpy().view(np.uint64)
+    rec = recall_of(ids_np)
+    max_rel = max_relative_error(ws, dist.cpu().numpy(), ids_np, args.err_sample)
+    cand_q = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:nq, 0].astype(np.uint64)
+    cand = int(cand_q.sum())
+    info = idx.info()
+    p0 = hg.parse_config(ws["hdgrid_conf"])
+    pre_q = np.full(nq, p0["exps0"] <= 1)
+    if learned:
+        pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
+    pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
+    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"])
+    pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
+    launches_per_step = int(stats["launches"])
 
     # end to end through the public API with host buffers
     q_h = torch.from_numpy(ws["queries"]).pin_memory()
@@ -374,37 +437,44 @@ def run_hdgrid(args):
         i_h.copy_(ids, non_blocking=True)
         torch.cuda.synchronize()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    idx.status()
     e2e_total = max_over_ranks(sum(e2e_ms), world)
-
-    plain_ref = None
-    if ws["name"] == "config5":
-        # the plain schedule (LEARNED=0) on the same batch at uniform probe counts, for the
-        # learned-vs-plain comparison: recall and device-timed QPS of each
-        plain_ref = []
-        idx.set_param("learned", 0)
-        p5 = hg.parse_config(ws["hdgrid_conf"])
-        for sl in (16, 64, 128, 256):
-            idx.set_param("sub_lists", sl)
-            do_query()
-            torch.cuda.synchronize()
-            r = L.micro_recall(ids.cpu().numpy().view(np.uint64), gt_np, ks)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            flush.fill_(1.0)
-            e0.record(stream)
-            do_query()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            plain_ref.append({"sub_lists": sl, "recall": r, "qps": nq / (e0.elapsed_time(e1) / 1e3)})
-        idx.set_param("sub_lists", int(p5["sub_lists"]))
-        idx.set_param("learned", 1)
-
     value = replica_value(world, nq, args.steps, total_ms)
+
+    plain, versus = None, None
+    if learned and not args.no_plain_sweep:
+        # the plain HDGrid schedules (no network) on the same batch, at uniform probe counts:
+        # the post-filter budget (exps0 as configured) and the pre-filter schedule (exps0 = 1),
+        # each the faster of two device-timed runs after a warm-up run
+        plain = []
+        idx.set_param("query_graph", 0)
+        idx.set_param("learned", 0)
+        for sched, e0v in (("post-filter", int(p0["exps0"])), ("pre-filter", 1)):
+            idx.set_param("exps0", e0v)
+            for p in PLAIN_PROBES:
+                idx.set_param("sub_lists", p)
+                do_query()
+                torch.cuda.synchronize()
+                r = recall_of(ids.cpu().numpy().view(np.uint64))
+                best = float("inf")
+                for rep in range(2):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    flush.fill_(float(rep))
+                    a.record(stream)
+                    do_query()
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    best = min(best, a.elapsed_time(b))
+                st = idx.last_query_stats()
+                plain.append({"schedule": sched, "exps0": e0v, "sub_lists": p, "recall": r, "qps": nq / (best / 1e3),
+                              "n_cand": int(st["n_cand_ref"]), "n_cand_used": int(st["n_cand_used"])})
+        idx.set_param("exps0", int(p0["exps0"]))
+        idx.set_param("sub_lists", int(p0["sub_lists"]))
+        idx.set_param("learned", 1)
+        versus = L.compare_at_equal_recall(rec, value / world, plain, TARGET_RECALL)
+
     peak, peak_kind = hbm_peak()
-    info = idx.info()
-    p = hg.parse_config(ws["hdgrid_conf"])
-    lbl = ws["labels"].shape[1]
     per_cand = scan_bytes / max(cand, 1)
-    scan_avg = float(np.nanmean(scan_ms))
     achieved = scan_bytes / (scan_avg / 1e3) / 1e9
     if rank != 0:
         return
@@ -416,21 +486,24 @@ def run_hdgrid(args):
                                                "candidates_per_step": cand,
                                                "predicate_pass_share": pass_share,
                                                "max_rel_dist_err_vs_fp64": max_rel}
-                  | ({"schedule": "learned (LEARNED=1)", "plain_schedule_same_batch": plain_ref}
-                     if plain_ref is not None else {})
+                  | ({"schedule": "learned (LEARNED=1)"} if learned else {})
                   | ({"cuda_graph": True, "autotuned": tuned} if graph_mode else {}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": scan_traffic(ws, cand), "kernel": "k_scan_fast", "peak_kind": f"{peak_kind} hbm_gbs",
-                     "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg},
+                     "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg,
+                     "kernel_ms_source": "event nodes around the scan inside every timed graph replay" if graph_mode
+                     else "events around the scan in every timed step"},
         "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4 + (k_h.numel() * 4 if k_h is not None else 0)),
                 "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},
-        # kernels the library launched per query (prologue, [coarse GEMM x3], coarse, batch,
-        # lut, scan, select, [refine]) times the timed steps
+        # kernels the library launched per query batch, times the timed steps
         "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
         "stage_ms": stage_ms,
     }
+    if versus is not None:
+        line["learned_vs_plain"] = versus
+        line["plain_sweep"] = plain
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_bruteforce(ws, args.cpu_sample)
     print(json.dumps(line), flush=True)
@@ -442,15 +515,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hdgrid", choices=["hdgrid", "reference"])
-    ap.add_argument("--config", default="config2")
+    ap.add_argument("--config", default="config5")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--queries", type=int, default=0, help="query batch size (0 = the workload's own)")
     ap.add_argument("--cpu-sample", type=int, default=100)
-    ap.add_argument("--ref-sample", type=int, default=50)
+    ap.add_argument("--ref-sample", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-sweep", action="store_true")
     ap.add_argument("--err-sample", type=int, default=200, help="queries checked against FP64 distances")
+    ap.add_argument("--build-index-only", default="", help=argparse.SUPPRESS)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.build_index_only:
+        build_index_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_hdgrid(args)

@@ -399,7 +399,7 @@ class SuperGridIndex:
         LIB.hdg_last_query_stats(self._h, v, 10)
         return {"queries": v[0], "n_cand_ref": v[1], "n_cand_used": v[2], "coarse_total": v[3], "exact_total": v[4],
                 "max_row": v[5], "beta": struct.unpack("f", struct.pack("I", v[6] & 0xFFFFFFFF))[0],
-                "schedule": ["pre-filter", "post-filter", "single-dim"][v[7]], "launches": v[8]}
+                "schedule": ["pre-filter", "post-filter", "single-dim"][v[7]], "launches": v[8], "dropped": v[9]}
 
     def stage_times(self) -> dict:
         ms = (C.c_float * 16)()

@@ -187,7 +187,7 @@ hdg_status hdg_build(hdg_index* index, const float* d_data, uint64_t n, uint32_t
 hdg_status hdg_reserve(hdg_index* index, uint64_t max_queries) {
     return guarded([&] {
         HDG_REQUIRE(index, HDG_ERR_INVALID_ARG, "null index");
-        reserve_workspace(index, max_queries, 0);
+        reserve_workspace(index, max_queries);
     });
 }
 
@@ -327,6 +327,9 @@ hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_
         if (std::string(name) == "distances") {  // the ADC distance buffer (qoff gives the rows)
             src = static_cast<const char*>(cx->dist_buf.ptr);
             sz = cx->dist_buf.bytes;
+        } else if (std::string(name) == "cand_pool") {  // selected candidates (sel_off gives the rows)
+            src = static_cast<const char*>(cx->sel_buf.ptr);
+            sz = cx->sel_buf.bytes;
         } else {
             auto it = cx->layout.find(name);
             HDG_REQUIRE(it != cx->layout.end(), HDG_ERR_INVALID_ARG,

@@ -370,10 +370,14 @@ GridMeta compute_grid_shape(const std::vector<float>& mins, const std::vector<fl
         if ((label_mask >> i) & 1) cnt++;
     std::vector<std::pair<uint64_t, int>> span_pairs(l);
     for (int i = 0; i < l; i++) {
-        const double mx = std::ceil((double)maxs[i]), mn = std::floor((double)mins[i]);
-        HDG_REQUIRE(mn >= 0.0, HDG_ERR_INVALID_ARG,
+        // ceil / floor of the f32 extremes and their difference stay in f32: the reference's
+        // `ceil(global_max[i]) - floor(global_min[i])` on float elements resolves to the float
+        // overloads under nvcc, so a span above 2^24 is rounded to f32 before the cast
+        const float mx = std::ceil(maxs[i]), mn = std::floor(mins[i]);
+        HDG_REQUIRE(mn >= 0.0f, HDG_ERR_INVALID_ARG,
                     "labels must be non-negative (label dim " + std::to_string(i) + ")");
-        uint64_t span = (uint64_t)(mx - mn);
+        const float diff = mx - mn;
+        uint64_t span = (uint64_t)diff;
         if (span == 0) span = 1;
         span_pairs[i] = {span, i};
     }

@@ -11,6 +11,7 @@
 // the reference does.
 #pragma once
 #include <cfloat>
+#include <climits>
 #include <cstdint>
 
 #include "hdg_index.h"
@@ -30,8 +31,10 @@ __device__ __forceinline__ void recover_dim(const FilterDev& f, const float* row
         *lo = (float)((double)x - sl);
         *hi = (float)((double)x + sr);
     } else if (t == 1) {
+        // the f32 -> s32 conversion saturates (a label >= 2^31 gives INT_MAX); the bound is
+        // checked in 64 bits so that 2 * v + 1 cannot wrap for labels of 2^30 and above
         const int v = (int)(row[i] - 1.0f);
-        if (v >= 0 && 2 * v + 1 < f.n_map) {
+        if (v >= 0 && 2 * (int64_t)v + 1 < (int64_t)f.n_map) {
             *lo = f.map[2 * v];
             *hi = f.map[2 * v + 1];
         } else {  // out-of-table label: the reference reads out of bounds; empty box here
@@ -39,8 +42,10 @@ __device__ __forceinline__ void recover_dim(const FilterDev& f, const float* row
             *hi = -FLT_MAX;
         }
     } else if (t == 2) {
-        const int v = (int)row[i];
-        *lo = (float)(v / f.div_value[i]);
+        const int v = (int)row[i];  // saturating, like the map type
+        const int dv = f.div_value[i];
+        // INT_MIN / -1 is the one quotient that overflows: kept as INT_MIN
+        *lo = (float)((v == INT_MIN && dv == -1) ? v : v / dv);
         *hi = FLT_MAX;
     } else {
         // type 3 reads a [lo, hi] pair from a filter_dim = 2 label row (preprocessing.cu:27-28)

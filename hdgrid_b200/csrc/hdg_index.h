@@ -106,6 +106,9 @@ void release_graphs(GraphState* g);
 struct QueryCtx {
     DeviceBuffer work;              // per-query workspace
     DeviceBuffer dist_buf;          // one f32 ADC distance per scanned candidate
+    DeviceBuffer pos_buf;           // u32 candidate positions of compact rows (same capacity)
+    DeviceBuffer sel_buf;           // u32 selected candidates: min(n_cand, candidates) per query
+    DeviceBuffer part_buf;          // u64 best keys of the refine work items
     uint64_t work_queries = 0;
     std::map<std::string, std::pair<size_t, size_t>> layout;  // name -> (offset, bytes)
     GraphState* graphs = nullptr;   // QUERY_GRAPH=1: graphs keyed by pointers and sizes

@@ -39,7 +39,7 @@ void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, co
 void upload_index(hdg_index* idx, cudaStream_t st);
 void upload_filter(hdg_index* idx);
 FilterDev filter_dev(const hdg_index* idx);
-void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand, cudaStream_t st = nullptr);
+void reserve_workspace(hdg_index* idx, uint64_t q, cudaStream_t st = nullptr);
 void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* d_query_labels,
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
                cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,

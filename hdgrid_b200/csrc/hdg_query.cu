@@ -34,7 +34,6 @@ namespace hdg {
 
 constexpr int kThreads = 256;
 constexpr uint32_t kInvalid = 0xffffffffu;
-constexpr int kMaxCand = 16384;     // largest candidate budget n_cand
 constexpr uint32_t kChunk = 32768;  // default candidates per scan work item (SCAN_CHUNK)
 constexpr int kBins = 4096;         // select histogram
 constexpr int kBCap = 4096;         // boundary-bin buffer of the select
@@ -51,7 +50,7 @@ struct Workspace {
     uint32_t* range_len;     // [q x Ps]
     uint32_t* qstat;         // [q x 4]: cand_total, exact_total, n_lists, n_clusters
     uint64_t* scal;          // [8]: cand sum, exact sum, max cand, items, beta (f32 bits),
-                             //      queries dropped by the distance capacity, kept candidates
+                             //      queries dropped by a capacity, kept candidates, selected sum
     uint64_t* qoff;          // [q + 1] candidate offsets into dist
     uint32_t* item_off;      // [q + 1] work-item offsets
     uint32_t* mm;            // [q x 2] min / max finite distance key
@@ -59,11 +58,18 @@ struct Workspace {
     uint32_t* counter;       // [4] work counter
     float* lut;              // [q x G x 256 x 32] f32, or __half when lut16
     int lut16;               // LUT stored in FP16 (LUT_FP16=1); the scan sums in FP32
-    uint32_t* cand_pool;     // [q x kcand]
+    uint32_t* qbud;          // [q] candidate budget n_cand of each query (k_batch)
+    uint64_t* soff;          // [q + 1] offsets of the queries' selections in cand_pool
+    uint32_t* cand_pool;     // [soff[q]] selected candidates: min(n_cand, candidates) per query
     uint32_t* cand_count;    // [q]
-    uint64_t kcand;
+    uint64_t sel_cap;        // cand_pool capacity in entries
+    uint32_t* ritem_off;     // [q + 1] refine work-item offsets (k_refine_plan)
+    uint32_t* rdone;         // [q] refine items finished per query
+    uint32_t* rsurv;         // [q] rows re-ranked exactly per query (predicate survivors of the selection)
+    uint64_t* rpart;         // [refine items x k_max] best keys of each refine item
     int surv_list;           // 1: the compacting scan lists each predicate-first query's survivors
     float* dist;             // [sum of candidates]
+    uint32_t* spos;          // [sum of candidates] candidate position of each entry of a compact row
     float* S;                // [q x (C + L)] tensor-core dot products (nullptr: exact path only)
     uint64_t ldS;
     float* qnorm;            // [q] squared query norms
@@ -95,30 +101,27 @@ __device__ __forceinline__ int q_sched(const Workspace& w, uint64_t qi) { return
 __device__ __forceinline__ bool q_prefilter(const Workspace& w, uint64_t qi) {
     return w.mode == kPre || q_sched(w, qi) == 1;
 }
-// Candidate budget of query qi: k for the reference pre-filter schedule (exps0 <= 1),
-// exps0 * k for the single-dim schedule and the predicate-first schedule, and the
-// reference's min(exps0 * k * beta, max_row_len) for the post-filter schedule
-// (Super-Grid-IVF_PQ.cu:1219-1222); capped by kMaxCand.
-__device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) {
+// Candidate budget n_cand of query qi given the batch's beta and max_row_len: k for the
+// reference pre-filter schedule (exps0 <= 1), exps0 * k for the single-dim schedule and the
+// predicate-first schedule, and the reference's min(exps0 * k * beta, max_row_len) for the
+// post-filter schedule (Super-Grid-IVF_PQ.cu:1219-1222), with no further cap.  k_batch
+// evaluates it once per query into w.qbud.
+__device__ __forceinline__ uint64_t budget_of(const Workspace& w, uint64_t qi, float beta, uint64_t max_row) {
     const uint32_t k = q_k(w, qi);
     if (w.mode == kPre) return k;
     uint64_t K;
     if (w.mode == kL1 || q_sched(w, qi) == 1) {
         K = (uint64_t)w.exps0 * k;
+    } else if (!(beta < INFINITY)) {
+        K = max_row;
     } else {
-        // beta and max_row of the batch, written by k_batch
-        const float beta = __uint_as_float((uint32_t)w.scal[4]);
-        const uint64_t max_row = w.scal[2];
-        if (!(beta < INFINITY)) {
-            K = max_row;
-        } else {
-            const float want = (float)((uint64_t)w.exps0 * k) * beta;
-            K = want >= 1.8e19f ? ~0ull : (uint64_t)want;
-            K = min(K, max_row);
-        }
+        const float want = (float)((uint64_t)w.exps0 * k) * beta;
+        K = want >= 1.8e19f ? ~0ull : (uint64_t)want;
+        K = min(K, max_row);
     }
-    return (uint32_t)max((uint64_t)1, min(K, (uint64_t)kMaxCand));
+    return max((uint64_t)1, min(K, (uint64_t)0xffffffffu));
 }
+__device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) { return w.qbud[qi]; }
 
 // Exclusive block-wide scan of n u32 values in shared memory (in place).  All threads.
 __device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_t* s_warp) {
@@ -152,6 +155,24 @@ __device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_
         run += vi;
     }
     __syncthreads();
+}
+
+// Slot of this lane among the lanes of its warp where f holds, taken from the counter *ctr
+// with one atomic per warp (~0u where f is false).  Every lane of the warp must call it.
+__device__ __forceinline__ uint32_t warp_reserve(bool f, uint32_t* ctr) {
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (!bal) return ~0u;
+    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return f ? base + __popc(bal & ((1u << lane) - 1u)) : ~0u;
+}
+
+// Appends v at the next free slot of dst (counter *ctr) where f holds; every lane calls it.
+__device__ __forceinline__ void warp_append(bool f, uint32_t v, uint32_t* ctr, uint32_t* dst) {
+    const uint32_t slot = warp_reserve(f, ctr);
+    if (f) dst[slot] = v;
 }
 
 // ------------------------------------------------------------------------------------
@@ -604,10 +625,37 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
 // ------------------------------------------------------------------------------------
 // k_batch: per-query candidate offsets and work items, batch sums (one block)
 // ------------------------------------------------------------------------------------
+// Inclusive sum of x over the block (blockDim.x a multiple of 32, <= 1024); s_w: 32 words of
+// shared scratch that no other thread touches until the following barrier.
+__device__ __forceinline__ unsigned long long block_inclusive_sum(unsigned long long x, unsigned long long* s_w,
+                                                                  unsigned long long* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long y = lane < nw ? s_w[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        s_w[lane] = y;
+    }
+    __syncthreads();
+    *total = s_w[nw - 1];
+    return x + (warp ? s_w[warp - 1] : 0);
+}
+
 __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
-    __shared__ unsigned long long s_tot[32], s_items[32];
+    __shared__ unsigned long long s_tot[32], s_items[32], s_sel[32];
     __shared__ unsigned long long s_red[3], s_drop[2];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    __shared__ float s_beta;
+    const int t = threadIdx.x;
     if (t == 0) s_red[0] = s_red[1] = s_red[2] = s_drop[0] = s_drop[1] = 0;
     __syncthreads();
     const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
@@ -620,40 +668,9 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         exact += w.qstat[i * 4 + 1];
         mx = max(mx, (unsigned long long)c);
     }
-    // inclusive scans of (cand, items) across the block
-    unsigned long long xc = cand, xi = items;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long yc = __shfl_up_sync(0xffffffffu, xc, o);
-        const unsigned long long yi = __shfl_up_sync(0xffffffffu, xi, o);
-        if (lane >= o) {
-            xc += yc;
-            xi += yi;
-        }
-    }
-    if (lane == 31) {
-        s_tot[warp] = xc;
-        s_items[warp] = xi;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        unsigned long long yc = lane < (int)(blockDim.x >> 5) ? s_tot[lane] : 0;
-        unsigned long long yi = lane < (int)(blockDim.x >> 5) ? s_items[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long zc = __shfl_up_sync(0xffffffffu, yc, o);
-            const unsigned long long zi = __shfl_up_sync(0xffffffffu, yi, o);
-            if (lane >= o) {
-                yc += zc;
-                yi += zi;
-            }
-        }
-        s_tot[lane] = yc;
-        s_items[lane] = yi;
-    }
-    __syncthreads();
-    unsigned long long rc = xc - cand + (warp ? s_tot[warp - 1] : 0);
-    unsigned long long ri = xi - items + (warp ? s_items[warp - 1] : 0);
+    unsigned long long tot_c = 0, tot_i = 0;
+    unsigned long long rc = block_inclusive_sum(cand, s_tot, &tot_c) - cand;
+    unsigned long long ri = block_inclusive_sum(items, s_items, &tot_i) - items;
     unsigned long long dropped = 0, kept = 0;
     for (uint64_t i = b; i < e; i++) {
         const uint32_t c = w.qstat[i * 4];
@@ -683,20 +700,50 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     atomicAdd(&s_red[0], cand);
     atomicAdd(&s_red[1], exact);
     atomicMax(&s_red[2], mx);
-    atomicAdd(&s_drop[0], dropped);
-    atomicAdd(&s_drop[1], kept);
     __syncthreads();
     if (t == 0) {
         w.scal[0] = s_red[0];
         w.scal[1] = s_red[1];
         w.scal[2] = s_red[2];
-        w.scal[3] = s_items[(blockDim.x >> 5) - 1];
+        w.scal[3] = tot_i;
         // beta = coarse / real as the reference computes it (Super-Grid-IVF_PQ.cu:1219)
         const float beta = s_red[1] == 0 ? INFINITY : __fdiv_rn((float)s_red[0], (float)s_red[1]);
         w.scal[4] = __float_as_uint(beta);
+        s_beta = beta;
+        w.counter[0] = 0;
+    }
+    __syncthreads();
+    // each query's budget n_cand, now that the batch's beta and max_row are known, and the
+    // offset of its selection (min(n_cand, candidates) entries) in cand_pool
+    const float beta = s_beta;
+    const uint64_t max_row = s_red[2];
+    unsigned long long sel = 0;
+    for (uint64_t i = b; i < e; i++) {
+        const uint64_t K = budget_of(w, i, beta, max_row);
+        w.qbud[i] = (uint32_t)K;
+        sel += min(K, (uint64_t)w.qstat[i * 4]);
+    }
+    unsigned long long tot_s = 0;
+    unsigned long long rs = block_inclusive_sum(sel, s_sel, &tot_s) - sel;
+    for (uint64_t i = b; i < e; i++) {
+        const uint32_t c = w.qstat[i * 4];
+        const uint64_t si = min((uint64_t)w.qbud[i], (uint64_t)c);
+        w.soff[i] = rs;
+        if (rs + si > w.sel_cap && c) {  // past the selection capacity: no candidates either
+            w.qstat[i * 4] = 0;
+            dropped++;
+            kept -= c;
+        }
+        rs += si;
+    }
+    if (e == q && b < e) w.soff[q] = rs;
+    atomicAdd(&s_drop[0], dropped);
+    atomicAdd(&s_drop[1], kept);
+    __syncthreads();
+    if (t == 0) {
         w.scal[5] = s_drop[0];
         w.scal[6] = s_drop[1];
-        w.counter[0] = 0;
+        w.scal[7] = tot_s;
     }
 }
 
@@ -963,6 +1010,10 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                 // take a whole predicate step, and at the end of the span until the queues
                 // are empty.
                 uint32_t* qe = s_queue + (uint32_t)(t >> 5) * (2 * kPreQueue * 32);
+                // survivors are appended to the query's row in arrival order -- distance and
+                // candidate position, one counter atomic per warp -- and rejected candidates
+                // write nothing; cand_count ends as the row's length
+                uint32_t* spos = w.spos + w.qoff[qq];
                 uint32_t* qp = qe + kPreQueue * 32;
                 int qh = 0, qn = 0, rr = r[0];
                 const bool lab4 = lbl == 4 && (reinterpret_cast<uintptr_t>(D.labels) & 15) == 0;
@@ -987,6 +1038,7 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                         float s0 = 0.f, s1 = 0.f;
                         adc_group1(planes + row, n_pts, 0, R, sh, lane4, s_lut, s0, s1);
                         s0 += s1;
+                        const uint32_t slot = warp_reserve(live, &w.cand_count[qq]);
                         if (live) {
                             if (s0 < INFINITY) {
                                 const uint32_t key = float_key(s0);
@@ -994,10 +1046,8 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                                 kmax = max(kmax, key);
                                 nf++;
                             }
-                            dst[e] = s0;
-                            // the survivor's position, for a select that takes every survivor
-                            const uint32_t slot = atomicAdd(&w.cand_count[qq], 1u);
-                            if (slot < w.kcand) w.cand_pool[(uint64_t)qq * w.kcand + slot] = e;
+                            dst[slot] = s0;
+                            spos[slot] = e;
                         }
                         continue;
                     }
@@ -1047,8 +1097,6 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                             qe[slot * 32 + lane] = pe[j];
                             qp[slot * 32 + lane] = pp[j];
                             qn++;
-                        } else {
-                            dst[pe[j]] = INFINITY;
                         }
                     }
                     eb += 32u * kPreStep;
@@ -1293,8 +1341,13 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     __shared__ uint32_t s_below, s_cntb, s_out, s_nb, s_bmin, s_bmax, s_need;
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
-    const uint32_t total = w.qstat[qi * 4];
+    // A predicate-first query of the compacting scan has a compact row: its survivors' distances
+    // in arrival order with their candidate positions beside them (cand_count entries); any
+    // other query's row holds one distance per candidate position.
+    const bool compact = w.surv_list && q_prefilter(w, qi);
+    const uint32_t total = compact ? w.cand_count[qi] : w.qstat[qi * 4];
     const float* dist = w.dist + w.qoff[qi];
+    const uint32_t* prow = compact ? w.spos + w.qoff[qi] : nullptr;
     for (int i = t; i < Ps; i += blockDim.x) {
         s_pre[i] = w.range_len[qi * Ps + i];
         s_start[i] = w.range_start[qi * Ps + i];
@@ -1307,34 +1360,67 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     block_exclusive_scan(s_pre, Ps + 1, s_warp);
     const uint32_t nfin = w.nfin[qi];
     const uint32_t need0 = min((uint32_t)K, nfin);
-    // emitted entries keep their candidate position; positions become pool slots once the
+    uint32_t* sel_dst = sorted_out ? nullptr : w.cand_pool + w.soff[qi];
+    // candidate position of row entry e (e < total)
+    auto posof = [&](uint32_t e) { return prow ? prow[e] : e; };
+    // Selected entries are recorded by candidate position; positions become pool slots once the
     // selection is complete, in one divergence-free loop over the K entries (converting at
-    // emit time made nearly every warp of the pass run the range search for one lane)
-    auto emit = [&](uint32_t e, float d) {
-        const uint32_t pos = atomicAdd(&s_out, 1u);
+    // emit time made nearly every warp of the pass run the range search for one lane).  Ties in
+    // distance are broken by the lower position.
+    auto emit = [&](uint32_t pos, float d) {
+        const uint32_t at = atomicAdd(&s_out, 1u);
         if (sorted_out)
-            s_sel[pos] = ((uint64_t)float_key(d) << 32) | e;
+            s_sel[at] = ((uint64_t)float_key(d) << 32) | pos;
         else
-            w.cand_pool[qi * w.kcand + pos] = e;
+            sel_dst[at] = pos;
     };
     auto inside = [&](float d, int nlv) {
         for (int l = 0; l < nlv; l++)
             if (sel_bin(d, s_lv[l].lo, s_lv[l].inv) != s_lv[l].bin) return false;
         return true;
     };
-    // A predicate-first query scanned by the compacting scan has its survivors' positions
-    // listed in its candidate slots already (cand_count of them, its finite count): when all
-    // are selected, the list is the selection and the distance row need not be read.
-    const bool listed = w.surv_list && !sorted_out && q_prefilter(w, qi) && w.cand_count[qi] == nfin &&
-                        nfin <= (uint32_t)K && nfin <= w.kcand;
-    if (listed) {
-        if (t == 0) s_out = nfin;
-        __syncthreads();
-    } else if (need0 > 0 && nfin <= (uint32_t)K) {
-        // every finite candidate is selected
-        for (uint32_t e = t; e < total; e += blockDim.x) {
-            const float d = dist[e];
-            if (d < INFINITY) emit(e, d);
+    // First bin of s_hist whose cumulative count reaches need: s_bin, s_below (count before
+    // it) and s_cntb (its count).  Warp 0 scans; the caller synchronises.
+    auto find_bin = [&](uint32_t need) {
+        if (t < 32) {
+            uint32_t run = 0, below = 0;
+            int found = -1;
+            for (int base = 0; base < kBins && found < 0; base += 32) {
+                const uint32_t v = s_hist[base + t];
+                uint32_t x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (t >= o) x += y;
+                }
+                const unsigned hit = __ballot_sync(0xffffffffu, run + x >= need);
+                if (hit) {
+                    const int l0 = __ffs(hit) - 1;
+                    found = base + l0;
+                    below = run + __shfl_sync(0xffffffffu, x - v, l0);
+                }
+                run += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (t == 0) {
+                s_bin = found;
+                s_below = below;
+                s_cntb = found >= 0 ? s_hist[found] : 0;
+            }
+        }
+    };
+    if (need0 > 0 && nfin <= (uint32_t)K) {
+        // every finite candidate is selected (the loop bound is block-uniform so that every
+        // lane reaches the warp appends)
+        for (uint32_t base = 0; base < total; base += blockDim.x) {
+            const uint32_t e = base + t;
+            const float d = e < total ? dist[e] : INFINITY;
+            const bool f = d < INFINITY;
+            const uint32_t p = f ? posof(e) : 0u;
+            if (sorted_out) {
+                if (f) emit(p, d);
+            } else {
+                warp_append(f, p, &s_out, sel_dst);
+            }
         }
         __syncthreads();
     } else if (need0 > 0) {
@@ -1361,54 +1447,32 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
                     if (dv[u] < INFINITY && inside(dv[u], level)) atomicAdd(&s_hist[sel_bin(dv[u], lo, inv)], 1u);
             }
             __syncthreads();
-            if (t < 32) {  // first bin whose cumulative count reaches need
-                uint32_t run = 0;
-                int found = -1;
-                uint32_t below = 0;
-                for (int base = 0; base < kBins && found < 0; base += 32) {
-                    const uint32_t v = s_hist[base + t];
-                    uint32_t x = v;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                        if (t >= o) x += y;
-                    }
-                    const unsigned hit = __ballot_sync(0xffffffffu, run + x >= need);
-                    if (hit) {
-                        const int l0 = __ffs(hit) - 1;
-                        found = base + l0;
-                        below = run + __shfl_sync(0xffffffffu, x - v, l0);
-                    }
-                    run += __shfl_sync(0xffffffffu, x, 31);
-                }
-                if (t == 0) {
-                    s_bin = found;
-                    s_below = below;
-                    s_cntb = s_hist[found];
-                }
-            }
+            find_bin(need);
             __syncthreads();
             const int b = s_bin;
             const bool fits = s_cntb <= (uint32_t)kBCap;
-            for (uint32_t e0 = t; e0 < total; e0 += 4 * blockDim.x) {
+            for (uint32_t e0 = 0; e0 < total; e0 += 4 * blockDim.x) {  // block-uniform bound
                 float dv[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    const uint32_t e = e0 + u * blockDim.x;
+                    const uint32_t e = e0 + t + u * blockDim.x;
                     dv[u] = e < total ? __ldg(dist + e) : INFINITY;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     const float d = dv[u];
-                    const uint32_t e = e0 + u * blockDim.x;
-                    if (!(d < INFINITY) || !inside(d, level)) continue;
-                    const int bb = sel_bin(d, lo, inv);
+                    const uint32_t e = e0 + t + u * blockDim.x;
+                    const bool in = d < INFINITY && inside(d, level);
+                    const int bb = in ? sel_bin(d, lo, inv) : kBins;
+                    const uint32_t p = bb <= b ? posof(e) : 0u;
+                    if (!sorted_out) warp_append(bb < b, p, &s_out, sel_dst);
+                    if (!in) continue;
                     if (bb < b) {
-                        emit(e, d);
+                        if (sorted_out) emit(p, d);
                     } else if (bb == b) {
                         if (fits) {
-                            const uint32_t p = atomicAdd(&s_nb, 1u);
-                            s_bbuf[p] = ((uint64_t)float_key(d) << 32) | e;
+                            const uint32_t at = atomicAdd(&s_nb, 1u);
+                            s_bbuf[at] = ((uint64_t)float_key(d) << 32) | p;
                         } else {
                             atomicMin(&s_bmin, float_key(d));
                             atomicMax(&s_bmax, float_key(d));
@@ -1419,6 +1483,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             __syncthreads();
             need -= s_below;
             if (fits) {
+                // the boundary bin, sorted by (distance, position)
                 const int nb = (int)s_nb;
                 const int n2 = (int)next_pow2_dev((uint32_t)max(nb, 2));
                 for (int i = nb + t; i < n2; i += blockDim.x) s_bbuf[i] = ~0ull;
@@ -1432,34 +1497,74 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
                 break;
             }
             if (s_bmin == s_bmax || level == kMaxLevels - 1) {
-                // one distance value (or no levels left): take the boundary bin in position order
+                // one distance value (or no levels left): the boundary bin's entries (of that
+                // one distance) are taken in position order
                 const uint32_t tie_key = s_bmin;
+                const bool one = s_bmin == s_bmax;
                 const int nlv = level;
+                auto tie = [&](float d) {
+                    return d < INFINITY && inside(d, nlv) && sel_bin(d, lo, inv) == b && (!one || float_key(d) == tie_key);
+                };
                 if (t == 0) s_need = need;
                 __syncthreads();
-                for (uint32_t base = 0; base < total && s_need > 0; base += blockDim.x) {
-                    const uint32_t e = base + t;
-                    bool f = false;
-                    float d = 0.f;
-                    if (e < total) {
-                        d = dist[e];
-                        f = d < INFINITY && inside(d, nlv) && sel_bin(d, lo, inv) == b &&
-                            (s_bmin == s_bmax ? float_key(d) == tie_key : true);
+                if (!compact) {
+                    // row order is position order: the first s_need tie entries of the row
+                    for (uint32_t base = 0; base < total && s_need > 0; base += blockDim.x) {
+                        const uint32_t e = base + t;
+                        bool f = false;
+                        float d = 0.f;
+                        if (e < total) {
+                            d = dist[e];
+                            f = tie(d);
+                        }
+                        const unsigned bal = __ballot_sync(0xffffffffu, f);
+                        if ((t & 31) == 0) s_warp[t >> 5] = __popc(bal);
+                        __syncthreads();
+                        uint32_t before = 0;
+                        for (int i = 0; i < (t >> 5); i++) before += s_warp[i];
+                        const uint32_t rank = before + __popc(bal & ((1u << (t & 31)) - 1));
+                        if (f && rank < s_need) emit(e, d);
+                        __syncthreads();
+                        if (t == 0) {
+                            uint32_t tot = 0;
+                            for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += s_warp[i];
+                            s_need = s_need > tot ? s_need - tot : 0;
+                        }
+                        __syncthreads();
                     }
-                    const unsigned bal = __ballot_sync(0xffffffffu, f);
-                    if ((t & 31) == 0) s_warp[t >> 5] = __popc(bal);
-                    __syncthreads();
-                    uint32_t before = 0;
-                    for (int i = 0; i < (t >> 5); i++) before += s_warp[i];
-                    const uint32_t rank = before + __popc(bal & ((1u << (t & 31)) - 1));
-                    if (f && rank < s_need) emit(e, d);
-                    __syncthreads();
-                    if (t == 0) {
-                        uint32_t tot = 0;
-                        for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += s_warp[i];
-                        s_need = s_need > tot ? s_need - tot : 0;
+                } else {
+                    // a compact row is in arrival order: the s_need smallest positions among
+                    // the tie entries, by a radix select over positions (kBins bins per level;
+                    // positions are unique, so a one-position bin holds one entry)
+                    uint32_t plo = 0, phi = w.qstat[qi * 4];
+                    for (;;) {
+                        const uint32_t binw = max(1u, (phi - plo + kBins - 1) / kBins);
+                        for (int i = t; i < kBins; i += blockDim.x) s_hist[i] = 0;
+                        __syncthreads();
+                        for (uint32_t e = t; e < total; e += blockDim.x) {
+                            const float d = dist[e];
+                            const uint32_t p = prow[e];
+                            if (tie(d) && p >= plo && p < phi) atomicAdd(&s_hist[(p - plo) / binw], 1u);
+                        }
+                        __syncthreads();
+                        find_bin(s_need);
+                        __syncthreads();
+                        const int pb = s_bin;
+                        const bool last = binw == 1;
+                        for (uint32_t e = t; e < total; e += blockDim.x) {
+                            const float d = dist[e];
+                            const uint32_t p = prow[e];
+                            if (!tie(d) || p < plo || p >= phi) continue;
+                            const int bin = (int)((p - plo) / binw);
+                            if (bin < pb || (last && bin == pb)) emit(p, d);
+                        }
+                        __syncthreads();
+                        if (last || pb < 0) break;
+                        if (t == 0) s_need -= s_below;
+                        plo += (uint32_t)pb * binw;
+                        phi = min(phi, plo + binw);
+                        __syncthreads();
                     }
-                    __syncthreads();
                 }
                 break;
             }
@@ -1476,7 +1581,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     __syncthreads();
     const uint32_t nsel = s_out;
     if (!sorted_out) {
-        uint32_t* pool = w.cand_pool + qi * w.kcand;
+        uint32_t* pool = w.cand_pool + w.soff[qi];
         for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
         if (t == 0) w.cand_count[qi] = nsel;
         return;
@@ -1500,164 +1605,270 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
 // ------------------------------------------------------------------------------------
 // k_refine: post-filter predicate, exact f32 L2, top-k
 // ------------------------------------------------------------------------------------
-// The predicate survivors of the query's candidates are compacted first; then every warp
-// computes exact distances of survivor rows in rounds, and the keys (distance, id) below the
-// running k-th go to a buffer of pow2(k + 4 * blockDim) entries that is sorted and cut to k
-// between rounds.
+// A query's selection (min(n_cand, candidates) entries, which the reference's uncapped
+// budget can put in the hundreds of thousands) is cut into work items of kRefChunk entries;
+// k_refine_plan lays them out and a persistent k_refine takes them from a counter.  An item
+// compacts its predicate survivors, computes their exact distances and keeps its best k;
+// a query with one item writes its output row directly, otherwise every item leaves its
+// best k in the partial buffer and the last item of the query to finish merges them.
+constexpr uint32_t kRefChunk = 4096;
+
+__global__ void __launch_bounds__(1024) k_refine_plan(uint64_t q, Workspace w) {
+    __shared__ unsigned long long s_w[32];
+    const int t = threadIdx.x;
+    const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = t * per, e = min(q, b + per);
+    unsigned long long items = 0;
+    for (uint64_t i = b; i < e; i++) items += max(1u, (w.cand_count[i] + kRefChunk - 1) / kRefChunk);
+    unsigned long long tot = 0;
+    unsigned long long r = block_inclusive_sum(items, s_w, &tot) - items;
+    for (uint64_t i = b; i < e; i++) {
+        w.ritem_off[i] = (uint32_t)r;
+        r += max(1u, (w.cand_count[i] + kRefChunk - 1) / kRefChunk);
+        w.rdone[i] = 0;
+        w.rsurv[i] = 0;
+    }
+    if (e == q && b < e) w.ritem_off[q] = (uint32_t)r;
+    if (t == 0) w.counter[1] = 0;
+}
+
+// Adds the keys below the running k-th to s_keys in rounds of at most cap - kq keys; the
+// buffer is sorted and cut to kq between rounds.  get(i) gives key i of n; all threads.
+template <typename Get>
+__device__ __forceinline__ void topk_rounds(uint64_t* s_keys, int cap, int kq, int n, int* s_cnt, uint64_t* s_th,
+                                            Get get) {
+    const int per_round = max(cap - kq, 1);
+    for (int r0 = 0; r0 < n; r0 += per_round) {
+        const int r1 = min(n, r0 + per_round);
+        for (int i = r0 + (int)threadIdx.x; i < r1; i += blockDim.x) {
+            const uint64_t key = get(i);
+            if (key < *s_th) s_keys[atomicAdd(s_cnt, 1)] = key;
+        }
+        __syncthreads();
+        const int c = *s_cnt;
+        __syncthreads();
+        if (r1 < n && c > kq) {
+            for (int i = c + threadIdx.x; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+            __syncthreads();
+            block_bitonic_sort(s_keys, cap);
+            if (threadIdx.x == 0) {
+                *s_cnt = kq;
+                *s_th = s_keys[kq - 1];
+            }
+            __syncthreads();
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __restrict__ queries,
                                                      const float* __restrict__ data, int cap, int apply_pred,
-                                                     int lbl, Workspace w, float* __restrict__ out_dist,
+                                                     int lbl, uint64_t q, Workspace w, float* __restrict__ out_dist,
                                                      uint64_t* __restrict__ out_ids, int k_out) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);           // [cap]
     float* s_q = reinterpret_cast<float*>(s_keys + cap);             // [d]
     __shared__ float s_box[2 * kMaxDims];
     __shared__ int s_wsum[kThreads / 32];
-    __shared__ int s_cnt, s_ns;
+    __shared__ int s_cnt, s_ns, s_item, s_qi, s_last;
     __shared__ uint64_t s_th;
-    const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = kThreads / 32;
     const int d = D.d;
-    for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
-    if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
-    if (t == 0) {
-        s_cnt = 0;
-        s_ns = 0;
-        s_th = ~0ull;
-    }
-    __syncthreads();
-    const int nc = (int)w.cand_count[qi];
-    const int kq = (int)q_k(w, qi);
-    const bool pred_q = apply_pred && q_sched(w, qi) == 0;  // predicate-first queries already passed it
-    uint32_t* list = w.cand_pool + qi * w.kcand;
-    // 1. the predicate survivors, compacted in place as original ids (each chunk is read
-    //    before the barrier and written at or below its own start)
-    for (int base = 0; base < nc; base += kThreads) {
-        const int e = base + t;
-        bool keep = false;
-        uint32_t pool = kInvalid;
-        if (e < nc) {
-            pool = list[e];
-            keep = pool != kInvalid;
-            if (keep && pred_q) {
-                const float* lab = D.labels + (uint64_t)pool * lbl;
-                for (int i = 0; i < lbl; i++) {
-                    const float v = lab[i];
-                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) keep = false;
+    const uint32_t n_items = w.ritem_off[q];
+    int cur = -1;
+    for (;;) {
+        if (t == 0) {
+            const int item = (int)atomicAdd(&w.counter[1], 1u);
+            s_item = item;
+            if (item < (int)n_items) {  // largest query with ritem_off <= item
+                int lo = 0, hi = (int)q - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (w.ritem_off[mid] <= (uint32_t)item) lo = mid;
+                    else hi = mid - 1;
                 }
-            }
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_wsum[warp] = __popc(bal);
-        __syncthreads();
-        int before = s_ns, tot = 0;
-        for (int i = 0; i < nw; i++) {
-            before += i < warp ? s_wsum[i] : 0;
-            tot += s_wsum[i];
-        }
-        if (keep) list[before + __popc(bal & ((1u << lane) - 1))] = D.ids[pool];
-        __syncthreads();
-        if (t == 0) s_ns += tot;
-    }
-    __syncthreads();
-    const int ns = s_ns;
-    // 2. exact distances in rounds of cap - kq rows: every warp takes rows of the round, the
-    //    keys (distance, id) below the running k-th go to the buffer, which is sorted and cut
-    //    to kq after each round
-    const int per_round = max(cap - kq, 1);
-    // rows 16-byte aligned with d % 4 == 0: four rows per warp at a time, 8 lanes per row,
-    // 16-byte loads, four independent partial sums per lane (the gathers are latency-bound:
-    // this keeps ~6 KB per warp in flight instead of one 128-byte load per lane)
-    const bool vec4 = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(data) & 15) == 0;
-    for (int r0 = 0; r0 < ns; r0 += per_round) {
-        const int r1 = min(ns, r0 + per_round);
-        if (vec4) {
-            const int g = lane >> 3, sl = lane & 7, d4 = d >> 2;
-            const float4* q4 = reinterpret_cast<const float4*>(s_q);
-            for (int i0 = r0 + warp * 4; i0 < r1; i0 += nw * 4) {
-                const int i = i0 + g;
-                const bool ok = i < r1;
-                const uint32_t id = ok ? list[i] : list[r0];
-                const float4* row = reinterpret_cast<const float4*>(data + (uint64_t)id * d);
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-                int j = sl;
-                for (; j + 24 < d4; j += 32) {
-                    const float4 x0 = __ldg(row + j), x1 = __ldg(row + j + 8), x2 = __ldg(row + j + 16),
-                                 x3 = __ldg(row + j + 24);
-                    const float4 y0 = q4[j], y1 = q4[j + 8], y2 = q4[j + 16], y3 = q4[j + 24];
-                    a0 = fmaf(y0.x - x0.x, y0.x - x0.x, a0);
-                    a0 = fmaf(y0.y - x0.y, y0.y - x0.y, a0);
-                    a0 = fmaf(y0.z - x0.z, y0.z - x0.z, a0);
-                    a0 = fmaf(y0.w - x0.w, y0.w - x0.w, a0);
-                    a1 = fmaf(y1.x - x1.x, y1.x - x1.x, a1);
-                    a1 = fmaf(y1.y - x1.y, y1.y - x1.y, a1);
-                    a1 = fmaf(y1.z - x1.z, y1.z - x1.z, a1);
-                    a1 = fmaf(y1.w - x1.w, y1.w - x1.w, a1);
-                    a2 = fmaf(y2.x - x2.x, y2.x - x2.x, a2);
-                    a2 = fmaf(y2.y - x2.y, y2.y - x2.y, a2);
-                    a2 = fmaf(y2.z - x2.z, y2.z - x2.z, a2);
-                    a2 = fmaf(y2.w - x2.w, y2.w - x2.w, a2);
-                    a3 = fmaf(y3.x - x3.x, y3.x - x3.x, a3);
-                    a3 = fmaf(y3.y - x3.y, y3.y - x3.y, a3);
-                    a3 = fmaf(y3.z - x3.z, y3.z - x3.z, a3);
-                    a3 = fmaf(y3.w - x3.w, y3.w - x3.w, a3);
-                }
-                for (; j < d4; j += 8) {
-                    const float4 x = __ldg(row + j), y = q4[j];
-                    a0 = fmaf(y.x - x.x, y.x - x.x, a0);
-                    a0 = fmaf(y.y - x.y, y.y - x.y, a0);
-                    a0 = fmaf(y.z - x.z, y.z - x.z, a0);
-                    a0 = fmaf(y.w - x.w, y.w - x.w, a0);
-                }
-                float sq = (a0 + a1) + (a2 + a3);
-                sq += __shfl_xor_sync(0xffffffffu, sq, 4);
-                sq += __shfl_xor_sync(0xffffffffu, sq, 2);
-                sq += __shfl_xor_sync(0xffffffffu, sq, 1);
-                const uint64_t key = ((uint64_t)float_key(sq) << 32) | id;
-                if (ok && sl == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
-            }
-        } else {
-            for (int i = r0 + warp; i < r1; i += nw) {
-                const uint32_t id = list[i];
-                const float* row = data + (uint64_t)id * d;
-                float sq = 0.f;
-                for (int j = lane; j < d; j += 32) {
-                    const float df = s_q[j] - __ldg(row + j);
-                    sq = fmaf(df, df, sq);
-                }
-                sq = warp_sum(sq);
-                const uint64_t key = ((uint64_t)float_key(sq) << 32) | id;
-                if (lane == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
+                s_qi = lo;
             }
         }
         __syncthreads();
-        const int c = s_cnt;
+        const int item = s_item;
+        if (item >= (int)n_items) break;
+        const uint64_t qi = (uint64_t)s_qi;
+        if ((int)qi != cur) {
+            for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
+            if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
+            cur = (int)qi;
+        }
+        if (t == 0) {
+            s_cnt = 0;
+            s_ns = 0;
+            s_th = ~0ull;
+        }
         __syncthreads();
-        if (r1 < ns && c > kq) {  // more rows follow: keep the kq best
-            for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+        const uint32_t it0 = w.ritem_off[qi], nq_items = w.ritem_off[qi + 1] - it0;
+        const uint32_t c0 = (uint32_t)(item - (int)it0) * kRefChunk;
+        const int nc = (int)(min(w.cand_count[qi], c0 + kRefChunk) - min(w.cand_count[qi], c0));
+        const int kq = (int)q_k(w, qi);
+        const bool pred_q = apply_pred && q_sched(w, qi) == 0;  // predicate-first queries already passed it
+        uint32_t* list = w.cand_pool + w.soff[qi] + c0;
+        // 1. the predicate survivors, compacted in place as original ids (each chunk is read
+        //    before the barrier and written at or below its own start)
+        for (int base = 0; base < nc; base += kThreads) {
+            const int e = base + t;
+            bool keep = false;
+            uint32_t pool = kInvalid;
+            if (e < nc) {
+                pool = list[e];
+                keep = pool != kInvalid;
+                if (keep && pred_q) {
+                    const float* lab = D.labels + (uint64_t)pool * lbl;
+                    for (int i = 0; i < lbl; i++) {
+                        const float v = lab[i];
+                        if (v < s_box[2 * i] || v > s_box[2 * i + 1]) keep = false;
+                    }
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) s_wsum[warp] = __popc(bal);
             __syncthreads();
-            block_bitonic_sort(s_keys, cap);
-            if (t == 0) {
-                s_cnt = kq;
-                s_th = s_keys[kq - 1];
+            int before = s_ns, tot = 0;
+            for (int i = 0; i < nw; i++) {
+                before += i < warp ? s_wsum[i] : 0;
+                tot += s_wsum[i];
+            }
+            if (keep) list[before + __popc(bal & ((1u << lane) - 1))] = D.ids[pool];
+            __syncthreads();
+            if (t == 0) s_ns += tot;
+        }
+        __syncthreads();
+        const int ns = s_ns;
+        if (t == 0 && ns) atomicAdd(&w.rsurv[qi], (uint32_t)ns);
+        // 2. exact distances in rounds of cap - kq rows: every warp takes rows of the round, the
+        //    keys (distance, id) below the running k-th go to the buffer, which is sorted and cut
+        //    to kq after each round
+        const int per_round = max(cap - kq, 1);
+        // rows 16-byte aligned with d % 4 == 0: four rows per warp at a time, 8 lanes per row,
+        // 16-byte loads, four independent partial sums per lane (the gathers are latency-bound:
+        // this keeps ~6 KB per warp in flight instead of one 128-byte load per lane)
+        const bool vec4 = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(data) & 15) == 0;
+        for (int r0 = 0; r0 < ns; r0 += per_round) {
+            const int r1 = min(ns, r0 + per_round);
+            if (vec4) {
+                const int g = lane >> 3, sl = lane & 7, d4 = d >> 2;
+                const float4* q4 = reinterpret_cast<const float4*>(s_q);
+                for (int i0 = r0 + warp * 4; i0 < r1; i0 += nw * 4) {
+                    const int i = i0 + g;
+                    const bool ok = i < r1;
+                    const uint32_t id = ok ? list[i] : list[r0];
+                    const float4* row = reinterpret_cast<const float4*>(data + (uint64_t)id * d);
+                    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+                    int j = sl;
+                    for (; j + 24 < d4; j += 32) {
+                        const float4 x0 = __ldg(row + j), x1 = __ldg(row + j + 8), x2 = __ldg(row + j + 16),
+                                     x3 = __ldg(row + j + 24);
+                        const float4 y0 = q4[j], y1 = q4[j + 8], y2 = q4[j + 16], y3 = q4[j + 24];
+                        a0 = fmaf(y0.x - x0.x, y0.x - x0.x, a0);
+                        a0 = fmaf(y0.y - x0.y, y0.y - x0.y, a0);
+                        a0 = fmaf(y0.z - x0.z, y0.z - x0.z, a0);
+                        a0 = fmaf(y0.w - x0.w, y0.w - x0.w, a0);
+                        a1 = fmaf(y1.x - x1.x, y1.x - x1.x, a1);
+                        a1 = fmaf(y1.y - x1.y, y1.y - x1.y, a1);
+                        a1 = fmaf(y1.z - x1.z, y1.z - x1.z, a1);
+                        a1 = fmaf(y1.w - x1.w, y1.w - x1.w, a1);
+                        a2 = fmaf(y2.x - x2.x, y2.x - x2.x, a2);
+                        a2 = fmaf(y2.y - x2.y, y2.y - x2.y, a2);
+                        a2 = fmaf(y2.z - x2.z, y2.z - x2.z, a2);
+                        a2 = fmaf(y2.w - x2.w, y2.w - x2.w, a2);
+                        a3 = fmaf(y3.x - x3.x, y3.x - x3.x, a3);
+                        a3 = fmaf(y3.y - x3.y, y3.y - x3.y, a3);
+                        a3 = fmaf(y3.z - x3.z, y3.z - x3.z, a3);
+                        a3 = fmaf(y3.w - x3.w, y3.w - x3.w, a3);
+                    }
+                    for (; j < d4; j += 8) {
+                        const float4 x = __ldg(row + j), y = q4[j];
+                        a0 = fmaf(y.x - x.x, y.x - x.x, a0);
+                        a0 = fmaf(y.y - x.y, y.y - x.y, a0);
+                        a0 = fmaf(y.z - x.z, y.z - x.z, a0);
+                        a0 = fmaf(y.w - x.w, y.w - x.w, a0);
+                    }
+                    float sq = (a0 + a1) + (a2 + a3);
+                    sq += __shfl_xor_sync(0xffffffffu, sq, 4);
+                    sq += __shfl_xor_sync(0xffffffffu, sq, 2);
+                    sq += __shfl_xor_sync(0xffffffffu, sq, 1);
+                    const uint64_t key = ((uint64_t)float_key(sq) << 32) | id;
+                    if (ok && sl == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
+                }
+            } else {
+                for (int i = r0 + warp; i < r1; i += nw) {
+                    const uint32_t id = list[i];
+                    const float* row = data + (uint64_t)id * d;
+                    float sq = 0.f;
+                    for (int j = lane; j < d; j += 32) {
+                        const float df = s_q[j] - __ldg(row + j);
+                        sq = fmaf(df, df, sq);
+                    }
+                    sq = warp_sum(sq);
+                    const uint64_t key = ((uint64_t)float_key(sq) << 32) | id;
+                    if (lane == 0 && key < s_th) s_keys[atomicAdd(&s_cnt, 1)] = key;
+                }
             }
             __syncthreads();
+            const int c = s_cnt;
+            __syncthreads();
+            if (r1 < ns && c > kq) {  // more rows follow: keep the kq best
+                for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+                __syncthreads();
+                block_bitonic_sort(s_keys, cap);
+                if (t == 0) {
+                    s_cnt = kq;
+                    s_th = s_keys[kq - 1];
+                }
+                __syncthreads();
+            }
         }
-    }
-    const int c = s_cnt;
-    __syncthreads();
-    for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
-    __syncthreads();
-    block_bitonic_sort(s_keys, cap);
-    for (int i = t; i < k_out; i += blockDim.x) {
-        if (i < min(c, kq)) {
-            const uint64_t key = s_keys[i];
-            out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
-            out_ids[qi * k_out + i] = (uint32_t)key;
-        } else {
-            out_dist[qi * k_out + i] = INFINITY;
-            out_ids[qi * k_out + i] = ~0ull;
+        int c = s_cnt;
+        __syncthreads();
+        for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_sort(s_keys, cap);
+        bool write_out = nq_items == 1;
+        if (!write_out) {
+            // this item's best kq keys go to its partial row; the query's last item merges
+            uint64_t* part = w.rpart + (uint64_t)item * k_out;
+            for (int i = t; i < kq; i += blockDim.x) part[i] = i < c ? s_keys[i] : ~0ull;
+            __threadfence();
+            __syncthreads();
+            if (t == 0) s_last = atomicAdd(&w.rdone[qi], 1u) == nq_items - 1;
+            __syncthreads();
+            if (s_last) {
+                __threadfence();  // the other items' partial rows are visible past their counts
+                if (t == 0) {
+                    s_cnt = 0;
+                    s_th = ~0ull;
+                }
+                __syncthreads();
+                const uint64_t* rows = w.rpart + (uint64_t)it0 * k_out;
+                topk_rounds(s_keys, cap, kq, (int)nq_items * kq, &s_cnt, &s_th,
+                            [&](int i) { return __ldcg(rows + (uint64_t)(i / kq) * k_out + (i % kq)); });
+                c = s_cnt;
+                for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+                __syncthreads();
+                block_bitonic_sort(s_keys, cap);
+                write_out = true;
+            }
         }
+        if (write_out) {
+            for (int i = t; i < k_out; i += blockDim.x) {
+                if (i < min(c, kq) && s_keys[i] != ~0ull) {
+                    const uint64_t key = s_keys[i];
+                    out_dist[qi * k_out + i] = key_float((uint32_t)(key >> 32));
+                    out_ids[qi * k_out + i] = (uint32_t)key;
+                } else {
+                    out_dist[qi * k_out + i] = INFINITY;
+                    out_ids[qi * k_out + i] = ~0ull;
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -1666,7 +1877,7 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
 // ------------------------------------------------------------------------------------
 static uint32_t lut_groups(const IndexDev& D) { return (D.M + 31) / 32; }
 
-static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand, bool record) {
+static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     const hdg_params& P = idx->params;
     const uint64_t l = idx->dev.l, L = idx->dev.n_lists, C = idx->dev.C;
     const uint64_t Pc = std::max<uint64_t>(1, P.n_list), Ps = std::max<uint64_t>(1, P.sub_lists);
@@ -1702,8 +1913,11 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand,
     w.lut16 = P.lut_fp16 != 0;
     w.lut = (float*)take("lut", q * G * kCodes * 32 * (w.lut16 ? 2 : 4));
     w.cand_count = (uint32_t*)take("cand_count", q * 4);
-    w.cand_pool = (uint32_t*)take("cand_pool", q * kcand * 4);
-    w.kcand = kcand;
+    w.qbud = (uint32_t*)take("budget", q * 4);
+    w.soff = (uint64_t*)take("sel_off", (q + 1) * 8);
+    w.ritem_off = (uint32_t*)take("refine_items", (q + 1) * 4);
+    w.rdone = (uint32_t*)take("refine_done", q * 4);
+    w.rsurv = (uint32_t*)take("refine_rows", q * 4);
     w.ldS = C + L;
     w.S = (float*)take("gemm_s", q * (C + L) * 4);
     w.qnorm = (float*)take("qnorm", q * 4);
@@ -1713,26 +1927,51 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand,
     w.lq_ps = (uint32_t*)take("learned_nprobe", q * 4);
     w.lq_sched = (uint8_t*)take("learned_schedule", q);
     w.dist = static_cast<float*>(cx.dist_buf.ptr);
+    w.spos = static_cast<uint32_t*>(cx.pos_buf.ptr);
+    w.cand_pool = static_cast<uint32_t*>(cx.sel_buf.ptr);
+    w.sel_cap = cx.sel_buf.bytes / 4;
+    w.rpart = static_cast<uint64_t*>(cx.part_buf.ptr);
     if (!base) cx.work.bytes = std::max(cx.work.bytes, off);  // size probe
     return w;
 }
 
-static size_t workspace_bytes(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand) {
+// Partial rows of the refine items: at most one item per query plus one per kRefChunk
+// entries of the selection buffer, k keys each.
+static size_t part_bytes(const QueryCtx& cx, uint64_t q, uint32_t k) {
+    return (q + (cx.sel_buf.bytes / 4) / kRefChunk + 1) * (size_t)k * 8;
+}
+static void invalidate_ctx_graphs(QueryCtx& cx);
+static void ensure_part_buf(QueryCtx& cx, uint64_t q, uint32_t k) {
+    const size_t need = part_bytes(cx, q, k);
+    if (cx.part_buf.bytes >= need) return;
+    invalidate_ctx_graphs(cx);
+    cx.part_buf.reset();
+    cx.part_buf.ensure(need);
+}
+
+// The per-candidate rows: one f32 distance and one u32 position per candidate, same capacity.
+static void resize_rows(QueryCtx& cx, size_t bytes) {
+    cx.dist_buf.reset();
+    cx.pos_buf.reset();
+    cx.dist_buf.ensure(bytes);
+    cx.pos_buf.ensure(bytes);
+}
+
+static size_t workspace_bytes(hdg_index* idx, QueryCtx& cx, uint64_t q) {
     void* saved = cx.work.ptr;
     cx.work.ptr = nullptr;
     const size_t before = cx.work.bytes;
     cx.work.bytes = 0;
-    carve(idx, cx, q, kcand, false);
+    carve(idx, cx, q, false);
     const size_t need = cx.work.bytes;
     cx.work.ptr = saved;
     cx.work.bytes = before;
     return need;
 }
 
-static void reserve_ctx(hdg_index* idx, QueryCtx& cx, uint64_t q, uint64_t kcand) {
+static void reserve_ctx(hdg_index* idx, QueryCtx& cx, uint64_t q) {
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
-    if (kcand == 0) kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
-    const size_t need = workspace_bytes(idx, cx, q, kcand);
+    const size_t need = workspace_bytes(idx, cx, q);
     if (cx.work.ptr && cx.work.bytes >= need) return;
     cx.work.reset();
     cx.work.ensure(need);
@@ -1748,10 +1987,10 @@ static QueryCtx& query_ctx(hdg_index* idx, cudaStream_t st) {
     return *slot;
 }
 
-void reserve_workspace(hdg_index* idx, uint64_t q, uint64_t kcand, cudaStream_t st) {
+void reserve_workspace(hdg_index* idx, uint64_t q, cudaStream_t st) {
     QueryCtx& cx = query_ctx(idx, st);
     std::lock_guard<std::mutex> g(cx.mu);
-    reserve_ctx(idx, cx, q, kcand);
+    reserve_ctx(idx, cx, q);
 }
 
 FilterDev filter_dev(const hdg_index* idx) {
@@ -1776,34 +2015,56 @@ void upload_filter(hdg_index* idx) {
     if (!m.empty()) CK(cudaMemcpy(idx->map_buf.ptr, m.data(), m.size() * 4, cudaMemcpyHostToDevice));
 }
 
+// Stage times from consecutive recorded events (the first marks the start).
+static void store_stage_times(hdg_index* idx, const std::vector<cudaEvent_t>& ev,
+                              const std::vector<std::string>& names) {
+    std::lock_guard<std::mutex> g(idx->stats_mu);
+    idx->stage_names.clear();
+    idx->stage_ms.clear();
+    for (size_t i = 1; i < ev.size(); i++) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev[i - 1], ev[i]));
+        idx->stage_names.push_back(names[i]);
+        idx->stage_ms.push_back(ms);
+    }
+}
+
 namespace {
+// Events between the stages of one query batch.  On the plain path they are recorded on
+// the stream and read by finish(); while a CUDA graph is captured (keep != nullptr) they
+// become external event-record nodes of the graph, owned by its entry, and every replay
+// records them again, so the stage times of each replay can be read once it completes.
 struct StageTimer {
     hdg_index* idx;
     cudaStream_t st;
     bool on;
     std::vector<cudaEvent_t> ev;
     std::vector<std::string> names;
-    StageTimer(hdg_index* i, cudaStream_t s, bool enabled) : idx(i), st(s), on(enabled) { mark(""); }
+    std::vector<cudaEvent_t>* keep;
+    std::vector<std::string>* keep_names;
+    StageTimer(hdg_index* i, cudaStream_t s, bool enabled, std::vector<cudaEvent_t>* k = nullptr,
+               std::vector<std::string>* kn = nullptr)
+        : idx(i), st(s), on(enabled), keep(k), keep_names(kn) {
+        mark("");
+    }
     void mark(const char* name) {
         if (!on) return;
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
-        CK(cudaEventRecord(e, st));
-        ev.push_back(e);
-        names.push_back(name);
+        if (keep) {
+            keep->push_back(e);
+            keep_names->push_back(name);
+            CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+        } else {
+            ev.push_back(e);
+            names.push_back(name);
+            CK(cudaEventRecord(e, st));
+        }
     }
     void finish() {
-        if (!on) return;
+        if (!on || keep) return;
         CK(cudaEventSynchronize(ev.back()));
-        std::lock_guard<std::mutex> g(idx->stats_mu);
-        idx->stage_names.clear();
-        idx->stage_ms.clear();
-        for (size_t i = 1; i < ev.size(); i++) {
-            float ms = 0;
-            CK(cudaEventElapsedTime(&ms, ev[i - 1], ev[i]));
-            idx->stage_names.push_back(names[i]);
-            idx->stage_ms.push_back(ms);
-        }
+        store_stage_times(idx, ev, names);
     }
     ~StageTimer() {
         for (auto e : ev) cudaEventDestroy(e);
@@ -1845,6 +2106,8 @@ struct QueryCall {
 struct GraphEntry {
     uint64_t key[24];
     cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> stage_ev;     // event-record nodes between the stages (break_down=1)
+    std::vector<std::string> stage_names;
     uint64_t q = 0, launches = 0;
     int mode = 0;
     uint32_t k = 0;
@@ -1859,10 +2122,17 @@ struct GraphState {
     GraphEntry last;                // description of the last replay (stats)
 };
 
+static void destroy_entry(GraphEntry& e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    for (auto ev : e.stage_ev) cudaEventDestroy(ev);
+    e.exec = nullptr;
+    e.stage_ev.clear();
+    e.stage_names.clear();
+}
+
 void release_graphs(GraphState* g) {
     if (!g) return;
-    for (auto& e : g->entries)
-        if (e.exec) cudaGraphExecDestroy(e.exec);
+    for (auto& e : g->entries) destroy_entry(e);
     if (g->ev_in) cudaEventDestroy(g->ev_in);
     if (g->ev_out) cudaEventDestroy(g->ev_out);
     if (g->stream) cudaStreamDestroy(g->stream);
@@ -1873,8 +2143,7 @@ void release_graphs(GraphState* g) {
 static void invalidate_ctx_graphs(QueryCtx& cx) {
     if (!cx.graphs) return;
     if (cx.graphs->pending) cudaEventSynchronize(cx.graphs->ev_out);
-    for (auto& e : cx.graphs->entries)
-        if (e.exec) cudaGraphExecDestroy(e.exec);
+    for (auto& e : cx.graphs->entries) destroy_entry(e);
     cx.graphs->entries.clear();
     cx.graphs->pending = false;
 }
@@ -1907,8 +2176,7 @@ static void fill_stats(hdg_index* idx, uint64_t q, uint32_t k, int mode, uint64_
     } else if (mode == kL1) {
         K = exps0 * k;
     }
-    idx->last_ncand = K;
-    if (mode != kPre) K = std::max<uint64_t>(1, std::min<uint64_t>(K, (uint64_t)kMaxCand));
+    idx->last_ncand = K;  // no cap: the budget the reference computes is the one used
     idx->last_beta = beta;
     idx->last_q = q;
     uint32_t bits;
@@ -1922,7 +2190,8 @@ static void fill_stats(hdg_index* idx, uint64_t q, uint32_t k, int mode, uint64_
 // host (the CUDA-graph path): the distance buffer keeps its capacity, queries past it are
 // cut by k_batch, and the scalars and the GEMM status word are copied to pinned memory.
 static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cudaStream_t st, bool sync_sizing,
-                          uint64_t* pinned, uint64_t* launches_out, int* mode_out, uint64_t* coarse_out = nullptr) {
+                          uint64_t* pinned, uint64_t* launches_out, int* mode_out, uint64_t* coarse_out = nullptr,
+                          uint64_t* sel_out = nullptr, GraphEntry* capture = nullptr) {
     const uint64_t q = c.q;
     const uint32_t k = c.k;
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
@@ -1945,12 +2214,11 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     HDG_REQUIRE(mode == kPre || c.data, HDG_ERR_INVALID_ARG, "d_data is required for the re-rank");
     HDG_REQUIRE(mode != kPre || !c.qsched, HDG_ERR_INVALID_ARG,
                 "per-query schedules need exps0 > 1 (the pre-filter schedule has no re-rank)");
-    const uint64_t kcand = mode == kPre ? 1 : (uint64_t)kMaxCand;
-    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q, kcand)) {
+    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q)) {
         HDG_REQUIRE(sync_sizing, HDG_ERR_STATE, "workspace too small for a captured query");
-        reserve_ctx(idx, cx, q, kcand);
+        reserve_ctx(idx, cx, q);
     }
-    Workspace w = carve(idx, cx, q, kcand, true);
+    Workspace w = carve(idx, cx, q, true);
     w.qk = c.qk;
     w.qps = c.qps;
     w.qsched = c.qsched;
@@ -1959,8 +2227,10 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     w.exps0 = (uint32_t)std::min<uint64_t>(exps0, 1u << 20);
     w.chunk = P.scan_chunk ? (uint32_t)P.scan_chunk : kChunk;
     w.cap = sync_sizing ? ~0ull : cx.dist_buf.bytes / 4;
+    if (sync_sizing) w.sel_cap = ~0ull;  // sized after k_batch
     const FilterDev f = filter_dev(idx);
-    StageTimer tm(idx, st, sync_sizing && P.break_down != 0);
+    StageTimer tm(idx, st, P.break_down != 0 && (sync_sizing || capture), capture ? &capture->stage_ev : nullptr,
+                  capture ? &capture->stage_names : nullptr);
 
     const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
     if (sm_pro > 48 * 1024)
@@ -2016,17 +2286,27 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
         CK(cudaMemcpyAsync(&gemm_err, w.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         HDG_REQUIRE(gemm_err == 0, HDG_ERR_TIMEOUT, "tensor-core wait expired in the coarse GEMM");
-        const uint64_t coarse = sc[0];
+        const uint64_t coarse = sc[0], selected = sc[7];
         if (coarse_out) *coarse_out = coarse;
+        if (sel_out) *sel_out = selected;
         if (cx.dist_buf.bytes < std::max<uint64_t>(coarse, 1) * 4) {
             invalidate_ctx_graphs(cx);  // their distance pointer dies with the old buffer
-            cx.dist_buf.reset();
-            cx.dist_buf.ensure(std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
+            resize_rows(cx, std::max<uint64_t>(coarse, 1) * 4 * 5 / 4);
         }
+        if (cx.sel_buf.bytes < std::max<uint64_t>(selected, 1) * 4) {
+            invalidate_ctx_graphs(cx);  // and their selection pointer with this one
+            cx.sel_buf.reset();
+            cx.sel_buf.ensure(std::max<uint64_t>(selected, 1) * 4 * 5 / 4);
+        }
+        ensure_part_buf(cx, q, k);
     } else {
-        HDG_REQUIRE(cx.dist_buf.ptr, HDG_ERR_STATE, "no distance buffer for a captured query");
+        HDG_REQUIRE(cx.dist_buf.ptr && cx.sel_buf.ptr && cx.part_buf.bytes >= part_bytes(cx, q, k), HDG_ERR_STATE,
+                    "no candidate buffers for a captured query");
     }
     w.dist = static_cast<float*>(cx.dist_buf.ptr);
+    w.spos = static_cast<uint32_t*>(cx.pos_buf.ptr);
+    w.cand_pool = static_cast<uint32_t*>(cx.sel_buf.ptr);
+    w.rpart = static_cast<uint64_t*>(cx.part_buf.ptr);
     tm.mark("budget");
 
     const uint32_t G = lut_groups(D);
@@ -2099,13 +2379,18 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     launches++;
     tm.mark("select");
     if (mode != kPre) {
+        k_refine_plan<<<1, 1024, 0, st>>>(q, w);
+        CK_LAUNCH();
         const int rcap = (int)next_pow2(k + 4 * kThreads);  // rounds of rcap - k exact distances
         const size_t sm_ref = sizeof(uint64_t) * rcap + sizeof(float) * D.d + 16;
         CK(cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ref));
-        k_refine<<<(unsigned)q, kThreads, sm_ref, st>>>(D, c.queries, c.data, rcap, mode == kPost ? 1 : 0, l, w,
-                                                       c.dist, c.ids, (int)k);
+        // persistent over the refine items; no more CTAs than queries are useful for small batches
+        const uint64_t blocks = std::min<uint64_t>((uint64_t)sm_count() * occupancy_blocks(k_refine, kThreads, sm_ref),
+                                                   q + (cx.sel_buf.bytes / 4) / kRefChunk + 1);
+        k_refine<<<(unsigned)blocks, kThreads, sm_ref, st>>>(D, c.queries, c.data, rcap, mode == kPost ? 1 : 0, l, q,
+                                                            w, c.dist, c.ids, (int)k);
         CK_LAUNCH();
-        launches++;
+        launches += 2;
         tm.mark("refine");
     }
     if (!sync_sizing && pinned) {
@@ -2123,6 +2408,7 @@ static hdg_status finish_ctx(hdg_index* idx, QueryCtx& cx) {
     CK(cudaEventSynchronize(g->ev_out));
     g->pending = false;
     fill_stats(idx, g->last.q, g->last.k, g->last.mode, idx->params.exps0, g->pinned, g->last.launches);
+    if (!g->last.stage_ev.empty()) store_stage_times(idx, g->last.stage_ev, g->last.stage_names);
     if (static_cast<int>(g->pinned[8] & 0xffffffffu) != 0) return HDG_ERR_TIMEOUT;
     if (g->pinned[5] != 0) return HDG_ERR_OOM;
     return HDG_OK;
@@ -2183,14 +2469,20 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
     if (!hit) {
         // first call of this shape: the plain path computes this call's results and sizes
         // the buffers; the captured graph serves the next calls
-        uint64_t coarse = 0;
-        enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr, &coarse);
+        uint64_t coarse = 0, selected = 0;
+        enqueue_query(idx, cx, c, st, true, nullptr, nullptr, nullptr, &coarse, &selected);
         const uint64_t need = std::max<uint64_t>(coarse, 1) * 4 * 5 / 4;  // 1.25x this batch
         if (cx.dist_buf.bytes < need) {
             invalidate_ctx_graphs(cx);
-            cx.dist_buf.reset();
-            cx.dist_buf.ensure(need);
+            resize_rows(cx, need);
         }
+        const uint64_t need_sel = std::max<uint64_t>(selected, 1) * 4 * 5 / 4;
+        if (cx.sel_buf.bytes < need_sel) {
+            invalidate_ctx_graphs(cx);
+            cx.sel_buf.reset();
+            cx.sel_buf.ensure(need_sel);
+        }
+        ensure_part_buf(cx, q, k);
         make_graph_key(idx, cx, c, key);
         CK(cudaStreamSynchronize(st));
         GraphEntry e;
@@ -2198,20 +2490,22 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed));
         try {
-            enqueue_query(idx, cx, c, g->stream, false, g->pinned, &e.launches, &e.mode);
+            enqueue_query(idx, cx, c, g->stream, false, g->pinned, &e.launches, &e.mode, nullptr, nullptr, &e);
         } catch (...) {
             cudaStreamEndCapture(g->stream, &graph);
             if (graph) cudaGraphDestroy(graph);
+            destroy_entry(e);
             throw;
         }
         CK(cudaStreamEndCapture(g->stream, &graph));
         const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
         cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) destroy_entry(e);
         CK(ie);
         e.q = q;
         e.k = k;
         if (g->entries.size() >= 8) {
-            cudaGraphExecDestroy(g->entries.front().exec);
+            destroy_entry(g->entries.front());
             g->entries.erase(g->entries.begin());
         }
         g->entries.push_back(e);
@@ -2235,11 +2529,10 @@ void query_features(hdg_index* idx, const float* d_queries, uint64_t q, const fl
     const int fd = (int)std::max<uint64_t>(1, idx->params.filter_dim);
     HDG_REQUIRE(label_cols == (uint32_t)(D.l * fd), HDG_ERR_INVALID_ARG,
                 "query label columns must equal l * filter_dim");
-    const uint64_t kcand = idx->params.exps0 <= 1 ? 1 : (uint64_t)kMaxCand;
     QueryCtx& cx = query_ctx(idx, st);
     std::lock_guard<std::mutex> lock(cx.mu);
-    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q, kcand)) reserve_ctx(idx, cx, q, kcand);
-    Workspace w = carve(idx, cx, q, kcand, true);
+    if (!cx.work.ptr || cx.work.bytes < workspace_bytes(idx, cx, q)) reserve_ctx(idx, cx, q);
+    Workspace w = carve(idx, cx, q, true);
     const FilterDev f = filter_dev(idx);
     const size_t sm_pro = sizeof(uint32_t) * D.n_lists;
     if (sm_pro > 48 * 1024)

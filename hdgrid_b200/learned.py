@@ -2,9 +2,10 @@
 
 Labelling follows the method itself: every training query is run through the index at each
 probe count of ``PROBES`` under both schedules (0 = the index's own post-filter schedule,
-Super-Grid-IVF_PQ.cu:1151-1241; 1 = predicate-first scan with an exact re-rank), and is
-labelled with the cheapest setting -- fewest bytes scanned -- whose recall@k against the
-exact filtered kNN reaches ``target``; when none does, the setting with the best recall.
+Super-Grid-IVF_PQ.cu:1196-1236; 1 = predicate-first scan with an exact re-rank of exps0 * k,
+the schedule of the reference's batch-split branch, :1165-1171), and is labelled with the
+cheapest setting -- fewest bytes read by the scan and the re-rank -- whose recall@k against
+the exact filtered kNN reaches ``target``; when none does, the setting with the best recall.
 The MLP (48 -> 128 -> 128 -> 2, BF16, trained by the library's own kernels) regresses
 log2(probe count) and classifies the schedule.  The plain schedule stays the fallback
 (LEARNED=0) and, with the brute-force kNN, the yardstick of the learned schedule's recall.
@@ -67,12 +68,32 @@ class Batch:
         self.qout = hg.query_output_t(self.dist, self.ids)
 
     def run(self, idx, n_probe=None, schedule=None):
-        """Query through hdg_query_ex; returns (ids [q x k_max] u64, scanned candidates [q])."""
+        """Query through hdg_query_ex; returns (ids [q x k_max] u64, per-query work): the
+        work dict holds, per query, the scanned candidates ``cand``, the candidates with a
+        finite ADC distance ``nfin`` (the predicate survivors of a predicate-first query), the
+        selection handed to the re-rank ``sel`` and the rows re-ranked exactly ``rows``."""
         import torch
         idx.query_ex(self.qin, self.qout, k=self.k, n_probe=n_probe, schedule=schedule)
         torch.cuda.synchronize()
-        cand = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:, 0].copy()
-        return self.ids.cpu().numpy().view(np.uint64).copy(), cand
+        n = self.q.shape[0]
+
+        def u32(name):
+            return np.frombuffer(idx.debug_fetch(name).tobytes(), np.uint32)[:n].astype(np.int64)
+        work = {"cand": np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:n, 0]
+                .astype(np.int64), "nfin": u32("nfin"), "sel": u32("cand_count"), "rows": u32("refine_rows")}
+        return self.ids.cpu().numpy().view(np.uint64).copy(), work
+
+
+def query_bytes(work: dict, schedule, m: int, l: int, d: int) -> np.ndarray:
+    """Bytes a query reads per schedule (0 = post-filter, 1 = predicate-first), per query:
+    the scan (M code bytes per candidate; predicate-first: 4*l label bytes per candidate and M
+    per predicate survivor), the post-filter predicate on the selection (4*l per selected
+    candidate) and the exact re-rank (4*d per row)."""
+    sch = np.broadcast_to(np.asarray(schedule), work["cand"].shape).astype(bool)
+    cand = work["cand"].astype(np.float64)
+    scan = np.where(sch, cand * (4 * l) + work["nfin"] * m, cand * m)
+    refine = np.where(sch, 0.0, work["sel"] * (4.0 * l)) + work["rows"] * (4.0 * d)
+    return scan + refine
 
 
 def scan_bytes(cand: np.ndarray, schedule: int, m: int, l: int) -> np.ndarray:
@@ -85,7 +106,7 @@ def label_queries(idx, batch: Batch, gt: np.ndarray, probes=PROBES, target: floa
     """Per-query labels y [q x 2] = (log2 probe count, schedule) and the recall / cost tables."""
     import torch
     info = idx.info()
-    m, l = info["M"], info["l"]
+    m, l, d = info["M"], info["l"], info["d"]
     nq = batch.q.shape[0]
     dev = batch.q.device
     rec = np.zeros((len(schedules), len(probes), nq))
@@ -96,11 +117,11 @@ def label_queries(idx, batch: Batch, gt: np.ndarray, probes=PROBES, target: floa
         sch = torch.full((nq,), s, dtype=torch.uint8, device=dev)
         for pi, p in enumerate(probes):
             npb = torch.full((nq,), p, dtype=torch.uint32, device=dev)
-            ids, cand = batch.run(idx, n_probe=npb, schedule=sch)
+            ids, work = batch.run(idx, n_probe=npb, schedule=sch)
             h, tot = _hits(ids, gt, batch.ks)
             hits[si, pi] = h
             rec[si, pi] = np.where(tot > 0, h / np.maximum(tot, 1), 1.0)
-            cost[si, pi] = scan_bytes(cand, s, m, l)
+            cost[si, pi] = query_bytes(work, s, m, l, d)
     y = np.zeros((nq, 2), np.float32)
     chosen_hits = np.zeros(nq, np.int64)
     chosen_cost = np.zeros(nq)
@@ -169,3 +190,21 @@ def predicted_settings(idx, feats, max_probe: int):
     z = idx.mlp_forward(feats).cpu().numpy()
     p = np.clip(np.rint(np.exp2(np.clip(z[:, 0], 0, 20))), 1, max_probe).astype(np.uint32)
     return p, (z[:, 1] > 0).astype(np.uint8)
+
+
+def compare_at_equal_recall(learned_recall: float, learned_qps: float, plain: list, target: float = 0.95) -> dict:
+    """The learned schedule against the plain schedules at equal recall.  ``plain`` holds one
+    dict per plain setting with its ``recall`` and ``qps``.  The bar is recall@k >= target and
+    >= the learned recall; the fastest plain setting over the bar is the comparator.  When no
+    plain setting reaches it, the comparator is the plain setting with the highest recall,
+    which the learned schedule then also beats in recall."""
+    bar = max(target, learned_recall) if learned_recall >= target else learned_recall
+    ok = [p for p in plain if p["recall"] >= bar]
+    if ok:
+        best = max(ok, key=lambda p: p["qps"])
+        basis = f"fastest plain setting with recall >= {bar:.4f}"
+    else:
+        best = max(plain, key=lambda p: (p["recall"], p["qps"]))
+        basis = f"no plain setting reaches recall {bar:.4f}: the plain setting with the highest recall"
+    return {"target_recall": target, "learned_recall": learned_recall, "learned_meets_target": learned_recall >= target,
+            "learned_qps": learned_qps, "plain": best, "speedup": learned_qps / best["qps"], "basis": basis}

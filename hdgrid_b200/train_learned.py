@@ -99,13 +99,18 @@ def main():
     log["calibration"] = L.calibrate(idx, vb, gt_tr[args.train:], max_probe=max(L.PROBES))
     print(json.dumps(log), flush=True)
 
-    # held-out evaluation
+    # held-out evaluation: the plain schedules (no network) at every uniform probe count --
+    # the post-filter budget with its exact re-rank, and the pre-filter schedule (exps0 = 1)
+    # -- and the learned schedule, each device-timed
     qev = torch.from_numpy(ev["queries"]).to(dev)
     qlev = torch.from_numpy(ev["query_labels"]).to(dev)
     ksev = ev["ks"].astype(np.uint32)
     gt_ev = _gt(hg, base, labels, qev, qlev, ev["filter_conf"], 100)
     info = idx.info()
-    plain = {p: [0, 0, 0.0, 0.0] for p in L.PROBES}
+    m, l, d = info["M"], info["l"], info["d"]
+    exps0 = int(idx.params["exps0"])
+    scheds = (("post-filter", exps0), ("pre-filter", 1))
+    plain = {(sname, p): [0, 0, 0.0, 0.0] for sname, _ in scheds for p in L.PROBES}
     learned = [0, 0, 0.0, 0.0]
 
     def timed(batch, **kw):
@@ -119,31 +124,37 @@ def main():
     for a in range(0, qev.shape[0], args.step):
         b = min(qev.shape[0], a + args.step)
         batch = L.Batch(base, qev[a:b], qlev[a:b], ksev[a:b])
-        for p in L.PROBES:
-            idx.set_param("sub_lists", p)
-            ids, cand = batch.run(idx)
-            h, t = L._hits(ids, gt_ev[a:b], batch.ks)
-            plain[p][0] += int(h.sum())
-            plain[p][1] += int(t.sum())
-            plain[p][2] += float(L.scan_bytes(cand, 0, info["M"], info["l"]).sum())
-            plain[p][3] += timed(batch)
+        for sname, e0v in scheds:
+            idx.set_param("exps0", e0v)
+            for p in L.PROBES:
+                idx.set_param("sub_lists", p)
+                ids, work = batch.run(idx)
+                if e0v <= 1:  # no re-rank in the pre-filter schedule
+                    work = dict(work, sel=np.zeros_like(work["sel"]), rows=np.zeros_like(work["rows"]))
+                h, t = L._hits(ids, gt_ev[a:b], batch.ks)
+                v = plain[(sname, p)]
+                v[0] += int(h.sum())
+                v[1] += int(t.sum())
+                v[2] += float(L.query_bytes(work, 1 if e0v <= 1 else 0, m, l, d).sum())
+                v[3] += timed(batch)
+        idx.set_param("exps0", exps0)
         idx.set_param("sub_lists", max(L.PROBES))
         fe = idx.query_features(batch.q, batch.ql, 100, k=batch.k)
         pp, ff = L.predicted_settings(idx, fe, max(L.PROBES))
         idx.set_param("learned", 1)
-        ids, cand = batch.run(idx)
+        ids, work = batch.run(idx)
         learned[3] += timed(batch)
         idx.set_param("learned", 0)
         h, t = L._hits(ids, gt_ev[a:b], batch.ks)
         learned[0] += int(h.sum())
         learned[1] += int(t.sum())
-        learned[2] += float((cand * np.where(ff == 1, info["M"] + 4 * info["l"], info["M"])).sum())
+        learned[2] += float(L.query_bytes(work, ff, m, l, d).sum())
     n = qev.shape[0]
-    report = dict(log, heldout=args.heldout, train=args.train,
-                  plain=[{"sub_lists": p, "recall": v[0] / max(v[1], 1), "scan_bytes": v[2], "qps": n / (v[3] / 1e3)}
-                         for p, v in plain.items()],
-                  learned={"recall": learned[0] / max(learned[1], 1), "scan_bytes": learned[2],
-                           "qps": n / (learned[3] / 1e3)})
+    plain_rows = [{"schedule": sname, "sub_lists": p, "recall": v[0] / max(v[1], 1), "bytes": v[2],
+                   "qps": n / (v[3] / 1e3)} for (sname, p), v in plain.items()]
+    lrow = {"recall": learned[0] / max(learned[1], 1), "bytes": learned[2], "qps": n / (learned[3] / 1e3)}
+    report = dict(log, heldout=args.heldout, train=args.train, plain=plain_rows, learned=lrow,
+                  learned_vs_plain=L.compare_at_equal_recall(lrow["recall"], lrow["qps"], plain_rows))
     out = Path(args.out)
     out.parent.mkdir(parents=True, exist_ok=True)
     np.save(out, idx.mlp_weights())

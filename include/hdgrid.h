@@ -184,11 +184,11 @@ hdg_status hdg_mlp_train(hdg_index* index, const float* d_x, const float* d_y, u
                          double* final_loss, void* stream);
 
 /* Scalars of the last hdg_query: out[0] queries, [1] candidate budget n_cand as the
- * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget actually used (capped by the
- * shared-memory top-K), [3] sum of Morton candidate-range sizes, [4] sum of exact filtered
- * counts of the probed lists, [5] largest per-query candidate count, [6] beta as float bits,
- * [7] schedule (0 pre-filter, 1 post-filter, 2 single label dim), [8] kernels launched,
- * [9] reserved.  Returns entries written (<= 10). */
+ * reference computes it (Super-Grid-IVF_PQ.cu:1222), [2] budget used (the same value: no
+ * cap), [3] sum of Morton candidate-range sizes, [4] sum of exact filtered counts of the
+ * probed lists, [5] largest per-query candidate count, [6] beta as float bits, [7] schedule
+ * (0 pre-filter, 1 post-filter, 2 single label dim), [8] kernels launched, [9] queries
+ * dropped by a captured graph's buffer capacity.  Returns entries written (<= 10). */
 int hdg_last_query_stats(hdg_index* index, uint64_t* out, int cap);
 
 /* With QUERY_GRAPH=1 hdg_query returns once the captured graph is enqueued; this waits for
@@ -217,9 +217,10 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
 
 /* Copy a named intermediate buffer of the last query to host memory (parity tests).
  * Names: "box", "cells", "zrange", "list_counts", "cluster_counts", "probe_clusters",
- * "probe_lists", "range_start", "range_len", "cand_pool", "cand_count", "scalars", "qoff",
- * "qstat", and "distances" (the f32 ADC distance of every scanned candidate, query rows at
- * the "qoff" offsets). */
+ * "probe_lists", "range_start", "range_len", "cand_count", "budget", "sel_off", "scalars",
+ * "qoff", "qstat", "distances" (the f32 ADC distance of every scanned candidate, query rows
+ * at the "qoff" offsets) and "cand_pool" (each query's selected candidates, rows at the
+ * "sel_off" offsets, "cand_count" of them). */
 hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,
                            size_t bytes, size_t* bytes_needed);
 
@@ -278,7 +279,11 @@ hdg_status hdg_bf16_gemm(const void* d_a, uint64_t rows, const void* d_b, uint64
  * return HDG_ERR_INVALID_ARG.  The first call on a device looks up the scratch array's
  * device address (make that device current, and make that first call before any stream
  * capture).  All calls share the one array: calls whose work overlaps on the GPU (other
- * streams, other threads) race on it and must be serialised by the caller. */
+ * streams, other threads) race on it and must be serialised by the caller.  The map is
+ * copied from spec->interval_map on `stream` (stream-ordered): that host memory must stay
+ * valid and unchanged until the call's stream work has completed.  The looked-up address
+ * is kept per device ordinal for the life of the process; it does not survive a
+ * cudaDeviceReset (or a primary-context reset) of that device. */
 #define HDG_NOALLOC_MAP_MAX 65536
 hdg_status hdg_recover_filters_noalloc(const hdg_filter_spec* spec, const float* d_query_labels,
                                        uint64_t n_queries, float* d_ranges, void* stream);

@@ -50,6 +50,8 @@ def _load() -> C.CDLL:
     lib.ora_select_elements.argtypes = [vp, C.c_uint64, C.c_uint64, vp, C.c_uint64, C.c_uint64, C.c_int, C.c_float,
                                         vp]
     lib.ora_recover_filters.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int, C.c_int, vp, C.c_uint64, vp]
+    lib.ora_cell_boxes.argtypes = [vp, C.c_uint64, C.c_int, vp, vp, vp, vp, vp]
+    lib.ora_next_in_box.argtypes = [vp, vp, C.c_uint64, C.c_int, C.c_int, C.c_int, vp, vp]
     lib.ora_grid_shape.restype = C.c_int
     lib.ora_grid_shape.argtypes = [vp, vp, C.c_int, C.c_uint64, C.c_uint64, vp, vp, vp, vp, vp, vp]
     lib.ora_info.argtypes = [vp, vp]
@@ -147,6 +149,26 @@ def grid_shape(mins, maxs, max_grids, label_mask=0):
                 max_bits=int(mb[0]), valid_map=int(vm[0]))
 
 
+def cell_boxes(boxes, dims, shuffle, left, span):
+    """Cell box [n x 2l] i32 of each f32 filter box [n x 2l] on a grid in shuffled order."""
+    boxes = _c(boxes, np.float32)
+    n, l = boxes.shape[0], boxes.shape[1] // 2
+    out = np.empty((n, 2 * l), np.int32)
+    dm, sh, lf, sp = _c(dims, np.int32), _c(shuffle, np.int32), _c(left, np.uint64), _c(span, np.uint64)
+    LIB.ora_cell_boxes(_p(boxes), n, l, _p(dm), _p(sh), _p(lf), _p(sp), _p(out))
+    return out
+
+
+def next_in_box(cur, boxes, dims, max_bits, valid_map):
+    """(next code, found) of the reference's next-in-box jump for each (code, cell box)."""
+    cur = _c(cur, np.uint64)
+    boxes = _c(boxes, np.int32)
+    nx = np.empty(cur.shape[0], np.uint64)
+    ok = np.empty(cur.shape[0], np.int32)
+    LIB.ora_next_in_box(_p(cur), _p(boxes), cur.shape[0], dims, max_bits, valid_map, _p(nx), _p(ok))
+    return nx, ok
+
+
 def bruteforce_f64(data, labels, queries, ranges, k, threads=0):
     data, labels = _c(data, np.float32), _c(labels, np.float32)
     queries, ranges = _c(queries, np.float32), _c(ranges, np.float32)
@@ -194,9 +216,10 @@ class OracleIndex:
         return int(LIB.ora_check_layout(self._h))
 
     def query(self, queries, query_labels, data, k, threads=0, trace=True, adc_rotated=False,
-              qk=None, n_probe=None, schedule=None):
+              qk=None, n_probe=None, schedule=None, prefix_counts=False):
         """The reference query; qk / n_probe (uint32) and schedule (uint8) are the optional
-        per-query arrays of hdg_query_ex."""
+        per-query arrays of hdg_query_ex.  prefix_counts: per-list counts by the reference's
+        inclusion-exclusion over the index's prefix counts instead of a direct count."""
         n_list, sub_lists = self.n_list, self.sub_lists
         qk = None if qk is None else _c(qk, np.uint32)
         n_probe = None if n_probe is None else _c(n_probe, np.uint32)
@@ -220,7 +243,75 @@ class OracleIndex:
             tr = _Trace(*(t[n].ctypes.data for n, _ in _Trace._fields_))
         opt = [None if a is None else _p(a) for a in (qk, n_probe, schedule)]
         rc = LIB.ora_query_ex(self._h, _p(queries), q, _p(ql), ql.shape[1], _p(data), k, *opt, _p(dist), _p(ids),
-                              C.byref(tr) if tr is not None else None, threads, 1 if adc_rotated else 0)
+                              C.byref(tr) if tr is not None else None, threads,
+                              (1 if adc_rotated else 0) | (2 if prefix_counts else 0))
         if rc != 0:
             raise RuntimeError(LIB.ora_last_error().decode())
         return dist, ids, t
+
+
+class ReferenceStages:
+    """The reference's own integer-stage device functions (oracle/_ref/libhdgref.so, built by
+    oracle/ref_build.py from a reference checkout), run on the GPU through a small harness:
+    the oracle's restatement is checked against them.  Inputs must stay inside what the
+    reference code indexes safely (map labels inside the table, a non-zero valid map)."""
+
+    def __init__(self, lib: C.CDLL):
+        self.lib = lib
+        u64, vp = C.c_uint64, C.c_void_p
+        lib.ref_denormalize.argtypes = [vp, u64, u64, vp, vp, vp, u64, vp, u64, vp]
+        lib.ref_filter_grid_ranges.argtypes = [vp, u64, C.c_int, vp, vp, vp, vp, vp]
+        lib.ref_grid_id.argtypes = [vp, u64, u64, u64, C.c_int, vp]
+        lib.ref_morton_encode.argtypes = [vp, u64, C.c_int, C.c_int, C.c_int, vp]
+        lib.ref_next_z.argtypes = [vp, vp, u64, C.c_int, C.c_int, C.c_int, vp, vp]
+
+    @staticmethod
+    def _ok(rc):
+        if rc != 0:
+            raise RuntimeError(f"reference stage kernel failed: CUDA error {rc}")
+
+    def denormalize(self, spec: dict, labels, filter_dim: int = 1):
+        lab = _c(labels, np.float32)
+        l = spec["l"]
+        out = np.empty((lab.shape[0], 2 * l), np.float32)
+        mp = _c(spec["interval_map"] or [0.0], np.float32)
+        sh, ty, dv = _c(spec["shift_val"], np.float32), _c(spec["type"], np.int32), _c(spec["div_value"], np.int32)
+        self._ok(self.lib.ref_denormalize(_p(lab), lab.shape[0], lab.shape[1], _p(sh), _p(ty), _p(mp),
+                                          len(spec["interval_map"]), _p(dv), l, _p(out)))
+        return out
+
+    def filter_grid_ranges(self, boxes, dims, shuffle, left, span):
+        boxes = _c(boxes, np.float32)
+        n, l = boxes.shape[0], boxes.shape[1] // 2
+        out = np.empty((n, 2 * l), np.int32)
+        dm, sp, lf, sh = _c(dims, np.int32), _c(span, np.uint64), _c(left, np.uint64), _c(shuffle, np.int32)
+        self._ok(self.lib.ref_filter_grid_ranges(_p(boxes), n, l, _p(dm), _p(sp), _p(lf), _p(sh), _p(out)))
+        return out
+
+    def grid_id(self, x, left, span, m):
+        x = _c(x, np.float32)
+        out = np.empty(x.shape[0], np.int32)
+        self._ok(self.lib.ref_grid_id(_p(x), x.shape[0], left, span, m, _p(out)))
+        return out
+
+    def morton_encode(self, coords, dims, max_bits, valid_map):
+        c = _c(coords, np.int32)
+        out = np.empty(c.shape[0], np.uint64)
+        self._ok(self.lib.ref_morton_encode(_p(c), c.shape[0], dims, max_bits, valid_map, _p(out)))
+        return out
+
+    def next_z(self, cur, boxes, dims, max_bits, valid_map):
+        cur = _c(cur, np.uint64)
+        b = _c(boxes, np.int32)
+        nx = np.empty(cur.shape[0], np.uint64)
+        ok = np.empty(cur.shape[0], np.int32)
+        self._ok(self.lib.ref_next_z(_p(cur), _p(b), cur.shape[0], dims, max_bits, valid_map, _p(nx), _p(ok)))
+        return nx, ok
+
+
+def reference_stages():
+    """The reference's integer-stage kernels, or None when oracle/_ref/libhdgref.so is absent."""
+    path = _DIR / "_ref" / "libhdgref.so"
+    if not path.exists():
+        return None
+    return ReferenceStages(C.CDLL(str(path)))

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -69,6 +70,15 @@ struct Filter {
     std::vector<float> map;
 };
 
+// A C-style f32 -> s32 cast as the GPU executes it (cvt.rzi.s32.f32): truncation, NaN -> 0,
+// saturating at INT_MIN / INT_MAX.  An x86 cast of an out-of-range value gives INT_MIN instead.
+static int cuda_f2i(float x) {
+    if (x != x) return 0;
+    if (x >= 2147483648.0f) return INT_MAX;
+    if (x <= -2147483648.0f) return INT_MIN;
+    return (int)x;
+}
+
 // denormalize_labels_kernel (src/core/preprocessing.cu:3-32) for one query row.
 void recover_row(const Filter& f, const float* row, float* out) {
     for (int i = 0; i < f.l; i++) {
@@ -83,8 +93,8 @@ void recover_row(const Filter& f, const float* row, float* out) {
             }
             case 1: {  // label - 1 indexes the flat interval table (:18-20)
                 volatile float t = row[i] - 1.0f;
-                const int v = (int)t;
-                if (v >= 0 && 2 * v + 1 < (int)f.map.size()) {
+                const int v = cuda_f2i(t);
+                if (v >= 0 && 2 * (int64_t)v + 1 < (int64_t)f.map.size()) {
                     lo = f.map[2 * v];
                     hi = f.map[2 * v + 1];
                 } else {  // out of the table: undefined in the reference; empty here
@@ -94,8 +104,10 @@ void recover_row(const Filter& f, const float* row, float* out) {
                 break;
             }
             case 2: {  // integer division, upper bound FLT_MAX (:22-25)
-                const int v = (int)row[i];
-                lo = (float)(v / (f.div[i] ? f.div[i] : 1));
+                const int v = cuda_f2i(row[i]);
+                const int dv = f.div[i] ? f.div[i] : 1;
+                // INT_MIN / -1 is the one quotient that overflows: kept as INT_MIN (as the kernels do)
+                lo = (float)((v == INT_MIN && dv == -1) ? v : v / dv);
                 hi = FLT_MAX;
                 break;
             }
@@ -400,6 +412,32 @@ uint64_t ora_morton_encode(const int* coords, int dims, int max_bits, int valid_
 
 int ora_grid_id(float x, uint64_t left, uint64_t len, int M) { return grid_id(x, left, len, M); }
 
+// get_filter_grid_ranges_kernel (Super-Grid-IVF_PQ.cu:930-961) for n boxes [n x 2l] f32 against
+// a grid given in shuffled order (dims, shuffle, left, span); cells [n x 2l] i32.
+void ora_cell_boxes(const float* boxes, uint64_t n, int l, const int* dims, const int* shuffle, const uint64_t* left,
+                    const uint64_t* span, int32_t* cells) {
+    Grid g;
+    g.l = l;
+    for (int i = 0; i < l; i++) {
+        g.dims[i] = dims[i];
+        g.shuffle[i] = shuffle[i];
+        g.left[i] = left[i];
+        g.span[i] = span[i];
+    }
+    for (uint64_t r = 0; r < n; r++) cell_box(g, boxes + r * 2 * l, cells + r * 2 * l);
+}
+
+// getNextZValueBaseline (zorder.cu:83-244) for n (code, cell box [2 * dims]) pairs: next[i] and
+// ok[i] (0 where the reference returns false).
+void ora_next_in_box(const uint64_t* cur, const int32_t* boxes, uint64_t n, int dims, int max_bits, int valid_map,
+                     uint64_t* next, int32_t* ok) {
+    for (uint64_t r = 0; r < n; r++) {
+        uint64_t nx = 0;
+        ok[r] = next_in_box(cur[r], boxes + r * 2 * dims, dims, max_bits, valid_map, &nx) ? 1 : 0;
+        next[r] = ok[r] ? nx : 0;
+    }
+}
+
 // calc_grid_shape (Super-Grid-IVF_PQ.cu:305-412).  Outputs dims/shuffle/left/span in shuffled
 // order plus max_bits and valid_map.  A zero span is raised to 1 (division by zero upstream).
 int ora_grid_shape(const float* mins, const float* maxs, int l, uint64_t max_grids, uint64_t label_mask, int* dims,
@@ -409,7 +447,13 @@ int ora_grid_shape(const float* mins, const float* maxs, int l, uint64_t max_gri
     for (int i = 0; i < l; i++) cnt += (lm >> i) & 1;
     std::vector<std::pair<uint64_t, int>> sp(l);
     for (int i = 0; i < l; i++) {
-        uint64_t s = (uint64_t)(std::ceil((double)maxs[i]) - std::floor((double)mins[i]));
+        // `ceil(global_max[i]) - floor(global_min[i])` (:326) on float elements: the float
+        // overloads, so the difference is rounded to f32 (a span above 2^24 with an odd
+        // exact difference loses its last bit) before the uint64 conversion
+        volatile float mx = std::ceil(maxs[i]);
+        volatile float mn = std::floor(mins[i]);
+        volatile float diff = mx - mn;
+        uint64_t s = (uint64_t)diff;
         sp[i] = {s ? s : 1, i};
     }
     int main_grids = (int)std::floor(std::sqrt((double)max_grids));
@@ -574,6 +618,27 @@ uint64_t ora_check_layout(void* h) {
     const Index& ix = *static_cast<Index*>(h);
     const Grid& g = ix.g;
     uint64_t bad = 0;
+    // the stored grid against calc_grid_shape re-derived here from the stored labels' extremes
+    // (calculate_batch_min_max, Super-Grid-IVF_PQ.cu:308-310)
+    if (ix.n && ix.l) {
+        std::vector<float> mn(ix.l, FLT_MAX), mx(ix.l, -FLT_MAX);
+        for (uint64_t p = 0; p < ix.n; p++)
+            for (uint64_t i = 0; i < ix.l; i++) {
+                mn[i] = std::min(mn[i], ix.labels[p * ix.l + i]);
+                mx[i] = std::max(mx[i], ix.labels[p * ix.l + i]);
+            }
+        int dims[kMaxDims], sh[kMaxDims], mb = 0, vm = 0;
+        uint64_t left[kMaxDims], span[kMaxDims];
+        if (ora_grid_shape(mn.data(), mx.data(), (int)ix.l, ix.params[7], ix.params[11], dims, sh, left, span, &mb,
+                           &vm) != 0)
+            bad++;
+        else {
+            for (uint64_t i = 0; i < ix.l; i++)
+                bad += (dims[i] != g.dims[i]) + (sh[i] != g.shuffle[i]) + (left[i] != g.left[i]) +
+                       (span[i] != g.span[i]);
+            bad += (mb != g.max_bits) + (vm != g.valid_map);
+        }
+    }
     std::vector<uint32_t> dense(g.tot_cells * ix.L, 0);
     for (uint64_t j = 0; j < ix.L; j++)
         for (uint32_t p = ix.list_off[j]; p < ix.list_off[j + 1]; p++) {
@@ -629,7 +694,9 @@ struct OraTrace {
 // count clamped to [1, k] (rows keep stride k); qps probed sub-lists clamped to
 // [1, sub_lists]; qsched 1 = label predicate during the ADC pass, budget exps0*k_q, exact
 // re-rank without a second predicate.  These have no reference counterpart; with all three
-// NULL this is the reference's query.
+// NULL this is the reference's query.  adc_mode bit 0: the scan's lane-rotated ADC order
+// (below); bit 1: per-list counts from the index's prefix counts, as the reference counts
+// (otherwise a direct count of the points in the cell box, the independent check).
 int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels, uint32_t label_cols,
                  const float* data, uint32_t k, const uint32_t* qk, const uint32_t* qps, const uint8_t* qsched,
                  float* out_dist, uint64_t* out_ids, OraTrace* tr, int threads, int adc_mode) {
@@ -668,17 +735,49 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
         // the cell box over the unmasked dims -- equal to the reference's 2^d-corner
         // inclusion-exclusion over its compressed prefix sums (:648-765).
         std::vector<uint32_t> lc(L, 0);
-        for (uint64_t j = 0; j < L; j++) {
-            uint32_t cnt = 0;
-            for (uint32_t p = ix.list_off[j]; p < ix.list_off[j + 1]; p++) {
-                int c[kMaxDims];
-                point_cell(g, &ix.labels[(uint64_t)p * l], c);
-                bool in = true;
-                for (int i = 0; i < l && in; i++)
-                    if (((g.valid_map >> i) & 1) && (c[i] < lo[i] || c[i] > hi[i])) in = false;
-                cnt += in;
+        if (adc_mode & 2) {
+            // the reference's own count (get_prefix_sum_device, :693-724): inclusion-exclusion
+            // over the 2^d corners of the cell box, read from the index's inclusive per-list
+            // prefix counts (a lower corner below cell 0 contributes nothing)
+            int dv = 0;
+            for (int i = 0; i < l; i++) dv += (g.valid_map >> i) & 1;
+            std::vector<long long> acc(L, 0);
+            for (int mask = 0; mask < (1 << dv); mask++) {
+                int sign = 1, vi = 0;
+                bool zero = false;
+                uint64_t flat = 0;
+                for (int i = 0; i < l; i++) {
+                    int c = 0;
+                    if ((g.valid_map >> i) & 1) {
+                        if ((mask >> vi) & 1) {
+                            c = lo[i] - 1;
+                            sign = -sign;
+                            if (c < 0) zero = true;
+                        } else {
+                            c = hi[i];
+                        }
+                        vi++;
+                    }
+                    flat += (uint64_t)(c < 0 ? 0 : c) * g.stride[i];
+                }
+                if (zero) continue;
+                const uint32_t* row = &ix.prefix[flat * L];
+                for (uint64_t j = 0; j < L; j++) acc[j] += sign * (long long)row[j];
             }
-            lc[j] = cnt;
+            for (uint64_t j = 0; j < L; j++) lc[j] = (uint32_t)acc[j];
+        } else {
+            for (uint64_t j = 0; j < L; j++) {
+                uint32_t cnt = 0;
+                for (uint32_t p = ix.list_off[j]; p < ix.list_off[j + 1]; p++) {
+                    int c[kMaxDims];
+                    point_cell(g, &ix.labels[(uint64_t)p * l], c);
+                    bool in = true;
+                    for (int i = 0; i < l && in; i++)
+                        if (((g.valid_map >> i) & 1) && (c[i] < lo[i] || c[i] > hi[i])) in = false;
+                    cnt += in;
+                }
+                lc[j] = cnt;
+            }
         }
         // coarse: exact L2 to clusters with a non-zero count, sorted (::refine, :1034-1042)
         std::vector<std::pair<float, uint32_t>> cl;
@@ -835,7 +934,7 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
         auto adc = [&](uint32_t pool, uint32_t pos) {
             float sum = 0.f;
             const uint8_t* cp = &ix.codes[(uint64_t)pool * ix.M_pad];
-            if (adc_mode == 1) {
+            if (adc_mode & 1) {
                 // even steps and odd steps in two running sums, added at the end
                 const int lane = (int)(pos & 31);
                 float s1 = 0.f;
@@ -863,8 +962,11 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
                 if (pre && !pred(p)) continue;  // query_prefilter (prefiltering.cu:36-51)
                 cand.push_back({adc(p, pos), p});
             }
-        std::sort(cand.begin(), cand.end());
+        // the smallest (distance, pool row) pairs; pairs are unique, so a selection gives the
+        // same set a full sort would
         if (mode == 0) {
+            const size_t nk = std::min<size_t>(cand.size(), kq);
+            std::partial_sort(cand.begin(), cand.begin() + nk, cand.end());
             for (uint32_t j = 0; j < k; j++) {
                 out_dist[qi * k + j] = j < std::min<size_t>(cand.size(), kq) ? cand[j].first : INFINITY;
                 out_ids[qi * k + j] = j < std::min<size_t>(cand.size(), kq) ? ix.ids[cand[j].second] : ~0ull;
@@ -872,7 +974,10 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
             continue;
         }
         const uint64_t Kq = (qk || qsched) ? budget(kq, sched1) : K;
-        if (cand.size() > Kq) cand.resize(Kq);
+        if (cand.size() > Kq) {
+            std::nth_element(cand.begin(), cand.begin() + Kq, cand.end());
+            cand.resize(Kq);
+        }
         std::vector<std::pair<float, uint32_t>> fin;
         for (const auto& c : cand) {
             if (mode == 1 && !sched1 && !pred(c.second)) continue;  // post-filter predicate (:1227-1236)

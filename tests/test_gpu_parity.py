@@ -153,9 +153,17 @@ def test_parity_config2_small_postfilter(cuda):
 
 
 def test_parity_config4_small_range_filters(cuda):
+    import oracle
     ws = datasets.config4(scale=0.002, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
                           max_grids=4096)
-    _parity(ws, cuda)
+    _, r = _parity(ws, cuda)
+    # the oracle's prefix-count mode (the reference's inclusion-exclusion, used by the timed CPU
+    # arm) gives the same per-list counts and results as its direct count
+    ora = oracle.OracleIndex(r["path"])
+    _, ids_p, tp = ora.query(ws["queries"], ws["query_labels"], ws["base"], ws["k"], prefix_counts=True)
+    _, ids_d, td = ora.query(ws["queries"], ws["query_labels"], ws["base"], ws["k"])
+    assert np.array_equal(tp["list_counts"], td["list_counts"])
+    assert np.array_equal(ids_p, ids_d)
 
 
 def test_parity_prefilter_rotated_adc(cuda):
@@ -244,6 +252,28 @@ def test_select_handles_large_budget(cuda):
     ws = datasets.config2(scale=0.01, n_queries=100, clusters=16, sub_clusters=4, n_list=16, sub_lists=64,
                           max_grids=20_000, exps0=40)
     _parity(ws, cuda)
+
+
+def test_parity_postfilter_budget_is_not_capped(cuda):
+    # The post-filter budget is the reference's min(exps0 * k * beta, max_row_len)
+    # (Super-Grid-IVF_PQ.cu:1219-1222) with no cap: exps0 = 200 and k = 100 put it at 20,000
+    # or more (beta >= 1), above the 16,384 clamp an earlier version applied.  The oracle
+    # takes the same uncapped budget; with its ADC summed in the scan's order the selected sets
+    # agree, and the re-ranked results match.
+    ws = datasets.config4(scale=0.01, n_queries=200, clusters=16, sub_clusters=4, n_list=16, sub_lists=64,
+                          max_grids=4096, exps0=200)
+    idx, r = _parity(ws, cuda, adc_rotated=True)
+    st = idx.last_query_stats()
+    assert st["schedule"] == "post-filter"
+    assert st["n_cand_ref"] == st["n_cand_used"] > 16384, st
+    qs = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)
+    bud = np.frombuffer(idx.debug_fetch("budget").tobytes(), np.uint32)[:qs.shape[0]]
+    sel = np.frombuffer(idx.debug_fetch("cand_count").tobytes(), np.uint32)[:qs.shape[0]]
+    nfin = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:qs.shape[0]]
+    assert (bud == st["n_cand_ref"]).all()
+    # every query selects min(n_cand, its finite ADC distances) candidates
+    assert np.array_equal(sel, np.minimum(bud, nfin))
+    assert (sel > 16384).any()
 
 
 def test_parity_masked_label_dim(cuda):

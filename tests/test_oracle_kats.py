@@ -96,6 +96,33 @@ def test_grid_shape_masked_dim_and_single_dim():
     assert g1["dims"] == [999_999] and g1["max_bits"] == 20
 
 
+def test_grid_shape_span_is_an_f32_difference():
+    # calc_grid_shape's `ceil(global_max[i]) - floor(global_min[i])` runs on float elements
+    # (Super-Grid-IVF_PQ.cu:326): under nvcc the float overloads are chosen, so a span above
+    # 2^24 whose exact difference is odd is rounded to f32 before the uint64 conversion
+    g = oracle.grid_shape([13.0], [29_999_980.0], 1_000_000_000)
+    want = int(np.float32(np.ceil(np.float32(29_999_980.0))) - np.float32(np.floor(np.float32(13.0))))
+    assert want == 29_999_968 and g["span"] == [want]
+    # below 2^24 the f32 difference is exact
+    assert oracle.grid_shape([3.0], [9_999.0], 1_000_000)["span"] == [9_996]
+
+
+def test_recover_filters_out_of_table_and_saturating_casts():
+    # map: label - 1 indexes a 2-row table; labels past it (also 2^30 and above, where
+    # 2 * v + 1 no longer fits in 32 bits, and 3e9, which the GPU's f32 -> s32 cast saturates
+    # to INT_MAX) and label 0 give the empty box (FLT_MAX, -FLT_MAX)
+    fmax = np.finfo(np.float32).max
+    spec = {"l": 1, "type": [1], "shift_val": [0.0, 0.0], "div_value": [0], "interval_map": [1.0, 2.0, 3.0, 4.0]}
+    bad = np.array([[3.0], [2.0 ** 30], [1.5e9], [3e9], [0.0], [-5.0]], np.float32)
+    out = oracle.recover_filters(spec, bad)
+    assert (out[:, 0] == fmax).all() and (out[:, 1] == -fmax).all(), out
+    assert oracle.recover_filters(spec, np.array([[2.0]], np.float32)).ravel().tolist() == [3.0, 4.0]
+    # div: (int)label saturates at INT_MAX / INT_MIN as on the GPU (an x86 cast gives INT_MIN)
+    spec2 = {"l": 1, "type": [2], "shift_val": [0.0, 0.0], "div_value": [10], "interval_map": []}
+    out2 = oracle.recover_filters(spec2, np.array([[3e9], [-3e9], [57.0]], np.float32))
+    assert out2[:, 0].tolist() == [np.float32(2147483647 // 10), np.float32(-(2147483648 // 10)), 5.0]
+
+
 def test_recover_filters_types():
     spec = {"l": 3, "type": [0, 1, 2], "shift_val": [604800.0, 0.0, 0, 0, 0, 0], "div_value": [0, 0, 10],
             "interval_map": [0.0, 9999.0, 100.0, 200.0]}

@@ -82,3 +82,25 @@ def test_noalloc_rejects_oversized_map(cuda):
     status = hg.LIB.hdg_recover_filters_noalloc(C.byref(spec), ql.data_ptr(), 4, out.data_ptr(), None)
     assert status == 1
     assert "exceeds" in hg.LIB.hdg_last_error().decode()
+
+
+def test_noalloc_out_of_table_labels_after_a_longer_map(cuda):
+    """A call whose map is shorter than the previous call's must not read the earlier
+    table's leftover entries: labels past the map (including 2^30 and 3e9, where 2 * v + 1
+    no longer fits in 32 bits) give the empty box (FLT_MAX, -FLT_MAX) from both entry points,
+    here on a non-default stream."""
+    import torch
+    import hdgrid_b200 as hg
+    rng = np.random.default_rng(9)
+    long_spec = hg.filter_spec(FILTER_A)
+    _run(hg.LIB.hdg_recover_filters_noalloc, long_spec, _labels(rng, 512, 3, 10), cuda)  # fills 20 entries
+    spec = hg.filter_spec(FILTER_B)  # 6 map entries: valid labels 1..3
+    bad = np.array([4, 5, 11, 1e6, 2.0 ** 30, 1.5e9, 3e9, 0], np.float32)
+    labels = np.stack([bad, np.full_like(bad, 1000.0)], axis=1)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        got = _run(hg.LIB.hdg_recover_filters_noalloc, spec, labels, cuda)
+        ref = _run(hg.LIB.hdg_recover_filters, spec, labels, cuda)
+    fmax = np.float32(np.finfo(np.float32).max)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert (got[:, 0] == fmax).all() and (got[:, 1] == -fmax).all(), got[:, :2]
