@@ -167,6 +167,7 @@ hdg_status hdg_set_param(hdg_index* index, const char* key, uint64_t value) {
         else if (k == "SCAN_CHUNK") f = &p.scan_chunk;
         else if (k == "QUERY_GRAPH") f = &p.query_graph;
         else if (k == "LEARNED") f = &p.learned;
+        else if (k == "PREFIX_ROWS") f = &p.prefix_rows;
         HDG_REQUIRE(f, HDG_ERR_INVALID_ARG, "not a search-time key: " + k);
         if (k == "SCAN_CHUNK")
             HDG_REQUIRE(value == 0 || (value >= 4096 && value <= 262144 && (value & (value - 1)) == 0),
@@ -370,6 +371,7 @@ hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out) {
         out->morton_valid_map = H.grid.morton_valid_map;
         out->diff_dim = H.grid.diff_dim;
         out->device_bytes = index->arena.bytes;
+        out->prefix_entries = index->host.prefix_off.empty() ? 0 : index->host.prefix_rows.size();
     });
 }
 

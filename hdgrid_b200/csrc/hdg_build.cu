@@ -11,8 +11,10 @@
 //  5. cell coords + Morton codes of every point on the GPU (get_grid_ids_kernel :28-52,
 //     encode_points_kernel zorder.cu:36-43); pool sorted by (list, Morton code, id)
 //     (thrust::sort_by_key per list, :607-611, is a stable radix sort over ids in ascending order)
-//  6. dense per-list inclusive prefix counts over the cell grid (HOPS multi_dim_scan,
-//     src/core/HOPS.cu:3-74), stored cell-major with the list index fastest.
+//  6. per-list inclusive prefix counts over the cell grid (HOPS multi_dim_scan,
+//     src/core/HOPS.cu:3-74): dense, cell-major with the list index fastest, or -- when that
+//     array would be large -- compressed into per-(grid row, list) change points along the diff
+//     dim (compress_HOPS_data, Super-Grid-IVF_PQ.cu:209-303).
 // k-means results are not pinned by any reference test (RAFT is not vendored), so the
 // build uses its own seeded Lloyd iterations.
 #include <cuda_bf16.h>
@@ -225,6 +227,56 @@ __global__ void k_count_cells(const uint64_t* __restrict__ cell, const int* __re
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     atomicAdd(&prefix[cell[r] * n_lists + list_of[r]], 1u);
+}
+
+// Counts of the lists [j0, j0 + B) over every cell: dense [cells][B], list fastest.
+__global__ void k_count_cells_range(const uint64_t* __restrict__ cell, const int* __restrict__ list_of, uint64_t n,
+                                    uint32_t j0, uint32_t B, uint32_t* __restrict__ dense) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t j = (uint32_t)list_of[r];
+    if (j >= j0 && j < j0 + B) atomicAdd(&dense[cell[r] * B + (j - j0)], 1u);
+}
+
+// Compressed prefix rows (compress_HOPS_data, Super-Grid-IVF_PQ.cu:209-303): the grid's last
+// dim of size > 1 (the diff dim, Dd cells, stride 1) runs along a row, every other dim is
+// flattened into the row index t, so cell (t, z) is flat t * Dd + z.  For every (t, list j0 + b)
+// of the dense inclusive prefix [cells][B] one thread walks z = 0..Dd-1 and keeps the points
+// where the value changes.  Without out it writes their number to cnt[t * L + j0 + b]; with out
+// it writes them as (z << 32 | value) at out + off[t * L + j0 + b].
+__global__ void k_prefix_rows(const uint32_t* __restrict__ dense, uint64_t T, uint32_t Dd, uint32_t B, uint32_t j0,
+                              uint32_t L, uint64_t* __restrict__ cnt, const uint64_t* __restrict__ off,
+                              uint64_t* __restrict__ out) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T * B) return;
+    const uint32_t b = (uint32_t)(e % B);
+    const uint64_t t = e / B, r = t * L + j0 + b;
+    const uint32_t* p = dense + t * (uint64_t)Dd * B + b;
+    uint64_t* o = out ? out + off[r] : nullptr;
+    uint32_t prev = 0;
+    uint64_t c = 0;
+    uint32_t z = 0;
+    for (; z + 4 <= Dd; z += 4) {  // four independent loads in flight
+        uint32_t v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = __ldg(p + (uint64_t)(z + u) * B);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (v[u] != prev) {
+                if (o) o[c] = ((uint64_t)(z + u) << 32) | v[u];
+                c++;
+                prev = v[u];
+            }
+    }
+    for (; z < Dd; z++) {
+        const uint32_t v = __ldg(p + (uint64_t)z * B);
+        if (v != prev) {
+            if (o) o[c] = ((uint64_t)z << 32) | v;
+            c++;
+            prev = v;
+        }
+    }
+    if (!out) cnt[r] = c;
 }
 
 // Inclusive scan along one grid dim of the cell-major [cells][lists] array.
@@ -443,6 +495,52 @@ GridMeta compute_grid_shape(const std::vector<float>& mins, const std::vector<fl
     return g;
 }
 
+// Dense prefix counts up to this size; beyond it the compressed rows.
+constexpr uint64_t kDensePrefixMax = 2ull << 30;
+
+// The compressed per-list prefix rows (the reference's compress_HOPS_data form, built per list
+// from a dense HOPS scan, Super-Grid-IVF_PQ.cu:209-303, 527-583).  Lists are taken in chunks of
+// B whose dense [cells][B] prefix fits a fixed budget: count, scan along every grid dim, then
+// one thread per (grid row, list) keeps the change points along the diff dim.  A first round
+// counts each row's change points (their exclusive sum over rows t * L + j gives the offsets),
+// a second round rebuilds each chunk and writes the (z << 32 | value) pairs.
+static void build_prefix_rows(const GridMeta& g, const uint64_t* d_cell, const int* d_list, uint64_t n, uint32_t L,
+                              HostIndex& H, cudaStream_t st) {
+    const uint32_t Dd = (uint32_t)g.grid_dims[g.diff_dim];
+    HDG_REQUIRE(g.cell_stride[g.diff_dim] == 1 && Dd >= 1 && g.tot_cells % Dd == 0, HDG_ERR_STATE,
+                "diff dim of the grid is not its last dim of size > 1");
+    const uint64_t T = g.tot_cells / Dd;
+    const uint64_t budget = 1ull << 30;
+    const uint32_t B = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(L, budget / (g.tot_cells * 4)));
+    DevMem<uint32_t> dense(g.tot_cells * B);
+    DevMem<uint64_t> cnt(T * L);
+    auto chunk = [&](uint32_t j0, uint32_t nb, const uint64_t* off, uint64_t* out) {
+        CK(cudaMemsetAsync(dense.p, 0, sizeof(uint32_t) * g.tot_cells * nb, st));
+        k_count_cells_range<<<blocks_for(n, 256), 256, 0, st>>>(d_cell, d_list, n, j0, nb, dense.p);
+        for (int a = 0; a < g.l; a++) {
+            const uint64_t lines = g.tot_cells / (uint64_t)g.grid_dims[a] * nb;
+            k_scan_axis<<<blocks_for(lines, 256), 256, 0, st>>>(dense.p, lines, g.cell_stride[a], g.grid_dims[a],
+                                                                nb);
+        }
+        k_prefix_rows<<<blocks_for(T * nb, 128), 128, 0, st>>>(dense.p, T, Dd, nb, j0, L, cnt.p, off, out);
+        CK_LAUNCH();
+    };
+    for (uint32_t j0 = 0; j0 < L; j0 += B) chunk(j0, std::min(B, L - j0), nullptr, nullptr);
+    std::vector<uint64_t> hc(T * L);
+    CK(cudaMemcpyAsync(hc.data(), cnt.p, sizeof(uint64_t) * hc.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    H.prefix_off.assign(T * L + 1, 0);
+    for (uint64_t r = 0; r < T * L; r++) H.prefix_off[r + 1] = H.prefix_off[r] + hc[r];
+    const uint64_t E = H.prefix_off.back();
+    DevMem<uint64_t> off(T * L + 1), rows(std::max<uint64_t>(E, 1));
+    CK(cudaMemcpyAsync(off.p, H.prefix_off.data(), sizeof(uint64_t) * (T * L + 1), cudaMemcpyHostToDevice, st));
+    for (uint32_t j0 = 0; j0 < L; j0 += B) chunk(j0, std::min(B, L - j0), off.p, rows.p);
+    H.prefix_rows.resize(E);
+    if (E) CK(cudaMemcpyAsync(H.prefix_rows.data(), rows.p, sizeof(uint64_t) * E, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    H.prefix.clear();
+}
+
 void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, const float* d_labels,
                  uint32_t l, cudaStream_t st) {
     const hdg_params& P = idx->params;
@@ -482,8 +580,12 @@ void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, co
         }
     H.grid = compute_grid_shape(mins, maxs, l, P.max_grids, P.label_mask);
     const GridMeta& g = H.grid;
-    HDG_REQUIRE(g.tot_cells * L * 4 <= (16ull << 30), HDG_ERR_UNSUPPORTED,
-                "prefix-count grid (cells x lists) exceeds 16 GiB; lower max_grids");
+    // per-list prefix counts: the dense cells x lists array while it stays small, else the
+    // compressed rows (PREFIX_ROWS)
+    const uint64_t dense_bytes = g.tot_cells * L * 4;
+    const bool rows_form = P.prefix_rows == 1 || (P.prefix_rows == 0 && dense_bytes > kDensePrefixMax);
+    HDG_REQUIRE(rows_form || dense_bytes <= (16ull << 30), HDG_ERR_UNSUPPORTED,
+                "dense prefix-count grid (cells x lists) exceeds 16 GiB; use PREFIX_ROWS or a lower max_grids");
 
     // ---- sample for training ---------------------------------------------------------
     std::vector<uint32_t> perm(n);
@@ -605,8 +707,12 @@ void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, co
     for (uint64_t r = 0; r < n; r++) H.zcodes[r] = hz[H.ids[r]];
 
     // ---- 6. prefix counts ------------------------------------------------------------------
-    DevMem<uint32_t> prefix(g.tot_cells * L);
-    {
+    if (rows_form) {
+        DevMem<int> dl(n);
+        CK(cudaMemcpyAsync(dl.p, hlist.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        build_prefix_rows(g, cell.p, dl.p, n, (uint32_t)L, H, st);
+    } else {
+        DevMem<uint32_t> prefix(g.tot_cells * L);
         DevMem<int> dl(n);
         CK(cudaMemcpyAsync(dl.p, hlist.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(prefix.p, 0, sizeof(uint32_t) * g.tot_cells * L, st));
@@ -620,6 +726,7 @@ void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, co
         H.prefix.resize(g.tot_cells * L);
         CK(cudaMemcpyAsync(H.prefix.data(), prefix.p, sizeof(uint32_t) * H.prefix.size(),
                            cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
     }
 
     // ---- pool-ordered codes and labels ---------------------------------------------------
@@ -668,6 +775,7 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_z = reserve(H.zcodes.size() * 8), o_id = reserve(H.ids.size() * 4);
     const size_t o_code = reserve(H.codes.size() + 64), o_lab = reserve(H.labels.size() * 4);
     const size_t o_pq = reserve(H.pq_centers.size() * 4), o_pre = reserve(H.prefix.size() * 4);
+    const size_t o_poff = reserve(H.prefix_off.size() * 8), o_prow = reserve(H.prefix_rows.size() * 8);
     idx->arena.reset();
     idx->arena.ensure(total);
     char* base = static_cast<char*>(idx->arena.ptr);
@@ -699,7 +807,14 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     }
     D.labels = (const float*)up(o_lab, H.labels.data(), H.labels.size() * 4);
     D.pq_centers = (const float*)up(o_pq, H.pq_centers.data(), H.pq_centers.size() * 4);
-    D.prefix = (const uint32_t*)up(o_pre, H.prefix.data(), H.prefix.size() * 4);
+    if (!H.prefix_off.empty()) {  // the compressed rows form
+        D.prefix = nullptr;
+        D.prefix_off = (const uint64_t*)up(o_poff, H.prefix_off.data(), H.prefix_off.size() * 8);
+        D.prefix_rows = (const uint64_t*)up(o_prow, H.prefix_rows.data(), H.prefix_rows.size() * 8);
+    } else {
+        D.prefix = (const uint32_t*)up(o_pre, H.prefix.data(), H.prefix.size() * 4);
+        D.prefix_off = D.prefix_rows = nullptr;
+    }
     k_to_bf16<<<blocks_for(H.centers.size(), 256), 256, 0, st>>>(D.centers, H.centers.size(),
                                                                 reinterpret_cast<__nv_bfloat16*>(cb));
     k_to_bf16<<<blocks_for(H.sub_centers.size(), 256), 256, 0, st>>>(

@@ -126,6 +126,7 @@ void parse_hdgrid_conf(const std::string& text, hdg_params* p) {
         {"SCAN_CHUNK", &p->scan_chunk},
         {"QUERY_GRAPH", &p->query_graph},
         {"LEARNED", &p->learned},
+        {"PREFIX_ROWS", &p->prefix_rows},
     };
     std::istringstream in(text);
     std::string line;

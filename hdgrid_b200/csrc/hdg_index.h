@@ -17,7 +17,11 @@
 //   labels       f32 [N x l]            labels in pool order (read by the fused predicate)
 //   pq_centers   f32 [M x 256 x pq_len] PQ codebooks (pq::index_data_t::centers, product-quantization.cuh:9)
 //   prefix       u32 [cells x L]        inclusive multi-dim prefix counts per list, cell-major,
-//                                       list fastest (dense form of compressed_sums, :67)
+//                                       list fastest (dense form of compressed_sums, :67), or
+//   prefix_off   u64 [T x L + 1]        the compressed form: for grid row t (every dim but the
+//   prefix_rows  u64 [E]                diff dim, T rows) and list j, the change points of the
+//                                       inclusive prefix along the diff dim, (coordinate << 32 |
+//                                       count) ascending, at [prefix_off[t*L+j], prefix_off[t*L+j+1])
 // L = C*S inverted lists; N points; M PQ subspaces; M_pad = M rounded up to 16.
 #pragma once
 #include <cuda_runtime.h>
@@ -75,7 +79,9 @@ struct IndexDev {
     const uint8_t* codes;
     const float* labels;
     const float* pq_centers;
-    const uint32_t* prefix;
+    const uint32_t* prefix;        // dense prefix counts (nullptr when the rows form is used)
+    const uint64_t* prefix_off;    // compressed rows (nullptr when dense)
+    const uint64_t* prefix_rows;
 };
 
 // Host-side copy of every index array (build output, save/load payload).
@@ -84,6 +90,7 @@ struct HostIndex {
     GridMeta grid;
     std::vector<float> centers, sub_centers, pq_centers;
     std::vector<uint32_t> cluster_off, list_off, ids, prefix;
+    std::vector<uint64_t> prefix_off, prefix_rows;  // compressed rows (prefix empty), see above
     std::vector<uint64_t> zcodes;
     std::vector<uint8_t> codes;
     std::vector<float> labels;

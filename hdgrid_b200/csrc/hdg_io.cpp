@@ -3,7 +3,7 @@
 // query run separately and lets the CPU oracle consume the exact index the GPU built.
 //
 // Layout (little-endian, fields written one by one, no struct padding):
-//   "HDGB200I" u32 version=1 u32 0
+//   "HDGB200I" u32 version=2 u32 0
 //   params   24 x u64 (order of kParamOrder below), u32 path length + bytes
 //   filter   i32 l, i32 type[8], f32 shift_val[16], i32 div_value[8], u32 n_map, f32 map[n_map]
 //   sizes    u64 n, d, l, M, M_pad, pq_len, n_lists, C
@@ -11,7 +11,8 @@
 //            u64 tot_cells, i32 morton_dims, morton_max_bits, morton_valid_map, diff_dim
 //   arrays   (u64 element count, raw elements) for: centers f32, sub_centers f32,
 //            pq_centers f32, cluster_off u32, list_off u32, ids u32, prefix u32,
-//            zcodes u64, codes u8 [n x M_pad], labels f32 [n x l]
+//            prefix_off u64, prefix_rows u64 (version 2; either the dense prefix array or the
+//            compressed rows is non-empty), zcodes u64, codes u8 [n x M_pad], labels f32 [n x l]
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -64,6 +65,14 @@ struct Reader {
         return v;
     }
     template <typename T>
+    void any(std::vector<T>& v) {  // an array of any length (bounded by the file)
+        const uint64_t n = get<uint64_t>();
+        if (n > (1ull << 40)) fail(HDG_ERR_IO, "index file " + path + ": implausible array size");
+        v.resize(n);
+        if (n) f.read(reinterpret_cast<char*>(v.data()), sizeof(T) * n);
+        if (!f) fail(HDG_ERR_IO, "truncated index file " + path);
+    }
+    template <typename T>
     void arr(std::vector<T>& v, uint64_t expect) {
         const uint64_t n = get<uint64_t>();
         if (n != expect) fail(HDG_ERR_IO, "index file " + path + ": array size mismatch");
@@ -77,7 +86,7 @@ void save_index(const hdg_index* idx, const std::string& path) {
     HDG_REQUIRE(idx->built, HDG_ERR_STATE, "index not built");
     Writer w(path);
     w.f.write(kMagic, 8);
-    w.put<uint32_t>(1);
+    w.put<uint32_t>(2);
     w.put<uint32_t>(0);
     hdg_params p = idx->params;
     for (int i = 0; i < kParams; i++) w.put<uint64_t>(*param_field(p, i));
@@ -109,6 +118,8 @@ void save_index(const hdg_index* idx, const std::string& path) {
     w.arr(H.list_off);
     w.arr(H.ids);
     w.arr(H.prefix);
+    w.arr(H.prefix_off);
+    w.arr(H.prefix_rows);
     w.arr(H.zcodes);
     w.arr(H.codes);
     w.arr(H.labels);
@@ -121,7 +132,7 @@ hdg_index* load_index(const std::string& path) {
     r.f.read(magic, 8);
     if (!r.f || std::memcmp(magic, kMagic, 8) != 0) fail(HDG_ERR_IO, path + " is not an HDGrid index file");
     const uint32_t ver = r.get<uint32_t>();
-    if (ver != 1) fail(HDG_ERR_UNSUPPORTED, "unsupported index file version " + std::to_string(ver));
+    if (ver != 1 && ver != 2) fail(HDG_ERR_UNSUPPORTED, "unsupported index file version " + std::to_string(ver));
     r.get<uint32_t>();
     std::unique_ptr<hdg_index> idx(new hdg_index());
     default_params(&idx->params);
@@ -165,7 +176,18 @@ hdg_index* load_index(const std::string& path) {
     r.arr(H.cluster_off, H.C + 1);
     r.arr(H.list_off, H.n_lists + 1);
     r.arr(H.ids, H.n);
-    r.arr(H.prefix, g.tot_cells * H.n_lists);
+    if (ver == 1) {
+        r.arr(H.prefix, g.tot_cells * H.n_lists);
+    } else {
+        r.any(H.prefix);
+        r.any(H.prefix_off);
+        r.any(H.prefix_rows);
+        const bool dense = H.prefix.size() == g.tot_cells * H.n_lists && H.prefix_off.empty();
+        const uint64_t rows = g.grid_dims[g.diff_dim] ? g.tot_cells / (uint64_t)g.grid_dims[g.diff_dim] : 0;
+        const bool packed = H.prefix.empty() && H.prefix_off.size() == rows * H.n_lists + 1 &&
+                            H.prefix_off.back() == H.prefix_rows.size();
+        if (!dense && !packed) fail(HDG_ERR_IO, "index file " + path + ": inconsistent prefix counts");
+    }
     r.arr(H.zcodes, H.n);
     r.arr(H.codes, H.n * H.M_pad);
     r.arr(H.labels, H.n * H.l);

@@ -243,14 +243,39 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
         s_sign[mask] = zero ? 0 : sign;
     }
     __syncthreads();
-    for (uint32_t j = t; j < L; j += blockDim.x) {
-        long long acc = 0;
-        for (int m = 0; m < n_corner; m++) {
-            const int sg = s_sign[m];
-            if (sg) acc += (long long)sg * (long long)D.prefix[s_corner[m] * L + j];
+    if (D.prefix) {  // dense: one coalesced row of L counts per corner
+        for (uint32_t j = t; j < L; j += blockDim.x) {
+            long long acc = 0;
+            for (int m = 0; m < n_corner; m++) {
+                const int sg = s_sign[m];
+                if (sg) acc += (long long)sg * (long long)D.prefix[s_corner[m] * L + j];
+            }
+            s_counts[j] = (uint32_t)acc;
+            w.list_counts[qi * L + j] = (uint32_t)acc;
         }
-        s_counts[j] = (uint32_t)acc;
-        w.list_counts[qi * L + j] = (uint32_t)acc;
+    } else {
+        // compressed rows (query_compressed_sum_device, Super-Grid-IVF_PQ.cu:648-691): the corner
+        // at flat cell t * Dd + z reads list j's row t, the last change point at or before z
+        const uint32_t Dd = (uint32_t)g.grid_dims[g.diff_dim];
+        for (uint32_t j = t; j < L; j += blockDim.x) {
+            long long acc = 0;
+            for (int m = 0; m < n_corner; m++) {
+                const int sg = s_sign[m];
+                if (!sg) continue;
+                const uint64_t r = (s_corner[m] / Dd) * L + j;
+                const uint32_t z = (uint32_t)(s_corner[m] % Dd);
+                const uint64_t b0 = D.prefix_off[r];
+                uint64_t lo = b0, hi = D.prefix_off[r + 1];
+                while (lo < hi) {  // first change point past z
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if ((uint32_t)(D.prefix_rows[mid] >> 32) <= z) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo > b0) acc += (long long)sg * (long long)(uint32_t)D.prefix_rows[lo - 1];
+            }
+            s_counts[j] = (uint32_t)acc;
+            w.list_counts[qi * L + j] = (uint32_t)acc;
+        }
     }
     __syncthreads();
     for (uint32_t c = t; c < D.C; c += blockDim.x) {

@@ -83,6 +83,9 @@ typedef struct hdg_params {
                              * (pointers, q, k); status of a replay via hdg_query_status */
     uint64_t learned;       /* LEARNED: 1 = per-query lists to probe and predicate-first flag
                              * from the index's trained MLP (hdg_mlp_*); 0 = plain schedule */
+    uint64_t prefix_rows;   /* PREFIX_ROWS: per-list prefix counts as compressed rows (the
+                             * reference's compress_HOPS_data form): 1 = always, 2 = never (dense
+                             * cells x lists array), 0 = rows when the dense array would pass 2 GiB */
 } hdg_params;
 
 /* filter.conf contents (config_utils.h:112-172).  interval_map is the flat
@@ -234,6 +237,7 @@ typedef struct hdg_index_info {
     uint64_t label_span[HDG_MAX_LABEL_DIMS];
     int32_t morton_dims, morton_max_bits, morton_valid_map, diff_dim;
     uint64_t device_bytes;
+    uint64_t prefix_entries;  /* change points of the compressed prefix rows; 0 = dense form */
 } hdg_index_info;
 hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out);
 

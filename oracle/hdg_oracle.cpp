@@ -290,7 +290,21 @@ struct Index {
     Grid g;
     std::vector<float> centers, sub_centers, pq_centers, labels;
     std::vector<uint32_t> cluster_off, list_off, ids, prefix;
+    // compressed prefix rows (file version 2, prefix empty): per (grid row t, list j) the change
+    // points (z << 32 | count) of the inclusive prefix along the diff dim
+    std::vector<uint64_t> prefix_off, prefix_rows;
     std::vector<uint64_t> zcodes;
+    // inclusive prefix count of list j at flat cell `flat` from either stored form
+    uint32_t prefix_at(uint64_t flat, uint64_t j) const {
+        if (prefix_off.empty()) return prefix[flat * L + j];
+        const uint64_t Dd = (uint64_t)g.dims[g.diff_dim];
+        const uint64_t r = (flat / Dd) * L + j, z = flat % Dd;
+        const uint64_t* b = prefix_rows.data() + prefix_off[r];
+        const uint64_t* e = prefix_rows.data() + prefix_off[r + 1];
+        // query_compressed_sum_device (Super-Grid-IVF_PQ.cu:648-691): the last change point <= z
+        const uint64_t* it = std::upper_bound(b, e, z, [](uint64_t key, uint64_t v) { return key < (v >> 32); });
+        return it == b ? 0u : (uint32_t)it[-1];
+    }
     std::vector<uint8_t> codes;
     uint64_t topk() const { return params[0]; }
     uint64_t filter_dim() const { return params[1]; }
@@ -550,7 +564,7 @@ void* ora_open(const char* path) {
     char magic[8];
     f.read(magic, 8);
     uint32_t ver, pad;
-    if (!f || std::memcmp(magic, "HDGB200I", 8) != 0 || !rd(f, ver) || ver != 1 || !rd(f, pad)) {
+    if (!f || std::memcmp(magic, "HDGB200I", 8) != 0 || !rd(f, ver) || (ver != 1 && ver != 2) || !rd(f, pad)) {
         g_err = "bad index file header";
         return nullptr;
     }
@@ -578,8 +592,9 @@ void* ora_open(const char* path) {
     for (int i = 0; i < kMaxDims; i++) ok = ok && rd(f, g.stride[i]);
     ok = ok && rd(f, g.tot_cells) && rd(f, g.mdims) && rd(f, g.max_bits) && rd(f, g.valid_map) && rd(f, g.diff_dim);
     ok = ok && rdv(f, ix->centers) && rdv(f, ix->sub_centers) && rdv(f, ix->pq_centers) && rdv(f, ix->cluster_off) &&
-         rdv(f, ix->list_off) && rdv(f, ix->ids) && rdv(f, ix->prefix) && rdv(f, ix->zcodes) && rdv(f, ix->codes) &&
-         rdv(f, ix->labels);
+         rdv(f, ix->list_off) && rdv(f, ix->ids) && rdv(f, ix->prefix) &&
+         (ver == 1 || (rdv(f, ix->prefix_off) && rdv(f, ix->prefix_rows))) && rdv(f, ix->zcodes) &&
+         rdv(f, ix->codes) && rdv(f, ix->labels);
     if (!ok) {
         g_err = "truncated index file";
         delete ix;
@@ -667,8 +682,10 @@ uint64_t ora_check_layout(void* h) {
                     }
                 }
     }
-    for (uint64_t e = 0; e < dense.size(); e++)
-        if (dense[e] != ix.prefix[e]) bad++;
+    // the stored counts, dense or compressed, against this dense recount at every cell and list
+    for (uint64_t c = 0; c < g.tot_cells; c++)
+        for (uint64_t j = 0; j < ix.L; j++)
+            if (dense[c * ix.L + j] != ix.prefix_at(c, j)) bad++;
     return bad;
 }
 
@@ -761,8 +778,7 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
                     flat += (uint64_t)(c < 0 ? 0 : c) * g.stride[i];
                 }
                 if (zero) continue;
-                const uint32_t* row = &ix.prefix[flat * L];
-                for (uint64_t j = 0; j < L; j++) acc[j] += sign * (long long)row[j];
+                for (uint64_t j = 0; j < L; j++) acc[j] += sign * (long long)ix.prefix_at(flat, j);
             }
             for (uint64_t j = 0; j < L; j++) lc[j] = (uint32_t)acc[j];
         } else {

@@ -276,6 +276,30 @@ def test_parity_postfilter_budget_is_not_capped(cuda):
     assert (sel > 16384).any()
 
 
+@pytest.mark.parametrize("case", ["config2", "config4", "config1"])
+def test_parity_compressed_prefix_rows(cuda, case):
+    # PREFIX_ROWS=1: the per-list prefix counts kept as compressed rows (change points along the
+    # grid's diff dim, the reference's compress_HOPS_data form); every stored count equals the
+    # oracle's dense recount (check_layout) and the per-list counts of every query equal its
+    # direct count (inside _parity)
+    if case == "config2":
+        ws = datasets.config2(scale=0.01, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                              max_grids=20_000, prefix_rows=1)
+    elif case == "config4":
+        ws = datasets.config4(scale=0.002, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                              max_grids=4096, prefix_rows=1)
+    else:
+        ws = datasets.config1(scale=0.05, n_queries=200, max_grids=100_000, prefix_rows=1)
+    idx, r = _parity(ws, cuda)
+    assert idx.info()["prefix_entries"] > 0
+    # the same index built dense gives the same results
+    ws_dense = dict(ws, hdgrid_conf=ws["hdgrid_conf"].replace("prefix_rows = 1", "prefix_rows = 2"))
+    idx2, base2, _ = build_gpu(ws_dense, cuda)
+    assert idx2.info()["prefix_entries"] == 0
+    d2, i2 = query_gpu(idx2, base2, ws_dense, ws["k"], cuda)
+    assert np.array_equal(i2, r["g_ids"]) and np.array_equal(d2.view(np.uint32), r["g_dist"].view(np.uint32))
+
+
 def test_parity_masked_label_dim(cuda):
     ws = datasets.config2(scale=0.01, n_queries=150, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
                           max_grids=20_000, label_mask=0b010)

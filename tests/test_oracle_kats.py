@@ -151,3 +151,31 @@ def test_bruteforce_respects_filter_and_order():
         order = ok[np.lexsort((ok, d))][:10]
         assert ids[i].tolist() == order.tolist()
         assert np.all(np.diff(dist[i]) >= 0)
+
+
+def test_oracle_matches_reference_stage_vectors():
+    # tests/golden/reference_stages.json: inputs of tests/golden/make_reference_stage_vectors.py
+    # with the outputs of the reference's own device functions (compiled from its sources by
+    # oracle/ref_build.py, run on a GPU); the oracle's restatements must reproduce them bit for bit
+    f = Path(__file__).parent / "golden" / "reference_stages.json"
+    if not f.exists():
+        pytest.skip("tests/golden/reference_stages.json not generated yet")
+    data = json.loads(f.read_text())
+    cs, ref = data["inputs"], data["reference"]
+    for name in ("recover_shift_map_div", "recover_ranges"):
+        c = cs[name]
+        o = oracle.recover_filters(c["spec"], np.array(c["labels"], np.float32), filter_dim=c["filter_dim"])
+        assert o.view(np.uint32).tolist() == ref[name], name
+    for g, r in zip(cs["grid_id"], ref["grid_id"]):
+        assert [oracle.grid_id(v, g["left"], g["span"], g["M"]) for v in np.array(g["x"], np.float32)] == r
+    g = cs["cell_boxes"]
+    o = oracle.cell_boxes(np.array(g["boxes"], np.float32), g["dims"], g["shuffle"], g["left"], g["span"])
+    assert o.tolist() == ref["cell_boxes"]
+    for m, r in zip(cs["morton"], ref["morton"]):
+        c = np.array(m["coords"], np.int32)
+        assert [oracle.morton_encode(row, m["dims"], m["max_bits"], m["valid_map"]) for row in c] == r
+    for z, r in zip(cs["next_z"], ref["next_z"]):
+        nx, ok = oracle.next_in_box(np.array(z["cur"], np.uint64), np.array(z["boxes"], np.int32), z["dims"],
+                                    z["max_bits"], z["valid_map"])
+        assert ok.tolist() == r["ok"]
+        assert [int(v) for v, f in zip(nx, ok) if f] == [v for v, f in zip(r["next"], r["ok"]) if f]
