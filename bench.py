@@ -78,21 +78,31 @@ def conf_values(text: str) -> dict:
     return out
 
 
-def workload(name: str, scale: float, n_queries: int = 0, with_base: bool = True):
+def parse_sets(items) -> dict:
+    """--set KEY=VALUE overrides of the workload's HDGrid.conf keys (integers)."""
+    out = {}
+    for it in items or []:
+        key, val = it.split("=", 1)
+        out[key.strip().lower()] = int(val)
+    return out
+
+
+def workload(name: str, scale: float, n_queries: int = 0, with_base: bool = True, sets=None):
     datasets = _datasets()
+    c = dict(sets or {})
     if name == "config1":
-        return datasets.config1(scale=scale, n_queries=n_queries or 1000, break_down=1)
+        return datasets.config1(scale=scale, n_queries=n_queries or 1000, break_down=1, **c)
     if name == "config2":
         nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
-        return datasets.config2(scale=scale, n_queries=nq, break_down=1)
+        return datasets.config2(scale=scale, n_queries=nq, break_down=1, **c)
     if name == "config3":
         nq = n_queries or max(1000, int(10_000 * min(1.0, scale * 4)))
-        return datasets.config3(scale=scale, n_queries=nq, break_down=1)
+        return datasets.config3(scale=scale, n_queries=nq, break_down=1, **c)
     if name == "config4":
         return datasets.config4(scale=scale, n_queries=n_queries or max(2000, int(100_000 * scale)), break_down=1,
-                                with_base=with_base)
+                                with_base=with_base, **c)
     if name == "config5":
-        return datasets.config5(scale=scale, n_queries=n_queries or 10_000, break_down=1, with_base=with_base)
+        return datasets.config5(scale=scale, n_queries=n_queries or 10_000, break_down=1, with_base=with_base, **c)
     raise SystemExit(f"unknown config {name}")
 
 
@@ -204,7 +214,7 @@ def build_index_only(args):
     """Child process of the reference arm: builds the workload's index on the GPU and saves it."""
     import torch
     import hdgrid_b200 as hg
-    ws = workload(args.config, args.scale, args.queries)
+    ws = workload(args.config, args.scale, args.queries, sets=parse_sets(args.set))
     idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
     base = torch.from_numpy(ws["base"]).cuda()
     labels = torch.from_numpy(ws["labels"]).cuda()
@@ -222,9 +232,9 @@ def run_reference(args):
     d = tempfile.mkdtemp(prefix="hdg_ref_")
     path = os.path.join(d, "index.hdg")
     cmd = [sys.executable, str(Path(__file__).resolve()), "--build-index-only", path, "--config", args.config,
-           "--scale", str(args.scale), "--queries", str(args.queries)]
+           "--scale", str(args.scale), "--queries", str(args.queries)] + [x for it in args.set for x in ("--set", it)]
     subprocess.run(cmd, check=True, env=dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("LOCAL_RANK", "0")))
-    ws = workload(args.config, args.scale, args.queries)
+    ws = workload(args.config, args.scale, args.queries, sets=parse_sets(args.set))
     ora = oracle.OracleIndex(path)
     n_sample = min(args.ref_sample, ws["queries"].shape[0])
     cores = os.cpu_count() or 1
@@ -318,7 +328,7 @@ def run_hdgrid(args):
     rank, world, local = dist_setup(args)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    ws = workload(args.config, args.scale, args.queries)
+    ws = workload(args.config, args.scale, args.queries, sets=parse_sets(args.set))
     k = ws["k"]
     idx = hg.SuperGridIndex.from_text(ws["hdgrid_conf"], ws["filter_conf"])
     base = torch.from_numpy(ws["base"]).to(dev)
@@ -449,7 +459,11 @@ def run_hdgrid(args):
         plain = []
         idx.set_param("query_graph", 0)
         idx.set_param("learned", 0)
-        for sched, e0v in (("post-filter", int(p0["exps0"])), ("pre-filter", 1)):
+        # post-filter at the index's exps0 and a quarter / four times it (the refine ratio trades
+        # recall for re-rank work), pre-filter once
+        e0 = int(p0["exps0"])
+        for sched, e0v in (("post-filter", max(2, e0 // 4)), ("post-filter", e0), ("post-filter", 4 * e0),
+                           ("pre-filter", 1)):
             idx.set_param("exps0", e0v)
             for p in PLAIN_PROBES:
                 idx.set_param("sub_lists", p)
@@ -518,6 +532,8 @@ def main():
     ap.add_argument("--config", default="config5")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--queries", type=int, default=0, help="query batch size (0 = the workload's own)")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="override an HDGrid.conf key of the workload (integer), e.g. max_grids=30000000")
     ap.add_argument("--cpu-sample", type=int, default=100)
     ap.add_argument("--ref-sample", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")

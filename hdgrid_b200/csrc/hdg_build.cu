@@ -836,6 +836,7 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     for (uint64_t c = 0; c < H.C; c++)
         D.S_max = std::max<uint32_t>(D.S_max, H.cluster_off[c + 1] - H.cluster_off[c]);
     idx->grid = H.grid;
+    morton_dim_masks(idx->grid);
     CK(cudaStreamSynchronize(st));
     CK_LAUNCH();
     idx->built = true;

@@ -7,8 +7,8 @@
 //   - cell box: get_filter_grid_ranges_kernel (Super-Grid-IVF_PQ.cu:930-961)
 //   - Morton: morton_encode (src/core/zorder.cu:3-15)
 // A C-style float->uint64 cast on the GPU is cvt.rzi.u64.f32, which saturates
-// (NaN and negatives -> 0, >= 2^64 -> UINT64_MAX); the kernels rely on that, exactly as
-// the reference does.
+// (negatives -> 0, >= 2^64 -> UINT64_MAX, NaN -> 2^63); the kernels use the same cast as the
+// reference, so they agree with it on every input.
 #pragma once
 #include <cfloat>
 #include <climits>

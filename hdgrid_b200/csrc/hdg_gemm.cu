@@ -13,9 +13,11 @@
 // reads the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows of the
 // tile) and writes S.  Every wait is bounded: on expiry the kernel records an error in *err,
 // lets its own copies land and stops instead of hanging.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "hdg_internal.h"
 
@@ -185,6 +187,173 @@ __global__ void __launch_bounds__(kGemmThreads) k_umma_dot(const __nv_bfloat16* 
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GN));
 }
 
+// ---- TMA-fed variant ----------------------------------------------------------------
+// The same product with the operands brought in by the Tensor Memory Accelerator: K chunks of
+// 64 bf16 (128 bytes) per row land in shared memory through cp.async.bulk.tensor (no
+// multicast: the tensor maps cover this GPU's buffers only) with the 128-byte swizzle that
+// the UMMA K-major SW128 descriptor reads (8-row groups 1024 bytes apart; a K step of 16
+// elements advances the start address by 32 bytes inside the swizzle atom).  A ring of
+// kTStages stages has a full barrier (TMA transaction bytes) and an empty barrier
+// (tcgen05.commit after the stage's MMAs) each; one thread issues the loads and the MMAs.
+// BN = 64 or 128 output columns per CTA (64 when 128-wide tiles would leave SMs idle).
+constexpr int kTStages = 4;
+constexpr uint32_t kTileA = GM * GK * 2;  // 16 KB per stage
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);
+    d |= (uint64_t)1 << 16;                   // leading byte offset (unused by K-major SW128)
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset: 8 rows x 128 bytes
+    d |= (uint64_t)1 << 46;                   // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads) k_umma_tma(const __grid_constant__ CUtensorMap mapA, uint64_t rows,
+                                                           const __grid_constant__ CUtensorMap mapB, uint64_t cols,
+                                                           int d, float* __restrict__ out, uint64_t ldo,
+                                                           int* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];  // kTStages x (A tile, B tile), 1024-aligned inside
+    __shared__ __align__(8) uint64_t s_full[kTStages], s_empty[kTStages], s_done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    constexpr uint32_t kTileB = BN * GK * 2;
+    constexpr uint32_t kIdescT = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                 ((uint32_t)(GM >> 4) << 24);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int r0 = (int)(blockIdx.x * GM), c0 = (int)(blockIdx.y * BN);
+    const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const int nchunks = (d + GK - 1) / GK;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        s_fail = 0;
+        for (int i = 0; i < kTStages; i++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[i])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_empty[i])), "r"(1));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_done)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = s_tmem;
+    if (t == 0) {
+        int issued = 0;  // chunks whose loads were issued
+        auto issue = [&](int kc) {
+            const int st = kc % kTStages;
+            const uint32_t sa = sbase + (uint32_t)st * (kTileA + kTileB), sb = sa + kTileA;
+            const uint32_t fb = smem_u32(&s_full[st]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(kTileA + kTileB)
+                         : "memory");
+            tma_load_2d(sa, &mapA, kc * GK, r0, fb);
+            tma_load_2d(sb, &mapB, kc * GK, c0, fb);
+            issued = kc + 1;
+        };
+        for (int kc = 0; kc < nchunks && kc < kTStages; kc++) issue(kc);
+        bool ok = true;
+        int committed = 0;  // chunks whose MMAs were committed
+        for (int kc = 0; kc < nchunks && ok; kc++) {
+            const int st = kc % kTStages;
+            const uint32_t ph = (uint32_t)(kc / kTStages) & 1u;
+            if (!mbar_wait(smem_u32(&s_full[st]), ph)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t sa = sbase + (uint32_t)st * (kTileA + kTileB), sb = sa + kTileA;
+#pragma unroll
+            for (int ks = 0; ks < GK / 16; ks++) {
+                const uint64_t da = umma_desc_sw128(sa + ks * 32);
+                const uint64_t db = umma_desc_sw128(sb + ks * 32);
+                const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kIdescT), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&s_empty[st]))
+                         : "memory");
+            committed = kc + 1;
+            if (kc + kTStages < nchunks) {  // refill this stage once its MMAs have read it
+                if (!mbar_wait(smem_u32(&s_empty[st]), ph)) {
+                    ok = false;
+                    break;
+                }
+                issue(kc + kTStages);
+            }
+        }
+        if (ok) {
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&s_done))
+                         : "memory");
+        } else {
+            // a wait expired: record it, then let the loads and MMAs already issued finish
+            // (bounded waits) before the shared memory and TMEM are given back
+            s_fail = 1;
+            for (int kc = committed; kc < issued; kc++)
+                mbar_wait(smem_u32(&s_full[kc % kTStages]), (uint32_t)(kc / kTStages) & 1u);
+            if (committed > 0) {
+                const int kc = committed - 1;
+                mbar_wait(smem_u32(&s_empty[kc % kTStages]), (uint32_t)(kc / kTStages) & 1u);
+            }
+        }
+    }
+    __syncthreads();
+    bool ok = s_fail == 0;
+    if (ok && !mbar_wait(smem_u32(&s_done), 0)) ok = false;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok) {
+        const uint64_t row = (uint64_t)r0 + warp * 32 + lane;
+        const bool vec = (ldo % 4 == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+        for (int cb = 0; cb < BN; cb += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cb;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row >= rows) continue;
+            const uint64_t col = (uint64_t)c0 + cb;
+            float* o = out + row * ldo + col;
+            if (vec && col + 16 <= cols) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(o + j) = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                                     __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    if (col + j < cols) o[j] = __uint_as_float(v[j]);
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
 __global__ void k_f32_to_bf16_rows(const float* __restrict__ x, uint64_t n, __nv_bfloat16* __restrict__ y,
                                    float* __restrict__ norms, int d) {
     const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
@@ -202,9 +371,78 @@ __global__ void k_f32_to_bf16_rows(const float* __restrict__ x, uint64_t n, __nv
 
 size_t umma_smem_bytes() { return 4 * kStage; }
 
-// S [rows x cols] (row stride ldo) = A . B^T in BF16 with FP32 accumulation.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    HDG_REQUIRE(fn != nullptr, HDG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    return fn;
+}
+
+// Tensor map of a row-major bf16 [n x d] matrix read in boxes of 64 (K) x box_rows, 128-byte
+// swizzle, zero fill past the edges.
+static CUtensorMap bf16_rows_map(const void* base, uint64_t n, int d, uint32_t box_rows) {
+    HDG_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0 && d % 8 == 0, HDG_ERR_UNSUPPORTED,
+                "TMA operands need 16-byte aligned rows");
+    CUtensorMap m;
+    const cuuint64_t gdim[2] = {(cuuint64_t)d, (cuuint64_t)n};
+    const cuuint64_t gstride[1] = {(cuuint64_t)d * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)GK, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), gdim, gstride,
+                                      box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    HDG_REQUIRE(r == CUDA_SUCCESS, HDG_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return m;
+}
+
+// S [rows x cols] (row stride ldo) = A . B^T in BF16 with FP32 accumulation, TMA-fed.
+void umma_dot_tma(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
+                  uint64_t ldo, int* err, cudaStream_t st, int sm_count) {
+    HDG_REQUIRE(d % 8 == 0, HDG_ERR_UNSUPPORTED, "tensor-core coarse GEMM needs d % 8 == 0");
+    HDG_REQUIRE(rows < (1ull << 31) && cols < (1ull << 31), HDG_ERR_UNSUPPORTED, "GEMM operand too large");
+    if (!rows || !cols) return;
+    const uint64_t row_tiles = (rows + GM - 1) / GM;
+    // 128-wide column tiles unless they would leave SMs without two CTAs each
+    const bool narrow = row_tiles * ((cols + 127) / 128) < (uint64_t)(2 * sm_count);
+    const CUtensorMap ma = bf16_rows_map(A_bf16, rows, d, GM);
+    auto launch = [&](auto kern, uint32_t bn) {
+        const CUtensorMap mb = bf16_rows_map(B_bf16, cols, d, bn);
+        const int sm = (int)(kTStages * (kTileA + bn * GK * 2) + 1024);
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        dim3 grid((unsigned)row_tiles, (unsigned)((cols + bn - 1) / bn));
+        kern<<<grid, kGemmThreads, sm, st>>>(ma, rows, mb, cols, d, out, ldo, err);
+    };
+    if (narrow) launch(k_umma_tma<64>, 64);
+    else launch(k_umma_tma<128>, 128);
+    CK_LAUNCH();
+}
+
+// S [rows x cols] (row stride ldo) = A . B^T in BF16 with FP32 accumulation (the TMA-fed kernel).
 void umma_dot(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
               uint64_t ldo, int* err, cudaStream_t st) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    umma_dot_tma(A_bf16, rows, B_bf16, cols, d, out, ldo, err, st, sms);
+}
+
+// The cp.async-fed kernel above, kept beside the TMA one for comparison runs.
+void umma_dot_cp_async(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
+                       uint64_t ldo, int* err, cudaStream_t st) {
     HDG_REQUIRE(d % 8 == 0, HDG_ERR_UNSUPPORTED, "tensor-core coarse GEMM needs d % 8 == 0");
     if (!rows || !cols) return;
     const int sm = (int)umma_smem_bytes();

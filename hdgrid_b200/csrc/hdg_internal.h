@@ -94,6 +94,10 @@ void recover_filters_noalloc(const FilterDev& f, const float* host_map, const fl
 // tcgen05 BF16 GEMM (hdg_gemm.cu)
 void umma_dot(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
               uint64_t ldo, int* err, cudaStream_t st);
+void umma_dot_tma(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
+                  uint64_t ldo, int* err, cudaStream_t st, int sm_count);
+void umma_dot_cp_async(const void* A_bf16, uint64_t rows, const void* B_bf16, uint64_t cols, int d, float* out,
+                       uint64_t ldo, int* err, cudaStream_t st);
 void rows_to_bf16(const float* x, uint64_t n, int d, void* y, float* norms, cudaStream_t st);
 void merge_topk(const float* dist, const uint64_t* ids, uint64_t q, uint32_t k, uint32_t nb, const uint64_t* offsets,
                 float* out_dist, uint64_t* out_ids, cudaStream_t st);

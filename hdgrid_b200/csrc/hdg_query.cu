@@ -101,14 +101,16 @@ __device__ __forceinline__ int q_sched(const Workspace& w, uint64_t qi) { return
 __device__ __forceinline__ bool q_prefilter(const Workspace& w, uint64_t qi) {
     return w.mode == kPre || q_sched(w, qi) == 1;
 }
-// Candidate budget n_cand of query qi given the batch's beta and max_row_len: k for the
-// reference pre-filter schedule (exps0 <= 1), exps0 * k for the single-dim schedule and the
+// Candidate budget n_cand of query qi given the batch's beta and max_row_len: the query's k for
+// the reference pre-filter schedule (exps0 <= 1), exps0 * k for the single-dim schedule and the
 // predicate-first schedule, and the reference's min(exps0 * k * beta, max_row_len) for the
-// post-filter schedule (Super-Grid-IVF_PQ.cu:1219-1222), with no further cap.  k_batch
-// evaluates it once per query into w.qbud.
+// post-filter schedule (Super-Grid-IVF_PQ.cu:1219-1222), with no further cap.  Here k is the
+// call's k (the width of the output rows): the reference has one topk per batch, so a batch
+// whose queries ask for different k runs as a batch of the largest k whose rows are cut to
+// each query's k.  k_batch evaluates it once per query into w.qbud.
 __device__ __forceinline__ uint64_t budget_of(const Workspace& w, uint64_t qi, float beta, uint64_t max_row) {
-    const uint32_t k = q_k(w, qi);
-    if (w.mode == kPre) return k;
+    if (w.mode == kPre) return q_k(w, qi);
+    const uint32_t k = w.k_max;
     uint64_t K;
     if (w.mode == kL1 || q_sched(w, qi) == 1) {
         K = (uint64_t)w.exps0 * k;
@@ -926,13 +928,39 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
     block_exclusive_scan(s_pre, Ps + 1, s_warp);
 }
 
+// The cell box of a query in the Morton domain (one entry per valid dim, shuffled order):
+// mask of the dim's bits, the low cell's masked code and the high cell's masked code, the
+// latter ~0 when the high side cannot reject exactly.  A candidate's cell below the low
+// cell means its label is below the box's low bound: the low cell comes from
+// max(trunc(lo), left), which is at most lo (or at most every label), and cell ids grow with
+// the label (get_grid_id_device, Super-Grid-IVF_PQ.cu:24-26).  Above the high cell only
+// proves the label exceeds r = (float)min(trunc(hi), left + span), the value the cell box was
+// computed from (:947-960); that rejects exactly when r >= hi.
+__device__ void morton_box_bounds(const GridMeta& g, uint64_t zlo, uint64_t zhi, const float* box, uint64_t* zm,
+                                  uint64_t* lo, uint64_t* hi, int* n) {
+    int k = 0;
+    for (int i = 0; i < g.l; i++) {
+        const uint64_t m = g.zmask[i];
+        if (!m) continue;
+        const float bh = box[2 * g.shuffle[i] + 1];
+        const uint64_t bhi = (uint64_t)bh;  // saturating, as in cell_range
+        const uint64_t rr = g.left[i] + g.span[i];
+        const float r = (float)(bhi < rr ? bhi : rr);
+        zm[k] = m;
+        lo[k] = zlo & m;
+        hi[k] = (r >= bh) ? (zhi & m) : ~0ull;
+        k++;
+    }
+    *n = k;
+}
+
 // Fast path (M a multiple of 32).  The CTA computes the query's LUT straight into shared
 // memory when it switches query (codeword-major loads, one subspace per lane), then streams
 // candidates; CPT candidates per thread are interleaved step by step so every thread keeps
 // CPT independent load->add chains in flight.
 template <int G, int NT, int CPT>
 __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast(IndexDev D, const float* __restrict__ queries, int Ps,
-                                                     int pre, int lbl, uint64_t q, Workspace w) {
+                                                     int pre, int lbl, uint64_t q, Workspace w, GridMeta g) {
     extern __shared__ __align__(16) float s_lut[];  // [G][256][64]
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 64);  // [Ps + 1]
     uint32_t* s_start = s_pre + Ps + 1;                                       // [Ps]
@@ -941,6 +969,10 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
     __shared__ ScanShared s;
     __shared__ uint32_t s_warp[32];
     __shared__ float s_box[2 * kMaxDims];
+    // the query's cell box in the Morton domain, one entry per valid dim: a candidate whose
+    // masked code lies below s_zlo or above s_zhi cannot pass the label predicate
+    __shared__ uint64_t s_zm[kMaxDims], s_zlo[kMaxDims], s_zhi[kMaxDims];
+    __shared__ int s_zn;
     const int t = threadIdx.x, lane = t & 31;
     const uint32_t R = lane >> 2, sh = 8u * (lane & 3), lane4 = 4u * lane;
     const uint32_t n_items = w.item_off[q];
@@ -996,7 +1028,10 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                 }
             }
             if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
-            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
+            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);  // ends with a barrier
+            if (t == 0) morton_box_bounds(g, w.zrange[(uint64_t)qq * 2], w.zrange[(uint64_t)qq * 2 + 1], s_box,
+                                          s_zm, s_zlo, s_zhi, &s_zn);
+            __syncthreads();
             cur = qq;
         }
         const uint32_t e1 = min(total, e0 + w.chunk);
@@ -1090,6 +1125,21 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                             while (s_pre[rr + 1] <= pe[j]) rr++;
                             pp[j] = s_start[rr] + (pe[j] - s_pre[rr]);
                         }
+                    }
+                    // the Morton code first (8 bytes): a candidate whose cell lies outside the
+                    // cell box on a side where that proves the label test fails is rejected
+                    // without reading its labels
+                    {
+                        uint64_t zc[kPreStep];
+#pragma unroll
+                        for (int j = 0; j < kPreStep; j++) zc[j] = pv[j] ? __ldg(D.zcodes + pp[j]) : 0ull;
+                        const int zn = s_zn;
+#pragma unroll
+                        for (int j = 0; j < kPreStep; j++)
+                            for (int i = 0; i < zn; i++) {
+                                const uint64_t c = zc[j] & s_zm[i];
+                                if (c < s_zlo[i] || c > s_zhi[i]) pv[j] = false;
+                            }
                     }
                     if (lab4) {
                         float4 v[kPreStep];
@@ -2368,7 +2418,7 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
-                kern<<<blocks, nt, sm, st>>>(D, c.queries, R, pre, l, q, w);
+                kern<<<blocks, nt, sm, st>>>(D, c.queries, R, pre, l, q, w, idx->grid);
             };
             if (G == 1) {
                 if (cpt == 1) launch(k_scan_fast<1, 512, 1>, 512);

@@ -147,11 +147,14 @@ hdg_status hdg_query(hdg_index* index, const float* d_queries, uint64_t q,
  * the uniform value).  No reference counterpart: super_grid::index::query
  * (Super-Grid-IVF_PQ.cu:985-1249) takes one k and one probe count for the whole batch.
  *   d_k        result count of each query, clamped to [1, k_max]; rows keep stride k_max and
- *              the slots past a query's k hold id UINT64_MAX and distance +inf;
+ *              the slots past a query's k hold id UINT64_MAX and distance +inf.  The candidate
+ *              budgets are those of a k_max batch (the reference has one topk per batch, so a
+ *              mixed-k batch is a k_max batch whose rows are cut to each query's k);
  *   d_nprobe   sub-lists probed per query, clamped to [1, sub_lists];
  *   d_schedule 0 = the index's schedule (Super-Grid-IVF_PQ.cu:1151-1241), 1 = predicate-first
- *              scan (label test fused into the ADC pass) with a budget of exps0*k and an exact
- *              re-rank; needs exps0 > 1. */
+ *              scan (label test fused into the ADC pass) with a budget of exps0*k_max and an
+ *              exact re-rank -- the schedule of the reference's batch-split branch
+ *              (:1165-1171); needs exps0 > 1. */
 hdg_status hdg_query_ex(hdg_index* index, const float* d_queries, uint64_t q,
                         const float* d_query_labels, uint32_t label_cols, const float* d_data,
                         uint32_t k_max, const uint32_t* d_k, const uint32_t* d_nprobe,

@@ -37,10 +37,13 @@ constexpr int kMaxDims = 8;
 constexpr int kCodes = 256;
 
 // ---- CUDA conversion semantics emulated on the host ------------------------------------
-// A float->uint64 C cast on the GPU (cvt.rzi.u64.f32) saturates: NaN and values below 0
-// give 0, values >= 2^64 give UINT64_MAX.  x86 casts differ, so the oracle spells it out.
+// A float->uint64 C cast on the GPU (cvt.rzi.u64.f32) saturates: values below 0 give 0,
+// values >= 2^64 give UINT64_MAX, and NaN gives 2^63 (measured on B200 through the
+// reference's own get_grid_id_device, tests/golden/reference_stages.json).  x86 casts differ,
+// so the oracle spells it out.
 uint64_t sat_f2u64(float x) {
-    if (std::isnan(x) || x <= 0.0f) return 0;
+    if (std::isnan(x)) return 1ull << 63;
+    if (x <= 0.0f) return 0;
     if (x >= 18446744073709551616.0f) return ~0ull;
     return (uint64_t)x;
 }
@@ -906,11 +909,13 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
     } else if (mode == 2) {
         K = exps0 * k;
     }
-    // the same budget for a query's own k and schedule
-    auto budget = [&](uint32_t kq, bool sched1) -> uint64_t {
-        if (mode == 2 || sched1) return exps0 * (uint64_t)kq;
+    // the same budget for a query's schedule; the batch's k, not the query's own: the reference
+    // has one topk per batch, so a mixed-k batch runs as a batch of the call's k whose rows are
+    // cut to each query's k
+    auto budget = [&](bool sched1) -> uint64_t {
+        if (mode == 2 || sched1) return exps0 * (uint64_t)k;
         if (real == 0) return max_row;
-        const float want = (float)(exps0 * (uint64_t)kq) * (float)beta;
+        const float want = (float)(exps0 * (uint64_t)k) * (float)beta;
         return std::min<uint64_t>(want >= 1.8e19f ? ~0ull : (uint64_t)want, max_row);
     };
     if (tr && tr->scalars) {
@@ -989,7 +994,7 @@ int ora_query_ex(void* h, const float* queries, uint64_t q, const float* qlabels
             }
             continue;
         }
-        const uint64_t Kq = (qk || qsched) ? budget(kq, sched1) : K;
+        const uint64_t Kq = qsched ? budget(sched1) : K;
         if (cand.size() > Kq) {
             std::nth_element(cand.begin(), cand.begin() + Kq, cand.end());
             cand.resize(Kq);

@@ -41,7 +41,8 @@ def cases(seed: int = 2024) -> dict:
     ts = rng.integers(0, 30_000_000, size=n).astype(np.float32)
     mp = rng.integers(1, 11, size=n).astype(np.float32)  # label - 1 inside the 10-row table
     dv = rng.integers(-200_000, 2_000_000, size=n).astype(np.float32)
-    dv[:6] = [3e9, -3e9, 2147483520.0, -2147483648.0, 0.0, 9.0]  # saturating casts, zero, below the divisor
+    dv[:7] = [3e9, -3e9, 2147483520.0, -2147483648.0, 0.0, 9.0, np.nan]  # saturating casts, zero, below the
+    # divisor, NaN (the map dim keeps in-table labels: the reference indexes its table with them)
     out["recover_shift_map_div"] = {
         "spec": {"l": 3, "type": [0, 1, 2], "shift_val": [604800.0, 0.0, 0.0, 0.0, 0.0, 0.0], "div_value": [0, 0, 10],
                  "interval_map": table},
@@ -70,6 +71,7 @@ def cases(seed: int = 2024) -> dict:
     b[:10, 1] = FMAX
     b[10:20, 4] = -5.0
     b[20:30, 2:4] = b[20:30, 3:1:-1]  # lo above hi: an empty box
+    b[30:34, 5] = np.nan  # NaN high bound (the cast gives 2^63, clamped to the grid's end)
     out["cell_boxes"] = dict(grid, boxes=b.tolist())
     # Morton codes
     mort = []
