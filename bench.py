@@ -298,13 +298,20 @@ def max_relative_error(ws, dist, ids, n_sample):
     return worst
 
 
-def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int) -> float:
+def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int, zin_q=None) -> float:
     """Bytes the ADC scan of one batch must read: M code bytes per candidate of a post-filter
     query; for a predicate-first query 4*l label bytes per candidate plus M code bytes per
-    candidate that passes the predicate (the others need no ADC)."""
+    candidate that passes the predicate (the others need no ADC).  With zin_q (the compacting
+    scan, which reads each candidate's 8-byte Morton code and the labels only of the zin_q
+    candidates whose cell lies in the query's cell box), a predicate-first query reads
+    8 * candidates + 4*l * zin + M * passing."""
     cand_q = np.asarray(cand_q, np.float64)
     pass_q = np.asarray(pass_q, np.float64)
-    return float(np.where(np.asarray(pre_q, bool), cand_q * (4 * l) + pass_q * M, cand_q * M).sum())
+    if zin_q is None:
+        pre_bytes = cand_q * (4 * l) + pass_q * M
+    else:
+        pre_bytes = cand_q * 8 + np.asarray(zin_q, np.float64) * (4 * l) + pass_q * M
+    return float(np.where(np.asarray(pre_q, bool), pre_bytes, cand_q * M).sum())
 
 
 def scan_traffic(ws, candidates):
@@ -423,7 +430,11 @@ def run_hdgrid(args):
     if learned:
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
     pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
-    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"])
+    # the compacting scan (one 32-subspace group, one candidate per thread) pre-checks Morton codes
+    compacting = (info["M"] + 31) // 32 == 1 and int(idx.params["scan_cpt"]) in (0, 1)
+    zin_q = (np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq].astype(np.uint64)
+             if compacting else None)
+    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"], zin_q)
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
 

@@ -55,6 +55,7 @@ struct Workspace {
     uint32_t* item_off;      // [q + 1] work-item offsets
     uint32_t* mm;            // [q x 2] min / max finite distance key
     uint32_t* nfin;          // [q] finite distances (predicate passed)
+    uint32_t* zin;           // [q] candidates of the compacting scan inside the cell box by their Morton code
     uint32_t* counter;       // [4] work counter
     float* lut;              // [q x G x 256 x 32] f32, or __half when lut16
     int lut16;               // LUT stored in FP16 (LUT_FP16=1); the scan sums in FP32
@@ -387,6 +388,19 @@ __device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32
     __syncthreads();
 }
 
+// Sorts keys[0, n) (n a power of two) of which at most nvalid are not ~0: when a shorter sort
+// suffices, the valid keys are first compacted to the front (stably, the rest set to ~0) and
+// only next_pow2(nvalid) of them are sorted -- the same result as sorting all n.  All threads.
+__device__ __forceinline__ void block_sort_valid(uint64_t* keys, int n, int nvalid, uint32_t* s_wc) {
+    const int n2 = (int)next_pow2_dev((uint32_t)max(nvalid, 2));
+    if (n2 < n) {
+        block_compact_keys(keys, n, s_wc);
+        block_bitonic_sort(keys, n2);
+    } else {
+        block_bitonic_sort(keys, n);
+    }
+}
+
 // One sub-range of a probed list's Morton interval [lo, hi) when is_split = 1.
 // get_query_end_points_kernel (zorder.cu:596-654) cuts the interval into
 // min(len, n_split) near-equal parts; zorder_range_query_kernel (:474-594) then moves each
@@ -480,7 +494,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
             s_keys[c] = key;
         }
         __syncthreads();
-        block_bitonic_sort(s_keys, sort_n1);
+        block_sort_valid(s_keys, sort_n1, s_nvalid, s_wc);
         if (t == 0) s_bound = key_float((uint32_t)(s_keys[Pc - 1] >> 32));
         __syncthreads();
     }
@@ -503,7 +517,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     __syncthreads();
     // with every non-empty cluster taken the keys hold no distance: cluster order, compacted
     if (all_c) block_compact_keys(s_keys, sort_n1, s_wc);
-    else block_bitonic_sort(s_keys, sort_n1);
+    else block_sort_valid(s_keys, sort_n1, s_nvalid, s_wc);
     const int npc = min(Pc, s_nvalid);
     for (int i = t; i < Pc; i += blockDim.x) {
         const uint32_t c = i < npc ? (uint32_t)s_keys[i] : kInvalid;
@@ -540,7 +554,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
             s_keys[e] = key;
         }
         __syncthreads();
-        block_bitonic_sort(s_keys, sort_n2);
+        block_sort_valid(s_keys, sort_n2, s_nvalid, s_wc);
         if (t == 0) s_bound = key_float((uint32_t)(s_keys[Psq - 1] >> 32));
         __syncthreads();
     }
@@ -570,7 +584,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     // every list taken and every cluster taken (chosen clusters in cluster order): the keys are
     // already in list-id order and only need compacting; otherwise the sort orders them
     if (all_l && all_c) block_compact_keys(s_keys, sort_n2, s_wc);
-    else block_bitonic_sort(s_keys, sort_n2);
+    else block_sort_valid(s_keys, sort_n2, s_nvalid, s_wc);
     const int nps = min(Psq, s_nvalid);
     // the probed lists in list-id (= pool) order, so candidate positions follow pool order
     // (with every list taken the keys carry no distance and are in list-id order already)
@@ -718,6 +732,7 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         w.mm[2 * i] = 0xffffffffu;
         w.mm[2 * i + 1] = 0u;
         w.nfin[i] = 0;
+        w.zin[i] = 0;
         w.cand_count[i] = 0;
     }
     if (e == q && b < e) {
@@ -1037,7 +1052,7 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
         const uint32_t e1 = min(total, e0 + w.chunk);
         float* dst = w.dist + w.qoff[qq];
         const bool preq = pre || q_prefilter(w, qq);
-        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
+        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0, zi = 0;
         // each warp takes a contiguous span of the item (a multiple of 32 * CPT positions,
         // so position mod 32 stays the lane), so a lane's walk to its candidate's range
         // crosses few range boundaries per step
@@ -1135,11 +1150,13 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                         for (int j = 0; j < kPreStep; j++) zc[j] = pv[j] ? __ldg(D.zcodes + pp[j]) : 0ull;
                         const int zn = s_zn;
 #pragma unroll
-                        for (int j = 0; j < kPreStep; j++)
+                        for (int j = 0; j < kPreStep; j++) {
                             for (int i = 0; i < zn; i++) {
                                 const uint64_t c = zc[j] & s_zm[i];
                                 if (c < s_zlo[i] || c > s_zhi[i]) pv[j] = false;
                             }
+                            zi += pv[j] ? 1u : 0u;
+                        }
                     }
                     if (lab4) {
                         float4 v[kPreStep];
@@ -1252,12 +1269,14 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
             kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
             kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
             nf += __shfl_xor_sync(0xffffffffu, nf, o);
+            zi += __shfl_xor_sync(0xffffffffu, zi, o);
         }
         if (lane == 0 && nf) {
             atomicMin(&w.mm[2 * qq], kmin);
             atomicMax(&w.mm[2 * qq + 1], kmax);
             atomicAdd(&w.nfin[qq], nf);
         }
+        if (lane == 0 && zi) atomicAdd(&w.zin[qq], zi);
         __syncthreads();
     }
 }
@@ -1723,9 +1742,10 @@ __device__ __forceinline__ void topk_rounds(uint64_t* s_keys, int cap, int kq, i
         const int c = *s_cnt;
         __syncthreads();
         if (r1 < n && c > kq) {
-            for (int i = c + threadIdx.x; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+            const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
+            for (int i = c + threadIdx.x; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
             __syncthreads();
-            block_bitonic_sort(s_keys, cap);
+            block_bitonic_sort(s_keys, n2);
             if (threadIdx.x == 0) {
                 *s_cnt = kq;
                 *s_th = s_keys[kq - 1];
@@ -1890,9 +1910,10 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
             const int c = s_cnt;
             __syncthreads();
             if (r1 < ns && c > kq) {  // more rows follow: keep the kq best
-                for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+                const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
+                for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
                 __syncthreads();
-                block_bitonic_sort(s_keys, cap);
+                block_bitonic_sort(s_keys, n2);
                 if (t == 0) {
                     s_cnt = kq;
                     s_th = s_keys[kq - 1];
@@ -1902,9 +1923,12 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
         }
         int c = s_cnt;
         __syncthreads();
-        for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
-        __syncthreads();
-        block_bitonic_sort(s_keys, cap);
+        {
+            const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
+            for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
+            __syncthreads();
+            block_bitonic_sort(s_keys, n2);
+        }
         bool write_out = nq_items == 1;
         if (!write_out) {
             // this item's best kq keys go to its partial row; the query's last item merges
@@ -1925,9 +1949,10 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
                 topk_rounds(s_keys, cap, kq, (int)nq_items * kq, &s_cnt, &s_th,
                             [&](int i) { return __ldcg(rows + (uint64_t)(i / kq) * k_out + (i % kq)); });
                 c = s_cnt;
-                for (int i = c + t; i < cap; i += blockDim.x) s_keys[i] = ~0ull;
+                const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
+                for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
                 __syncthreads();
-                block_bitonic_sort(s_keys, cap);
+                block_bitonic_sort(s_keys, n2);
                 write_out = true;
             }
         }
@@ -1984,6 +2009,7 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     w.item_off = (uint32_t*)take("item_off", (q + 1) * 4);
     w.mm = (uint32_t*)take("minmax", q * 2 * 4);
     w.nfin = (uint32_t*)take("nfin", q * 4);
+    w.zin = (uint32_t*)take("morton_in", q * 4);
     w.counter = (uint32_t*)take("counter", 16);
     w.lut16 = P.lut_fp16 != 0;
     w.lut = (float*)take("lut", q * G * kCodes * 32 * (w.lut16 ? 2 : 4));

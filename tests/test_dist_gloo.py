@@ -59,3 +59,11 @@ def test_algorithmic_scan_bytes():
     import bench
     got = bench.algorithmic_scan_bytes([1000, 2000, 0], [900, 10, 0], [False, True, True], M=32, l=4)
     assert got == 1000 * 32 + (2000 * 16 + 10 * 32)
+
+
+def test_algorithmic_scan_bytes_with_morton_precheck():
+    import bench
+    # predicate-first query: 8 bytes of Morton code per candidate, labels only for the 300
+    # candidates inside the cell box, codes for the 10 survivors; post-filter unchanged
+    got = bench.algorithmic_scan_bytes([1000, 2000], [900, 10], [False, True], M=32, l=4, zin_q=[0, 300])
+    assert got == 1000 * 32 + (2000 * 8 + 300 * 16 + 10 * 32)
