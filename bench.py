@@ -298,27 +298,31 @@ def max_relative_error(ws, dist, ids, n_sample):
     return worst
 
 
-def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int, zin_q=None) -> float:
-    """Bytes the ADC scan of one batch must read: M code bytes per candidate of a post-filter
-    query; for a predicate-first query 4*l label bytes per candidate plus M code bytes per
-    candidate that passes the predicate (the others need no ADC).  With zin_q (the compacting
-    scan, which reads each candidate's 8-byte Morton code and the labels only of the zin_q
-    candidates whose cell lies in the query's cell box), a predicate-first query reads
-    8 * candidates + 4*l * zin + M * passing."""
+def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int, read_q=None, chk_q=None, cbytes: int = 4):
+    """Bytes the candidate stream of one batch must read, as (predicate pass, ADC scan).
+
+    A post-filter query: M code bytes per candidate, in the ADC scan.  A predicate-first query
+    with the predicate inside the ADC scan (read_q None): 4*l label bytes per candidate plus M
+    code bytes per candidate that passes, all in the ADC scan.  A predicate-first query of the
+    predicate pass: cbytes of packed cell coordinates per candidate whose cell it tested (chk_q)
+    and 4*l label bytes per candidate whose labels it read (read_q), then M code bytes per
+    survivor in the ADC scan."""
     cand_q = np.asarray(cand_q, np.float64)
     pass_q = np.asarray(pass_q, np.float64)
-    if zin_q is None:
-        pre_bytes = cand_q * (4 * l) + pass_q * M
-    else:
-        pre_bytes = cand_q * 8 + np.asarray(zin_q, np.float64) * (4 * l) + pass_q * M
-    return float(np.where(np.asarray(pre_q, bool), pre_bytes, cand_q * M).sum())
+    pre = np.asarray(pre_q, bool)
+    adc = float(np.where(pre, pass_q * M, cand_q * M).sum())
+    if read_q is None:
+        return 0.0, adc + float((cand_q * (4 * l))[pre].sum())
+    read_q = np.asarray(read_q, np.float64)
+    chk_q = np.zeros_like(read_q) if chk_q is None else np.asarray(chk_q, np.float64)
+    return float((chk_q * cbytes + read_q * (4 * l))[pre].sum()), adc
 
 
-def scan_traffic(ws, candidates):
-    """DRAM bytes of one k_scan_fast launch: the per-candidate figure of the committed ncu
+def scan_traffic(ws, candidates, kernel="k_scan_fast"):
+    """DRAM bytes of one launch of the kernel: the per-candidate figure of the committed ncu
     summary for this workload (dram__bytes_read.sum + dram__bytes_write.sum over the
     candidates of the captured launch) times this launch's candidates; None without one."""
-    f = ROOT / "profiles" / f"k_scan_fast_{ws['name']}.md"
+    f = ROOT / "profiles" / f"{kernel}_{ws['name']}.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -422,7 +426,8 @@ def run_hdgrid(args):
     ids_np = ids.cpu().numpy().view(np.uint64)
     rec = recall_of(ids_np)
     max_rel = max_relative_error(ws, dist.cpu().numpy(), ids_np, args.err_sample)
-    cand_q = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:nq, 0].astype(np.uint64)
+    qstat = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:nq]
+    cand_q, exact_q = qstat[:, 0].astype(np.uint64), qstat[:, 1].astype(np.uint64)
     cand = int(cand_q.sum())
     info = idx.info()
     p0 = hg.parse_config(ws["hdgrid_conf"])
@@ -430,11 +435,15 @@ def run_hdgrid(args):
     if learned:
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
     pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
-    # the compacting scan (one 32-subspace group, one candidate per thread) pre-checks Morton codes
-    compacting = (info["M"] + 31) // 32 == 1 and int(idx.params["scan_cpt"]) in (0, 1)
-    zin_q = (np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq].astype(np.uint64)
-             if compacting else None)
-    scan_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"], zin_q)
+    # the predicate pass (the fast ADC path: M a multiple of 32, at most 96) counts the packed
+    # cells and labels it read per query
+    pred_pass = info["M"] % 32 == 0 and info["M"] <= 96
+    read_q = chk_q = None
+    if pred_pass:
+        read_q = np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq].astype(np.uint64)
+        chk_q = np.frombuffer(idx.debug_fetch("morton_checked").tobytes(), np.uint32)[:nq].astype(np.uint64)
+    pred_bytes, adc_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"], read_q, chk_q,
+                                                   info["cell_pack_bytes"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
 
@@ -499,8 +508,19 @@ def run_hdgrid(args):
         versus = L.compare_at_equal_recall(rec, value / world, plain, TARGET_RECALL)
 
     peak, peak_kind = hbm_peak()
-    per_cand = scan_bytes / max(cand, 1)
-    achieved = scan_bytes / (scan_avg / 1e3) / 1e9
+    # the roofline of the dominant kernel of the candidate stream: the predicate pass
+    # (k_pre_scan) or the ADC scan (k_scan_fast), by their stage times
+    pred_avg = stage_ms.get("predicate", 0.0)
+    if pred_avg > scan_avg:
+        kern, k_ms, k_bytes, k_cand = "k_pre_scan", pred_avg, pred_bytes, int(cand_q[pre_q].sum())
+        other = {"kernel": "k_scan_fast", "kernel_ms": scan_avg, "algorithmic_bytes": adc_bytes,
+                 "achieved": adc_bytes / (scan_avg / 1e3) / 1e9}
+    else:
+        kern, k_ms, k_bytes, k_cand = "k_scan_fast", scan_avg, adc_bytes, cand
+        other = ({"kernel": "k_pre_scan", "kernel_ms": pred_avg, "algorithmic_bytes": pred_bytes,
+                  "achieved": pred_bytes / (pred_avg / 1e3) / 1e9} if pred_avg > 0 else None)
+    per_cand = k_bytes / max(k_cand, 1)
+    achieved = k_bytes / (k_ms / 1e3) / 1e9
     if rank != 0:
         return
     line = {
@@ -514,10 +534,11 @@ def run_hdgrid(args):
                   | ({"schedule": "learned (LEARNED=1)"} if learned else {})
                   | ({"cuda_graph": True, "autotuned": tuned} if graph_mode else {}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": scan_traffic(ws, cand), "kernel": "k_scan_fast", "peak_kind": f"{peak_kind} hbm_gbs",
-                     "algorithmic_bytes_per_candidate": per_cand, "kernel_ms": scan_avg,
-                     "kernel_ms_source": "event nodes around the scan inside every timed graph replay" if graph_mode
-                     else "events around the scan in every timed step"},
+                     "traffic": scan_traffic(ws, k_cand, kern), "kernel": kern, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_candidate": per_cand, "candidates": k_cand, "kernel_ms": k_ms,
+                     "kernel_ms_source": "event nodes around the stage inside every timed graph replay" if graph_mode
+                     else "events around the stage in every timed step"}
+                    | ({"other_stream_kernel": other} if other else {}),
         "e2e": {"value": world * nq * args.steps / (e2e_total / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": int(q_h.numel() * 4 + ql_h.numel() * 4 + (k_h.numel() * 4 if k_h is not None else 0)),
                 "d2h_bytes_per_step": int(d_h.numel() * 4 + i_h.numel() * 8)},

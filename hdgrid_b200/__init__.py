@@ -53,7 +53,8 @@ class hdg_index_info(C.Structure):
         ("grid_dims", C.c_int32 * MAX_DIMS), ("shuffle", C.c_int32 * MAX_DIMS),
         ("label_left", C.c_uint64 * MAX_DIMS), ("label_span", C.c_uint64 * MAX_DIMS),
         ("morton_dims", C.c_int32), ("morton_max_bits", C.c_int32), ("morton_valid_map", C.c_int32),
-        ("diff_dim", C.c_int32), ("device_bytes", C.c_uint64), ("prefix_entries", C.c_uint64)]
+        ("diff_dim", C.c_int32), ("device_bytes", C.c_uint64), ("prefix_entries", C.c_uint64),
+        ("cell_pack_bytes", C.c_uint64)]
 
 
 class HDGError(RuntimeError):
@@ -266,7 +267,8 @@ class SuperGridIndex:
                 "shuffle": list(i.shuffle[:l]), "label_left": list(i.label_left[:l]),
                 "label_span": list(i.label_span[:l]), "morton_dims": i.morton_dims,
                 "morton_max_bits": i.morton_max_bits, "morton_valid_map": i.morton_valid_map,
-                "diff_dim": i.diff_dim, "device_bytes": i.device_bytes, "prefix_entries": i.prefix_entries}
+                "diff_dim": i.diff_dim, "device_bytes": i.device_bytes, "prefix_entries": i.prefix_entries,
+                "cell_pack_bytes": i.cell_pack_bytes}
 
     def build(self, build_in: build_input_t, stream=None) -> None:
         ds, lb = build_in.dataset, build_in.data_labels

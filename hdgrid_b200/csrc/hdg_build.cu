@@ -297,6 +297,23 @@ __global__ void k_scan_axis(uint32_t* __restrict__ prefix, uint64_t n_lines, uin
     }
 }
 
+// Packed cell coordinates of every point from its Morton code: dim i's coordinate is the
+// code's bits under zmask[i] in ascending order (morton_dim_masks), placed at pack_off[i].
+template <typename T>
+__global__ void k_pack_cells(const uint64_t* __restrict__ z, uint64_t n, GridMeta g, T* __restrict__ out) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint64_t code = z[r];
+    uint64_t packed = 0;
+    for (int i = 0; i < g.l; i++) {
+        if (!g.pack_w[i]) continue;
+        uint64_t m = g.zmask[i], c = 0;
+        for (int k = 0; m; k++, m &= m - 1) c |= ((code >> (__ffsll((long long)m) - 1)) & 1ull) << k;
+        packed |= c << g.pack_off[i];
+    }
+    out[r] = (T)packed;
+}
+
 // codes [n][chunks] (16-byte chunks, row-major) -> [chunks][n]: chunk j of point p at j*n + p
 __global__ void k_interleave_codes(const uint4* __restrict__ rows, uint64_t n, uint32_t chunks,
                                    uint4* __restrict__ out) {
@@ -772,7 +789,12 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_cb = reserve(H.centers.size() * 2), o_scb = reserve(H.sub_centers.size() * 2);
     const size_t o_cn = reserve((H.C + H.n_lists) * 4);
     const size_t o_co = reserve(H.cluster_off.size() * 4), o_lo = reserve(H.list_off.size() * 4);
+    GridMeta gp = H.grid;
+    morton_dim_masks(gp);
+    cell_pack_layout(gp);
+    const uint32_t pack_bytes = gp.pack_bits <= 16 ? 2u : gp.pack_bits <= 32 ? 4u : gp.pack_bits <= 64 ? 8u : 0u;
     const size_t o_z = reserve(H.zcodes.size() * 8), o_id = reserve(H.ids.size() * 4);
+    const size_t o_pk = reserve(H.zcodes.size() * pack_bytes);
     const size_t o_code = reserve(H.codes.size() + 64), o_lab = reserve(H.labels.size() * 4);
     const size_t o_pq = reserve(H.pq_centers.size() * 4), o_pre = reserve(H.prefix.size() * 4);
     const size_t o_poff = reserve(H.prefix_off.size() * 8), o_prow = reserve(H.prefix_rows.size() * 8);
@@ -792,6 +814,19 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.list_off = (const uint32_t*)up(o_lo, H.list_off.data(), H.list_off.size() * 4);
     D.zcodes = (const uint64_t*)up(o_z, H.zcodes.data(), H.zcodes.size() * 8);
     D.ids = (const uint32_t*)up(o_id, H.ids.data(), H.ids.size() * 4);
+    D.pack_bytes = pack_bytes;
+    D.labels_nan = std::any_of(H.labels.begin(), H.labels.end(), [](float v) { return std::isnan(v); }) ? 1u : 0u;
+    D.cellpack = pack_bytes ? base + o_pk : nullptr;
+    if (pack_bytes && H.n) {
+        const unsigned nb = blocks_for(H.n, 256);
+        if (pack_bytes == 2)
+            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint16_t*>(base + o_pk));
+        else if (pack_bytes == 4)
+            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint32_t*>(base + o_pk));
+        else
+            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint64_t*>(base + o_pk));
+        CK_LAUNCH();
+    }
     {
         // pool-ordered rows -> 16-byte chunk planes (the scan's coalesced layout)
         DevMem<uint8_t> rows(std::max<size_t>(H.codes.size(), 16));
@@ -835,8 +870,7 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.S_max = 0;
     for (uint64_t c = 0; c < H.C; c++)
         D.S_max = std::max<uint32_t>(D.S_max, H.cluster_off[c + 1] - H.cluster_off[c]);
-    idx->grid = H.grid;
-    morton_dim_masks(idx->grid);
+    idx->grid = gp;
     CK(cudaStreamSynchronize(st));
     CK_LAUNCH();
     idx->built = true;

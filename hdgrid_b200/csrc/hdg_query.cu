@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "hdg_device.cuh"
 #include "hdg_internal.h"
@@ -37,6 +38,7 @@ constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr uint32_t kChunk = 32768;  // default candidates per scan work item (SCAN_CHUNK)
 constexpr int kBins = 4096;         // select histogram
 constexpr int kBCap = 4096;         // boundary-bin buffer of the select
+constexpr uint32_t kPreChunk = 8192; // candidates per work item of the predicate pass
 
 struct Workspace {
     float* box;              // [q x 2l]
@@ -48,15 +50,18 @@ struct Workspace {
     uint32_t* probe_lists;   // [q x Ps]
     uint32_t* range_start;   // [q x Ps]
     uint32_t* range_len;     // [q x Ps]
+    uint32_t* range_pre;     // [q x (Ps + 1)] exclusive prefix of range_len (last: the candidate total)
     uint32_t* qstat;         // [q x 4]: cand_total, exact_total, n_lists, n_clusters
     uint64_t* scal;          // [8]: cand sum, exact sum, max cand, items, beta (f32 bits),
                              //      queries dropped by a capacity, kept candidates, selected sum
     uint64_t* qoff;          // [q + 1] candidate offsets into dist
-    uint32_t* item_off;      // [q + 1] work-item offsets
+    uint32_t* item_off;      // [q + 1] work-item offsets of the ADC scan
+    uint32_t* pitem_off;     // [q + 1] work-item offsets of the predicate pass (predicate-first queries)
     uint32_t* mm;            // [q x 2] min / max finite distance key
     uint32_t* nfin;          // [q] finite distances (predicate passed)
-    uint32_t* zin;           // [q] candidates of the compacting scan inside the cell box by their Morton code
-    uint32_t* counter;       // [4] work counter
+    uint32_t* zin;           // [q] candidates of the predicate pass whose labels were read
+    uint32_t* zchk;          // [q] candidates of the predicate pass whose Morton code was read
+    uint32_t* counter;       // [4] work counters: ADC scan, refine, predicate pass
     float* lut;              // [q x G x 256 x 32] f32, or __half when lut16
     int lut16;               // LUT stored in FP16 (LUT_FP16=1); the scan sums in FP32
     uint32_t* qbud;          // [q] candidate budget n_cand of each query (k_batch)
@@ -68,7 +73,7 @@ struct Workspace {
     uint32_t* rdone;         // [q] refine items finished per query
     uint32_t* rsurv;         // [q] rows re-ranked exactly per query (predicate survivors of the selection)
     uint64_t* rpart;         // [refine items x k_max] best keys of each refine item
-    int surv_list;           // 1: the compacting scan lists each predicate-first query's survivors
+    int surv_list;           // 1: the predicate pass lists each predicate-first query's survivors
     float* dist;             // [sum of candidates]
     uint32_t* spos;          // [sum of candidates] candidate position of each entry of a compact row
     float* S;                // [q x (C + L)] tensor-core dot products (nullptr: exact path only)
@@ -102,6 +107,9 @@ __device__ __forceinline__ int q_sched(const Workspace& w, uint64_t qi) { return
 __device__ __forceinline__ bool q_prefilter(const Workspace& w, uint64_t qi) {
     return w.mode == kPre || q_sched(w, qi) == 1;
 }
+// true when query qi's row is compact: the predicate pass lists its survivors (position and
+// pool row), the ADC scan replaces each pool row by the survivor's distance
+__device__ __forceinline__ bool compacts(const Workspace& w, uint64_t qi) { return w.surv_list && q_prefilter(w, qi); }
 // Candidate budget n_cand of query qi given the batch's beta and max_row_len: the query's k for
 // the reference pre-filter schedule (exps0 <= 1), exps0 * k for the single-dim schedule and the
 // predicate-first schedule, and the reference's min(exps0 * k * beta, max_row_len) for the
@@ -126,40 +134,6 @@ __device__ __forceinline__ uint64_t budget_of(const Workspace& w, uint64_t qi, f
 }
 __device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) { return w.qbud[qi]; }
 
-// Exclusive block-wide scan of n u32 values in shared memory (in place).  All threads.
-__device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_t* s_warp) {
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int b = t * per, e = min(n, b + per);
-    uint32_t local = 0;
-    for (int i = b; i < e; i++) local += v[i];
-    uint32_t x = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t y = lane < nw ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
-            if (lane >= o) y += z;
-        }
-        if (lane < nw) s_warp[lane] = y;
-    }
-    __syncthreads();
-    uint32_t run = x - local + (warp ? s_warp[warp - 1] : 0);
-    for (int i = b; i < e; i++) {
-        const uint32_t vi = v[i];
-        v[i] = run;
-        run += vi;
-    }
-    __syncthreads();
-}
-
 // Slot of this lane among the lanes of its warp where f holds, taken from the counter *ctr
 // with one atomic per warp (~0u where f is false).  Every lane of the warp must call it.
 __device__ __forceinline__ uint32_t warp_reserve(bool f, uint32_t* ctr) {
@@ -176,6 +150,32 @@ __device__ __forceinline__ uint32_t warp_reserve(bool f, uint32_t* ctr) {
 __device__ __forceinline__ void warp_append(bool f, uint32_t v, uint32_t* ctr, uint32_t* dst) {
     const uint32_t slot = warp_reserve(f, ctr);
     if (f) dst[slot] = v;
+}
+
+// Inclusive sum of x over the block (blockDim.x a multiple of 32, <= 1024); s_w: 32 words of
+// shared scratch that no other thread touches until the following barrier.
+__device__ __forceinline__ unsigned long long block_inclusive_sum(unsigned long long x, unsigned long long* s_w,
+                                                                  unsigned long long* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long y = lane < nw ? s_w[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        s_w[lane] = y;
+    }
+    __syncthreads();
+    *total = s_w[nw - 1];
+    return x + (warp ? s_w[warp - 1] : 0);
 }
 
 // ------------------------------------------------------------------------------------
@@ -463,6 +463,7 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     __shared__ uint32_t s_chosen[1024];
     __shared__ uint32_t s_red[2];
     __shared__ uint32_t s_wc[32];
+    __shared__ unsigned long long s_scan[32];
     __shared__ int s_nvalid;
     __shared__ float s_bound;
     const uint64_t qi = blockIdx.x;
@@ -654,6 +655,24 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     atomicAdd(&s_red[0], my_cand);
     atomicAdd(&s_red[1], my_exact);
     __syncthreads();
+    // the exclusive prefix of the ranges' lengths (its last entry the candidate total): the
+    // predicate pass, the scan and the select find a position's range by searching it
+    {
+        const int Rq = Ps * ns;
+        const uint32_t* len = w.range_len + qi * Rq;
+        uint32_t* pre = w.range_pre + qi * (Rq + 1);
+        unsigned long long run = 0;
+        for (int b0 = 0; b0 < Rq; b0 += blockDim.x) {
+            const int i = b0 + t;
+            const unsigned long long x = i < Rq ? len[i] : 0;
+            unsigned long long tot = 0;
+            const unsigned long long inc = block_inclusive_sum(x, s_scan, &tot);
+            if (i < Rq) pre[i] = (uint32_t)(run + inc - x);
+            run += tot;
+            __syncthreads();  // s_scan is reused by the next chunk
+        }
+        if (t == 0) pre[Rq] = (uint32_t)run;
+    }
     if (t == 0) {
         w.qstat[qi * 4 + 0] = s_red[0];
         w.qstat[qi * 4 + 1] = s_red[1];
@@ -666,34 +685,8 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
 // ------------------------------------------------------------------------------------
 // k_batch: per-query candidate offsets and work items, batch sums (one block)
 // ------------------------------------------------------------------------------------
-// Inclusive sum of x over the block (blockDim.x a multiple of 32, <= 1024); s_w: 32 words of
-// shared scratch that no other thread touches until the following barrier.
-__device__ __forceinline__ unsigned long long block_inclusive_sum(unsigned long long x, unsigned long long* s_w,
-                                                                  unsigned long long* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_w[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        unsigned long long y = lane < nw ? s_w[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, o);
-            if (lane >= o) y += z;
-        }
-        s_w[lane] = y;
-    }
-    __syncthreads();
-    *total = s_w[nw - 1];
-    return x + (warp ? s_w[warp - 1] : 0);
-}
-
 __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
-    __shared__ unsigned long long s_tot[32], s_items[32], s_sel[32];
+    __shared__ unsigned long long s_tot[32], s_items[32], s_pitems[32], s_sel[32];
     __shared__ unsigned long long s_red[3], s_drop[2];
     __shared__ float s_beta;
     const int t = threadIdx.x;
@@ -701,22 +694,29 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
     __syncthreads();
     const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
     const uint64_t b = t * per, e = min(q, b + per);
-    unsigned long long cand = 0, items = 0, exact = 0, mx = 0;
+    // a predicate-first query of the predicate pass has predicate items over its candidates
+    // (its ADC items follow from its survivors, k_scan_plan); any other query has ADC items
+    auto n_items = [&](uint64_t i, uint32_t c) { return compacts(w, i) ? 0u : (c + w.chunk - 1) / w.chunk; };
+    auto n_pitems = [&](uint64_t i, uint32_t c) { return compacts(w, i) ? (c + kPreChunk - 1) / kPreChunk : 0u; };
+    unsigned long long cand = 0, items = 0, pitems = 0, exact = 0, mx = 0;
     for (uint64_t i = b; i < e; i++) {
         const uint32_t c = w.qstat[i * 4];
         cand += c;
-        items += (c + w.chunk - 1) / w.chunk;
+        items += n_items(i, c);
+        pitems += n_pitems(i, c);
         exact += w.qstat[i * 4 + 1];
         mx = max(mx, (unsigned long long)c);
     }
-    unsigned long long tot_c = 0, tot_i = 0;
+    unsigned long long tot_c = 0, tot_i = 0, tot_p = 0;
     unsigned long long rc = block_inclusive_sum(cand, s_tot, &tot_c) - cand;
     unsigned long long ri = block_inclusive_sum(items, s_items, &tot_i) - items;
+    unsigned long long rp = block_inclusive_sum(pitems, s_pitems, &tot_p) - pitems;
     unsigned long long dropped = 0, kept = 0;
     for (uint64_t i = b; i < e; i++) {
         const uint32_t c = w.qstat[i * 4];
         w.qoff[i] = rc;
         w.item_off[i] = (uint32_t)ri;
+        w.pitem_off[i] = (uint32_t)rp;
         // queries past the distance capacity (a prefix cut: offsets grow with i) get no
         // candidates; the batch's beta and max_row above still count them
         if (rc + c > w.cap) {
@@ -727,17 +727,20 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         } else {
             kept += c;
         }
+        ri += n_items(i, c);
+        rp += n_pitems(i, c);
         rc += c;
-        ri += (c + w.chunk - 1) / w.chunk;
         w.mm[2 * i] = 0xffffffffu;
         w.mm[2 * i + 1] = 0u;
         w.nfin[i] = 0;
         w.zin[i] = 0;
+        w.zchk[i] = 0;
         w.cand_count[i] = 0;
     }
     if (e == q && b < e) {
         w.qoff[q] = rc;
         w.item_off[q] = (uint32_t)ri;
+        w.pitem_off[q] = (uint32_t)rp;
     }
     atomicAdd(&s_red[0], cand);
     atomicAdd(&s_red[1], exact);
@@ -747,12 +750,13 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         w.scal[0] = s_red[0];
         w.scal[1] = s_red[1];
         w.scal[2] = s_red[2];
-        w.scal[3] = tot_i;
+        w.scal[3] = tot_i + tot_p;
         // beta = coarse / real as the reference computes it (Super-Grid-IVF_PQ.cu:1219)
         const float beta = s_red[1] == 0 ? INFINITY : __fdiv_rn((float)s_red[0], (float)s_red[1]);
         w.scal[4] = __float_as_uint(beta);
         s_beta = beta;
         w.counter[0] = 0;
+        w.counter[2] = 0;
     }
     __syncthreads();
     // each query's budget n_cand, now that the batch's beta and max_row are known, and the
@@ -926,70 +930,344 @@ __device__ __forceinline__ void adc_group1(const uint4* cp, uint64_t n_pts, int 
     }
 }
 
-// Predicate-first candidates queued per lane before their ADC (fast path, one 32-subspace
-// group, one candidate per thread): the queue of each lane holds up to kPreQueue entries.
-constexpr int kPreQueue = 8;
-constexpr int kPreStep = 4;  // positions per lane in one predicate step (<= kPreQueue / 2)
-constexpr bool scan_compacts(int G, int CPT) { return G == 1 && CPT == 1; }
-
+// Loads the query's range table (prefix of the range lengths and range starts) into shared
+// memory.  All threads; ends with a barrier.
 __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int qq, uint32_t* s_pre,
-                                                uint32_t* s_start, uint32_t* s_warp) {
-    for (int i = threadIdx.x; i < Ps; i += blockDim.x) {
-        s_pre[i] = w.range_len[(uint64_t)qq * Ps + i];
-        s_start[i] = w.range_start[(uint64_t)qq * Ps + i];
-    }
-    if (threadIdx.x == 0) s_pre[Ps] = 0;
+                                                uint32_t* s_start) {
+    const uint32_t* pre = w.range_pre + (uint64_t)qq * (Ps + 1);
+    for (int i = threadIdx.x; i <= Ps; i += blockDim.x) s_pre[i] = pre[i];
+    for (int i = threadIdx.x; i < Ps; i += blockDim.x) s_start[i] = w.range_start[(uint64_t)qq * Ps + i];
     __syncthreads();
-    block_exclusive_scan(s_pre, Ps + 1, s_warp);
 }
 
-// The cell box of a query in the Morton domain (one entry per valid dim, shuffled order):
-// mask of the dim's bits, the low cell's masked code and the high cell's masked code, the
-// latter ~0 when the high side cannot reject exactly.  A candidate's cell below the low
-// cell means its label is below the box's low bound: the low cell comes from
-// max(trunc(lo), left), which is at most lo (or at most every label), and cell ids grow with
-// the label (get_grid_id_device, Super-Grid-IVF_PQ.cu:24-26).  Above the high cell only
-// proves the label exceeds r = (float)min(trunc(hi), left + span), the value the cell box was
-// computed from (:947-960); that rejects exactly when r >= hi.
-__device__ void morton_box_bounds(const GridMeta& g, uint64_t zlo, uint64_t zhi, const float* box, uint64_t* zm,
-                                  uint64_t* lo, uint64_t* hi, int* n) {
-    int k = 0;
-    for (int i = 0; i < g.l; i++) {
-        const uint64_t m = g.zmask[i];
-        if (!m) continue;
-        const float bh = box[2 * g.shuffle[i] + 1];
-        const uint64_t bhi = (uint64_t)bh;  // saturating, as in cell_range
-        const uint64_t rr = g.left[i] + g.span[i];
-        const float r = (float)(bhi < rr ? bhi : rr);
-        zm[k] = m;
-        lo[k] = zlo & m;
-        hi[k] = (r >= bh) ? (zhi & m) : ~0ull;
-        k++;
+// ------------------------------------------------------------------------------------
+// k_pre_scan: the label predicate of the predicate-first queries, ahead of their ADC
+// ------------------------------------------------------------------------------------
+// A predicate-first query (query_prefilter, prefiltering.cu:36-51; the learned schedule's
+// predicate-first flag) keeps only its candidates that pass the label predicate
+// (filter.cu:30-64), and only those need an ADC distance.  This pass runs before the ADC scan:
+// one warp per work item (kPreChunk consecutive candidate positions of one query), no
+// shared-memory LUT, so it runs at full occupancy and streams the candidates' packed cell
+// coordinates and labels.  A lane tests positions lane, lane + 32, ... of every step of 32 * J:
+//   1. the candidate's cell against the query's cell box, all dims in one guarded-field range
+//      test: a cell outside the box on a side where that proves the label test fails rejects
+//      the candidate without reading its labels;
+//   2. the labels of the other candidates against the query's f32 box, 32 per round from a
+//      per-warp queue, so that a round's label loads are all useful;
+//   3. the survivors are staged per warp and appended to the query's row 32 at a time -- the
+//      candidate position into spos and the pool row into the distance slot, which the ADC
+//      scan then overwrites with the survivor's distance.
+// The row's order depends on timing; the distance of each survivor does not (the ADC order
+// follows its position) and the select orders ties by position.
+constexpr int kPreThreads = 256;
+
+// Largest i in [0, n) with a[i] <= key (a nondecreasing, a[0] <= key), by 32-way rounds.
+// Every lane of the warp calls it and gets the answer.
+__device__ __forceinline__ int warp_find_le(const uint32_t* a, int n, uint32_t key) {
+    const int lane = threadIdx.x & 31;
+    int lo = 0, len = n;
+    while (len > 1) {
+        const int step = (len + 31) >> 5;
+        const int off = lane * step;
+        const bool ok = off < len && a[lo + off] <= key;
+        const unsigned b = __ballot_sync(0xffffffffu, ok);  // bit 0 set: a[lo] <= key
+        const int j = 31 - __clz(b);
+        lo += j * step;
+        len = min(step, len - j * step);
     }
-    *n = k;
+    return lo;
+}
+
+// Appends (a, b) of the lanes where f holds to a per-warp buffer ([0, 64) first words, [64,
+// 128) second words) that holds n entries (warp-uniform, n < 32 on entry).
+__device__ __forceinline__ void warp_push(uint32_t* buf, int& n, bool f, uint32_t a, uint32_t b) {
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (f) {
+        const int s = n + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+        buf[s] = a;
+        buf[64 + s] = b;
+    }
+    n += __popc(bal);
+}
+
+// Drops the first 32 of the buffer's n entries (32 <= n < 64).
+__device__ __forceinline__ void warp_drop32(uint32_t* buf, int& n) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    const bool mv = lane < n - 32;
+    uint32_t a = 0, b = 0;
+    if (mv) {
+        a = buf[32 + lane];
+        b = buf[96 + lane];
+    }
+    __syncwarp();
+    if (mv) {
+        buf[lane] = a;
+        buf[64 + lane] = b;
+    }
+    __syncwarp();
+    n -= 32;
+}
+
+// One predicate-pass work item: positions [e0, e1) of one query.  PT: the packed cell type,
+// CHECK: test the cell box first (lo_f / hi_g / gd: the box's low fields, its high fields with
+// the guard bits set, the guard bits), LAB4: four 16-byte-aligned label dims in registers.
+template <typename PT, bool CHECK, bool LAB4>
+__device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float* bx_s, PT lo_f, PT hi_g, PT gd,
+                                         const uint32_t* pre, const uint32_t* start, int r0, uint32_t e0,
+                                         uint32_t e1, uint32_t* qb, uint32_t* sb, uint32_t* ctr, uint32_t* drow,
+                                         uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
+    constexpr int J = 8;  // positions per lane in one step
+    const int lane = threadIdx.x & 31;
+    float bx[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) bx[i] = LAB4 ? bx_s[i] : 0.f;
+    const PT* cells = static_cast<const PT*>(D.cellpack);
+    const float4* lab4 = reinterpret_cast<const float4*>(D.labels);
+    // the lane's walk over the query's ranges: positions only grow along it
+    int rr = r0;
+    uint32_t nb = pre[rr + 1], base = start[rr] - pre[rr];
+    int qn = 0, sn = 0;
+    // the label predicate of the candidate at pool row p (a NaN label passes, as in the reference)
+    auto label_ok = [&](uint32_t p) -> bool {
+        if (LAB4) {
+            const float4 v = __ldg(lab4 + p);
+            return !(v.x < bx[0] || v.x > bx[1]) && !(v.y < bx[2] || v.y > bx[3]) && !(v.z < bx[4] || v.z > bx[5]) &&
+                   !(v.w < bx[6] || v.w > bx[7]);
+        }
+        bool ok = true;
+        const float* lab = D.labels + (uint64_t)p * lbl;
+        for (int i = 0; i < lbl; i++) {
+            const float v = __ldg(lab + i);
+            if (v < bx_s[2 * i] || v > bx_s[2 * i + 1]) ok = false;
+        }
+        return ok;
+    };
+    // the first m (<= 32) staged survivors to the row
+    auto flush = [&](int m) {
+        __syncwarp();
+        uint32_t at = 0;
+        if (lane == 0) at = atomicAdd(ctr, (uint32_t)m);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (lane < m) {
+            prow[at + lane] = sb[lane];
+            drow[at + lane] = sb[64 + lane];
+        }
+    };
+    auto stage = [&](bool f, uint32_t e, uint32_t p) {
+        warp_push(sb, sn, f, e, p);
+        if (sn >= 32) {
+            flush(32);
+            warp_drop32(sb, sn);
+        }
+    };
+    // label tests of the first m (<= 32) queued candidates, one per lane
+    auto label_round = [&](int m) {
+        __syncwarp();
+        const bool v = lane < m;
+        const uint32_t e = v ? qb[lane] : 0u, p = v ? qb[64 + lane] : 0u;
+        stage(v && label_ok(p), e, p);
+    };
+    for (uint32_t eb = e0; eb < e1; eb += 32u * J) {
+        uint32_t pp[J];
+        bool pv[J];
+#pragma unroll
+        for (int j = 0; j < J; j++) {
+            const uint32_t e = eb + lane + 32u * j;
+            pv[j] = e < e1;
+            pp[j] = 0;
+            if (pv[j]) {
+                while (nb <= e) {
+                    rr++;
+                    nb = pre[rr + 1];
+                    base = start[rr] - pre[rr];
+                }
+                pp[j] = base + e;
+            }
+        }
+        if constexpr (CHECK) {
+            PT c[J];
+#pragma unroll
+            for (int j = 0; j < J; j++) c[j] = pv[j] ? __ldg(cells + pp[j]) : PT(0);
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                n_chk += pv[j] ? 1u : 0u;
+                // every field at or above its low bound and at or below its high bound: the
+                // guard bit above a field survives both subtractions exactly then
+                const PT t = (PT)((PT)((c[j] | gd) - lo_f) & (PT)(hi_g - c[j]));
+                pv[j] = pv[j] && (PT)(t & gd) == gd;
+                n_read += pv[j] ? 1u : 0u;
+                warp_push(qb, qn, pv[j], eb + lane + 32u * j, pp[j]);
+                if (qn >= 32) {
+                    label_round(32);
+                    warp_drop32(qb, qn);
+                }
+            }
+        } else if (LAB4) {
+            // four 16-byte label loads in flight at a time
+#pragma unroll
+            for (int j0 = 0; j0 < J; j0 += 4) {
+                float4 v[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    v[j] = pv[j0 + j] ? __ldg(lab4 + pp[j0 + j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    n_read += pv[j0 + j] ? 1u : 0u;
+                    const bool ok = pv[j0 + j] && !(v[j].x < bx[0] || v[j].x > bx[1]) &&
+                                    !(v[j].y < bx[2] || v[j].y > bx[3]) && !(v[j].z < bx[4] || v[j].z > bx[5]) &&
+                                    !(v[j].w < bx[6] || v[j].w > bx[7]);
+                    stage(ok, eb + lane + 32u * (j0 + j), pp[j0 + j]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                n_read += pv[j] ? 1u : 0u;
+                stage(pv[j] && label_ok(pp[j]), eb + lane + 32u * j, pp[j]);
+            }
+        }
+    }
+    if (CHECK && qn > 0) label_round(qn);
+    if (sn > 0) flush(sn);
+}
+
+template <typename PT, bool LAB4>
+__global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMeta g, int R, int lbl, uint64_t q,
+                                                             Workspace w) {
+    constexpr int NW = kPreThreads / 32;
+    __shared__ uint32_t s_qb[NW][128], s_sb[NW][128];  // cell-passed queue, survivor staging
+    __shared__ float s_bx[NW][2 * kMaxDims];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const uint32_t n_items = w.pitem_off[q];
+    const int l = g.l;
+    for (;;) {
+        __syncwarp();  // the previous item's reads of the warp's tables are done
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(&w.counter[2], 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= n_items) break;
+        const int qq = warp_find_le(w.pitem_off, (int)q, item);
+        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const uint32_t e0 = (item - w.pitem_off[qq]) * kPreChunk;
+        if (e0 >= total) continue;  // a query cut by a capacity
+        const uint32_t e1 = min(total, e0 + kPreChunk);
+        if (lane < 2 * lbl) s_bx[wp][lane] = w.box[(uint64_t)qq * 2 * lbl + lane];
+        // The cell box as packed fields, per dim (shuffled order) and side that can reject: a
+        // cell below the low cell means a label below l = (float)max(trunc(lo), left), as cells
+        // grow with the label (get_grid_id_device, Super-Grid-IVF_PQ.cu:24-26), which rejects
+        // exactly when l <= lo; above the high cell only proves the label exceeds
+        // r = (float)min(trunc(hi), left + span) (:947-960), exact when r >= hi.  The other
+        // sides take every cell.  Skipped when the index holds NaN labels (a NaN passes the
+        // label test in any cell) or when the query's count of points in its cell box over the
+        // probed lists says the codes would cost more label bytes than they save.
+        const uint32_t inbox = w.qstat[(uint64_t)qq * 4 + 1];
+        const bool check = D.pack_bytes && !D.labels_nan &&
+                           (uint64_t)inbox * 16 < (uint64_t)total * (16 - D.pack_bytes);
+        uint64_t lo_f = 0, hi_f = 0, gd = 0;
+        bool act = false;
+        {
+            // lane i < l takes dim i of the grid (selected by unrolled compares: no local copy of g)
+            uint64_t left = 0, top = 0;
+            int shf = 0, gdim = 0, off = 0, wd = 0;
+#pragma unroll
+            for (int i = 0; i < kMaxDims; i++)
+                if (i == lane) {
+                    left = g.left[i];
+                    top = g.left[i] + g.span[i];
+                    shf = g.shuffle[i];
+                    gdim = g.grid_dims[i];
+                    off = g.pack_off[i];
+                    wd = g.pack_w[i];
+                }
+            if (check && lane < l && wd > 0) {
+                const int clo = w.cells[(uint64_t)qq * 2 * l + 2 * lane];
+                const int chi = w.cells[(uint64_t)qq * 2 * l + 2 * lane + 1];
+                const float blo = w.box[(uint64_t)qq * 2 * lbl + 2 * shf];
+                const float bhi = w.box[(uint64_t)qq * 2 * lbl + 2 * shf + 1];
+                const uint64_t tlo = (uint64_t)blo, thi = (uint64_t)bhi;  // saturating, as in cell_range
+                const float lf = (float)(tlo > left ? tlo : left);
+                const float rf = (float)(thi < top ? thi : top);
+                const bool lo_rej = clo > 0 && lf <= blo;
+                const bool hi_rej = chi < gdim - 1 && rf >= bhi;
+                act = lo_rej || hi_rej;
+                lo_f = (uint64_t)(lo_rej ? clo : 0) << off;
+                hi_f = (uint64_t)(hi_rej ? (uint32_t)chi : (1u << wd) - 1u) << off;
+                gd = 1ull << (off + wd);
+            }
+        }
+        // every field's bounds to every lane (fields are disjoint: OR them together)
+        const bool use = __any_sync(0xffffffffu, act);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo_f |= __shfl_xor_sync(0xffffffffu, lo_f, o);
+            hi_f |= __shfl_xor_sync(0xffffffffu, hi_f, o);
+            gd |= __shfl_xor_sync(0xffffffffu, gd, o);
+        }
+        __syncwarp();
+        const uint32_t* pre = w.range_pre + (uint64_t)qq * (R + 1);
+        const uint32_t* start = w.range_start + (uint64_t)qq * R;
+        const int r0 = warp_find_le(pre, R, e0);
+        uint32_t* ctr = &w.cand_count[qq];
+        uint32_t* drow = reinterpret_cast<uint32_t*>(w.dist + w.qoff[qq]);
+        uint32_t* prow = w.spos + w.qoff[qq];
+        uint32_t n_read = 0, n_chk = 0;
+        const float* bxs = s_bx[wp];
+        uint32_t* qb = s_qb[wp];
+        uint32_t* sb = s_sb[wp];
+        if (use)
+            pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, r0, e0, e1, qb, sb,
+                                     ctr, drow, prow, n_read, n_chk);
+        else
+            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, r0, e0, e1, qb, sb, ctr, drow,
+                                      prow, n_read, n_chk);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_read += __shfl_xor_sync(0xffffffffu, n_read, o);
+            n_chk += __shfl_xor_sync(0xffffffffu, n_chk, o);
+        }
+        if (lane == 0 && n_read) atomicAdd(&w.zin[qq], n_read);
+        if (lane == 0 && n_chk) atomicAdd(&w.zchk[qq], n_chk);
+    }
+}
+
+// ADC work items once the predicate pass has listed the survivors: a compact row has
+// cand_count entries, any other row one per candidate position.  One block.
+__global__ void __launch_bounds__(1024) k_scan_plan(uint64_t q, Workspace w) {
+    __shared__ unsigned long long s_w[32];
+    const int t = threadIdx.x;
+    const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = t * per, e = min(q, b + per);
+    auto n_items = [&](uint64_t i) {
+        const uint32_t c = compacts(w, i) ? w.cand_count[i] : w.qstat[i * 4];
+        return (c + w.chunk - 1) / w.chunk;
+    };
+    unsigned long long items = 0;
+    for (uint64_t i = b; i < e; i++) items += n_items(i);
+    unsigned long long tot = 0;
+    unsigned long long r = block_inclusive_sum(items, s_w, &tot) - items;
+    for (uint64_t i = b; i < e; i++) {
+        w.item_off[i] = (uint32_t)r;
+        r += n_items(i);
+    }
+    if (e == q && b < e) w.item_off[q] = (uint32_t)r;
+    if (t == 0) w.counter[0] = 0;
 }
 
 // Fast path (M a multiple of 32).  The CTA computes the query's LUT straight into shared
 // memory when it switches query (codeword-major loads, one subspace per lane), then streams
 // candidates; CPT candidates per thread are interleaved step by step so every thread keeps
-// CPT independent load->add chains in flight.
+// CPT independent load->add chains in flight.  A candidate at position e sums from subspace
+// (e mod 32) of each group: for a full row that is the lane, for a compact row (the predicate
+// pass's survivors) it comes from the survivor's recorded position.
 template <int G, int NT, int CPT>
-__global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast(IndexDev D, const float* __restrict__ queries, int Ps,
-                                                     int pre, int lbl, uint64_t q, Workspace w, GridMeta g) {
+__global__ void __launch_bounds__(NT, (G == 1 && CPT == 1) ? 2 : 1) k_scan_fast(IndexDev D, int Ps, uint64_t q,
+                                                                                 Workspace w) {
     extern __shared__ __align__(16) float s_lut[];  // [G][256][64]
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 64);  // [Ps + 1]
     uint32_t* s_start = s_pre + Ps + 1;                                       // [Ps]
-    // [NT/32][2][kPreQueue][32] queued (position, pool row) pairs, 16-byte aligned
-    uint32_t* s_queue = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_start + Ps) + 15) & ~uintptr_t(15));
     __shared__ ScanShared s;
-    __shared__ uint32_t s_warp[32];
-    __shared__ float s_box[2 * kMaxDims];
-    // the query's cell box in the Morton domain, one entry per valid dim: a candidate whose
-    // masked code lies below s_zlo or above s_zhi cannot pass the label predicate
-    __shared__ uint64_t s_zm[kMaxDims], s_zlo[kMaxDims], s_zhi[kMaxDims];
-    __shared__ int s_zn;
     const int t = threadIdx.x, lane = t & 31;
-    const uint32_t R = lane >> 2, sh = 8u * (lane & 3), lane4 = 4u * lane;
     const uint32_t n_items = w.item_off[q];
     int cur = -1;
     for (;;) {
@@ -1010,7 +1288,8 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
         const int item = s.item;
         if (item >= (int)n_items) break;
         const int qq = s.query;
-        const uint32_t total = w.qstat[(uint64_t)qq * 4];
+        const bool compact = compacts(w, qq);
+        const uint32_t total = compact ? w.cand_count[qq] : w.qstat[(uint64_t)qq * 4];
         const uint32_t e0 = (uint32_t)(item - w.item_off[qq]) * w.chunk;
         if (e0 >= total) {  // a query cut by the distance capacity
             __syncthreads();
@@ -1042,19 +1321,18 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                     dstl[8] = v;  // columns 32..63 repeat 0..31
                 }
             }
-            if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
-            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);  // ends with a barrier
-            if (t == 0) morton_box_bounds(g, w.zrange[(uint64_t)qq * 2], w.zrange[(uint64_t)qq * 2 + 1], s_box,
-                                          s_zm, s_zlo, s_zhi, &s_zn);
-            __syncthreads();
+            // a query's rows are all compact or all full: a compact query needs no range table
+            if (!compact) scan_load_query(w, Ps, qq, s_pre, s_start);  // ends with a barrier
+            else __syncthreads();
             cur = qq;
         }
         const uint32_t e1 = min(total, e0 + w.chunk);
         float* dst = w.dist + w.qoff[qq];
-        const bool preq = pre || q_prefilter(w, qq);
-        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0, zi = 0;
-        // each warp takes a contiguous span of the item (a multiple of 32 * CPT positions,
-        // so position mod 32 stays the lane), so a lane's walk to its candidate's range
+        const uint32_t* srow = reinterpret_cast<const uint32_t*>(dst);  // compact: the survivors' pool rows
+        const uint32_t* sp = w.spos + w.qoff[qq];
+        uint32_t kmin = 0xffffffffu, kmax = 0u, nf = 0;
+        // each warp takes a contiguous span of the item (a multiple of 32 * CPT entries, so in
+        // a full row position mod 32 stays the lane), so a lane's walk to its candidate's range
         // crosses few range boundaries per step
         constexpr uint32_t kStep = 32u * CPT;
         const uint32_t span = ((e1 - e0 + NT / 32 - 1) / (NT / 32) + kStep - 1) / kStep * kStep;
@@ -1063,6 +1341,8 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
         int r[CPT];
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
+            r[u] = 0;
+            if (compact) continue;
             const uint32_t e = wb + lane + u * 32;
             int lo = 0, hi = Ps - 1;
             while (lo < hi) {
@@ -1074,155 +1354,27 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
         }
         const uint4* planes = reinterpret_cast<const uint4*>(D.codes);
         const uint64_t n_pts = D.n;
-        bool compacted = false;
-        if constexpr (scan_compacts(G, CPT)) {
-            if (preq) {
-                // Predicate first, ADC for the survivors only.  A predicate step tests one
-                // position per lane (position mod 32 = lane, as in the loop below) and queues
-                // a survivor in that lane's queue; an ADC step takes one queued candidate per
-                // lane, so every sum is formed by the lane, and in the order, of the loop below.
-                // ADC steps run when every lane has a candidate queued, when a queue might not
-                // take a whole predicate step, and at the end of the span until the queues
-                // are empty.
-                uint32_t* qe = s_queue + (uint32_t)(t >> 5) * (2 * kPreQueue * 32);
-                // survivors are appended to the query's row in arrival order -- distance and
-                // candidate position, one counter atomic per warp -- and rejected candidates
-                // write nothing; cand_count ends as the row's length
-                uint32_t* spos = w.spos + w.qoff[qq];
-                uint32_t* qp = qe + kPreQueue * 32;
-                int qh = 0, qn = 0, rr = r[0];
-                const bool lab4 = lbl == 4 && (reinterpret_cast<uintptr_t>(D.labels) & 15) == 0;
-                float bx[8];
-#pragma unroll
-                for (int i = 0; i < 8; i++) bx[i] = lab4 ? s_box[i] : 0.f;
-                uint32_t eb = wb;
-                for (;;) {
-                    const bool more = eb < we;  // warp-uniform
-                    const bool adc = __all_sync(0xffffffffu, qn > 0) ||
-                                     __any_sync(0xffffffffu, qn > kPreQueue - kPreStep) ||
-                                     (!more && __any_sync(0xffffffffu, qn > 0));
-                    if (adc) {
-                        const bool live = qn > 0;
-                        uint32_t e = 0, row = 0;  // an idle lane reads row 0 (in bounds), result discarded
-                        if (live) {
-                            e = qe[qh * 32 + lane];
-                            row = qp[qh * 32 + lane];
-                            qh = (qh + 1) & (kPreQueue - 1);
-                            qn--;
-                        }
-                        float s0 = 0.f, s1 = 0.f;
-                        adc_group1(planes + row, n_pts, 0, R, sh, lane4, s_lut, s0, s1);
-                        s0 += s1;
-                        const uint32_t slot = warp_reserve(live, &w.cand_count[qq]);
-                        if (live) {
-                            if (s0 < INFINITY) {
-                                const uint32_t key = float_key(s0);
-                                kmin = min(kmin, key);
-                                kmax = max(kmax, key);
-                                nf++;
-                            }
-                            dst[slot] = s0;
-                            spos[slot] = e;
-                        }
-                        continue;
-                    }
-                    if (!more) break;
-                    // kPreStep positions per lane (e, e + 32, ...), their label loads in flight
-                    // together (one 16-byte load each with 4 aligned label dims)
-                    uint32_t pe[kPreStep], pp[kPreStep];
-                    bool pv[kPreStep], ps[kPreStep];
-#pragma unroll
-                    for (int j = 0; j < kPreStep; j++) {
-                        pe[j] = eb + lane + 32u * j;
-                        pv[j] = pe[j] < we;
-                        pp[j] = 0;
-                        if (pv[j]) {
-                            while (s_pre[rr + 1] <= pe[j]) rr++;
-                            pp[j] = s_start[rr] + (pe[j] - s_pre[rr]);
-                        }
-                    }
-                    // the Morton code first (8 bytes): a candidate whose cell lies outside the
-                    // cell box on a side where that proves the label test fails is rejected
-                    // without reading its labels
-                    {
-                        uint64_t zc[kPreStep];
-#pragma unroll
-                        for (int j = 0; j < kPreStep; j++) zc[j] = pv[j] ? __ldg(D.zcodes + pp[j]) : 0ull;
-                        const int zn = s_zn;
-#pragma unroll
-                        for (int j = 0; j < kPreStep; j++) {
-                            for (int i = 0; i < zn; i++) {
-                                const uint64_t c = zc[j] & s_zm[i];
-                                if (c < s_zlo[i] || c > s_zhi[i]) pv[j] = false;
-                            }
-                            zi += pv[j] ? 1u : 0u;
-                        }
-                    }
-                    if (lab4) {
-                        float4 v[kPreStep];
-#pragma unroll
-                        for (int j = 0; j < kPreStep; j++)
-                            v[j] = pv[j] ? __ldg(reinterpret_cast<const float4*>(D.labels) + pp[j])
-                                         : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                        for (int j = 0; j < kPreStep; j++)
-                            ps[j] = pv[j] && !(v[j].x < bx[0] || v[j].x > bx[1]) && !(v[j].y < bx[2] || v[j].y > bx[3]) &&
-                                    !(v[j].z < bx[4] || v[j].z > bx[5]) && !(v[j].w < bx[6] || v[j].w > bx[7]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < kPreStep; j++) {
-                            ps[j] = pv[j];
-                            if (pv[j]) {
-                                const float* lab = D.labels + (uint64_t)pp[j] * lbl;
-                                for (int i = 0; i < lbl; i++) {
-                                    const float v = lab[i];
-                                    if (v < s_box[2 * i] || v > s_box[2 * i + 1]) ps[j] = false;
-                                }
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < kPreStep; j++) {
-                        if (!pv[j]) continue;
-                        if (ps[j]) {  // qn <= kPreQueue - kPreStep before this step: room for all
-                            const int slot = (qh + qn) & (kPreQueue - 1);
-                            qe[slot * 32 + lane] = pe[j];
-                            qp[slot * 32 + lane] = pp[j];
-                            qn++;
-                        }
-                    }
-                    eb += 32u * kPreStep;
-                }
-                compacted = true;
-            }
-        }
-        for (uint32_t eb = wb + lane; !compacted && eb < we; eb += kStep) {
+        for (uint32_t eb = wb + lane; eb < we; eb += kStep) {
             const uint4* cp[CPT];
             bool live[CPT];
+            uint32_t rot[CPT];
             float sum[CPT], sum1[CPT];  // even / odd steps, added at the end
 #pragma unroll
             for (int u = 0; u < CPT; u++) {
                 const uint32_t e = eb + u * 32;
                 live[u] = e < we;
-                sum[u] = INFINITY;
-                uint32_t row = 0;  // dead / filtered candidates read row 0 (in bounds), result discarded
+                sum[u] = sum1[u] = 0.f;
+                uint32_t row = 0;  // a dead lane reads row 0 (in bounds), result discarded
+                rot[u] = (uint32_t)lane;
                 if (live[u]) {
-                    while (s_pre[r[u] + 1] <= e) r[u]++;
-                    const uint32_t pool = s_start[r[u]] + (e - s_pre[r[u]]);
-                    bool pass = true;
-                    if (preq) {
-                        const float* lab = D.labels + (uint64_t)pool * lbl;
-                        for (int i = 0; i < lbl; i++) {
-                            const float v = lab[i];
-                            if (v < s_box[2 * i] || v > s_box[2 * i + 1]) pass = false;
-                        }
-                    }
-                    if (pass) {
-                        sum[u] = 0.f;
-                        row = pool;
+                    if (compact) {
+                        row = srow[e];
+                        rot[u] = sp[e] & 31u;
+                    } else {
+                        while (s_pre[r[u] + 1] <= e) r[u]++;
+                        row = s_start[r[u]] + (e - s_pre[r[u]]);
                     }
                 }
-                sum1[u] = sum[u];
                 cp[u] = planes + row;  // chunk j of this point at cp[u][j * n_pts]
             }
 #pragma unroll
@@ -1232,7 +1384,8 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                 for (int u = 0; u < CPT; u++) {
                     const uint4 a = __ldg(cp[u] + (2 * g) * n_pts), b = __ldg(cp[u] + (2 * g + 1) * n_pts);
                     uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-                    rotate_words(wv, R);
+                    rotate_words(wv, rot[u] >> 2);
+                    const uint32_t sh = 8u * (rot[u] & 3u);
 #pragma unroll
                     for (int i = 0; i < 8; i++) x[u][i] = __funnelshift_r(wv[i], wv[(i + 1) & 7], sh);
                 }
@@ -1241,10 +1394,11 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
                 for (int st = 0; st < 32; st += 2) {
 #pragma unroll
                     for (int u = 0; u < CPT; u++) {
-                        // one PRMT builds the byte offset c*256 + lane*4 (code byte -> byte 1,
-                        // the lane's column byte -> byte 0); the step's column is the immediate
-                        const uint32_t a0 = __byte_perm(x[u][st >> 2], lane4, 0x5504u | ((st & 3) << 4));
-                        const uint32_t a1 = __byte_perm(x[u][st >> 2], lane4, 0x5504u | (((st + 1) & 3) << 4));
+                        // one PRMT builds the byte offset c*256 + rot*4 (code byte -> byte 1,
+                        // the column byte -> byte 0); the step's column is the immediate
+                        const uint32_t c4 = 4u * rot[u];
+                        const uint32_t a0 = __byte_perm(x[u][st >> 2], c4, 0x5504u | ((st & 3) << 4));
+                        const uint32_t a1 = __byte_perm(x[u][st >> 2], c4, 0x5504u | (((st + 1) & 3) << 4));
                         add_f32x2(sum[u], sum1[u], reinterpret_cast<const float*>(L + a0)[st],
                                   reinterpret_cast<const float*>(L + a1)[st + 1]);
                     }
@@ -1269,14 +1423,12 @@ __global__ void __launch_bounds__(NT, scan_compacts(G, CPT) ? 2 : 1) k_scan_fast
             kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
             kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
             nf += __shfl_xor_sync(0xffffffffu, nf, o);
-            zi += __shfl_xor_sync(0xffffffffu, zi, o);
         }
         if (lane == 0 && nf) {
             atomicMin(&w.mm[2 * qq], kmin);
             atomicMax(&w.mm[2 * qq + 1], kmax);
             atomicAdd(&w.nfin[qq], nf);
         }
-        if (lane == 0 && zi) atomicAdd(&w.zin[qq], zi);
         __syncthreads();
     }
 }
@@ -1287,7 +1439,6 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
     uint32_t* s_pre = reinterpret_cast<uint32_t*>(s_lut + G * kCodes * 32);
     uint32_t* s_start = s_pre + Ps + 1;
     __shared__ ScanShared s;
-    __shared__ uint32_t s_warp[32];
     __shared__ float s_box[2 * kMaxDims];
     const int t = threadIdx.x, lane = t & 31;
     const uint32_t n_items = w.item_off[q];
@@ -1327,7 +1478,7 @@ __global__ void __launch_bounds__(512) k_scan_generic(IndexDev D, int G, int Ps,
                 for (int e = t; e < G * kCodes * 32; e += blockDim.x) s_lut[e] = src[e];
             }
             if (t < 2 * lbl) s_box[t] = w.box[(uint64_t)qq * 2 * lbl + t];
-            scan_load_query(w, Ps, qq, s_pre, s_start, s_warp);
+            scan_load_query(w, Ps, qq, s_pre, s_start);  // ends with a barrier
             cur = qq;
         }
         const uint32_t e1 = min(total, e0 + w.chunk);
@@ -1435,23 +1586,18 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     __shared__ uint32_t s_below, s_cntb, s_out, s_nb, s_bmin, s_bmax, s_need;
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
-    // A predicate-first query of the compacting scan has a compact row: its survivors' distances
+    // A predicate-first query of the predicate pass has a compact row: its survivors' distances
     // in arrival order with their candidate positions beside them (cand_count entries); any
     // other query's row holds one distance per candidate position.
-    const bool compact = w.surv_list && q_prefilter(w, qi);
+    const bool compact = compacts(w, qi);
     const uint32_t total = compact ? w.cand_count[qi] : w.qstat[qi * 4];
     const float* dist = w.dist + w.qoff[qi];
     const uint32_t* prow = compact ? w.spos + w.qoff[qi] : nullptr;
-    for (int i = t; i < Ps; i += blockDim.x) {
-        s_pre[i] = w.range_len[qi * Ps + i];
-        s_start[i] = w.range_start[qi * Ps + i];
-    }
-    if (t == 0) {
-        s_pre[Ps] = 0;
-        s_out = 0;
-    }
+    const uint32_t* rpre = w.range_pre + qi * (Ps + 1);
+    for (int i = t; i <= Ps; i += blockDim.x) s_pre[i] = rpre[i];
+    for (int i = t; i < Ps; i += blockDim.x) s_start[i] = w.range_start[qi * Ps + i];
+    if (t == 0) s_out = 0;
     __syncthreads();
-    block_exclusive_scan(s_pre, Ps + 1, s_warp);
     const uint32_t nfin = w.nfin[qi];
     const uint32_t need0 = min((uint32_t)K, nfin);
     uint32_t* sel_dst = sorted_out ? nullptr : w.cand_pool + w.soff[qi];
@@ -2001,15 +2147,18 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     const uint64_t ns = P.is_split ? std::max<uint64_t>(1, P.n_split) : 1;
     w.range_start = (uint32_t*)take("range_start", q * Ps * ns * 4);
     w.range_len = (uint32_t*)take("range_len", q * Ps * ns * 4);
+    w.range_pre = (uint32_t*)take("range_pre", q * (Ps * ns + 1) * 4);
     w.is_split = P.is_split ? 1 : 0;
     w.nsplit = (int)ns;
     w.qstat = (uint32_t*)take("qstat", q * 4 * 4);
     w.scal = (uint64_t*)take("scalars", 8 * 8);
     w.qoff = (uint64_t*)take("qoff", (q + 1) * 8);
     w.item_off = (uint32_t*)take("item_off", (q + 1) * 4);
+    w.pitem_off = (uint32_t*)take("pre_items", (q + 1) * 4);
     w.mm = (uint32_t*)take("minmax", q * 2 * 4);
     w.nfin = (uint32_t*)take("nfin", q * 4);
     w.zin = (uint32_t*)take("morton_in", q * 4);
+    w.zchk = (uint32_t*)take("morton_checked", q * 4);
     w.counter = (uint32_t*)take("counter", 16);
     w.lut16 = P.lut_fp16 != 0;
     w.lut = (float*)take("lut", q * G * kCodes * 32 * (w.lut16 ? 2 : 4));
@@ -2320,6 +2469,9 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
         reserve_ctx(idx, cx, q);
     }
     Workspace w = carve(idx, cx, q, true);
+    const uint32_t G = lut_groups(D);
+    const bool fast = (D.M % 32 == 0) && G <= 3;
+    w.surv_list = fast ? 1 : 0;  // the fast path lists the predicate-first queries' survivors
     w.qk = c.qk;
     w.qps = c.qps;
     w.qsched = c.qsched;
@@ -2410,8 +2562,6 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     w.rpart = static_cast<uint64_t*>(cx.part_buf.ptr);
     tm.mark("budget");
 
-    const uint32_t G = lut_groups(D);
-    const bool fast = (D.M % 32 == 0) && G <= 3;
     {
         if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
             const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
@@ -2432,19 +2582,39 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     const int R = Ps * w.nsplit;
     const size_t sm_tab = sizeof(uint32_t) * (2 * R + 1);
     if (!sync_sizing || sc[3] > 0) {
+        if (fast && (pre || w.qsched)) {
+            // the predicate pass of the predicate-first queries, then the ADC items that
+            // follow from their survivors
+            const bool lab4 = l == 4 && (reinterpret_cast<uintptr_t>(D.labels) & 15) == 0;
+            auto launch_pre = [&](auto kern) {
+                const int blocks = sm_count() * occupancy_blocks(kern, kPreThreads, 0);
+                kern<<<blocks, kPreThreads, 0, st>>>(D, idx->grid, R, l, q, w);
+            };
+            if (D.pack_bytes == 2) {
+                if (lab4) launch_pre(k_pre_scan<uint16_t, true>);
+                else launch_pre(k_pre_scan<uint16_t, false>);
+            } else if (D.pack_bytes == 8) {
+                if (lab4) launch_pre(k_pre_scan<uint64_t, true>);
+                else launch_pre(k_pre_scan<uint64_t, false>);
+            } else {  // 4 bytes, or no packed cells (the pass then reads labels only)
+                if (lab4) launch_pre(k_pre_scan<uint32_t, true>);
+                else launch_pre(k_pre_scan<uint32_t, false>);
+            }
+            CK_LAUNCH();
+            k_scan_plan<<<1, 1024, 0, st>>>(q, w);
+            CK_LAUNCH();
+            launches += 2;
+            tm.mark("predicate");
+        }
         if (fast) {
             // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
             const int cpt = (P.scan_cpt == 1 || P.scan_cpt == 2 || P.scan_cpt == 4) ? (int)P.scan_cpt : 1;
-            size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
-            // the compacting variant (one group, one candidate per thread, 512 threads) adds the
-            // per-lane survivor queues: 2 x kPreQueue words per thread, 16-byte aligned
-            if (scan_compacts((int)G, cpt)) sm += 16 + sizeof(uint32_t) * 2 * kPreQueue * 512;
-            w.surv_list = scan_compacts((int)G, cpt) ? 1 : 0;
+            const size_t sm = sizeof(float) * G * kCodes * 64 + sm_tab;
             HDG_REQUIRE(sm <= 227 * 1024, HDG_ERR_UNSUPPORTED, "scan tables exceed shared memory");
             auto launch = [&](auto kern, int nt) {
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 const int blocks = sm_count() * occupancy_blocks(kern, nt, sm);
-                kern<<<blocks, nt, sm, st>>>(D, c.queries, R, pre, l, q, w, idx->grid);
+                kern<<<blocks, nt, sm, st>>>(D, R, q, w);
             };
             if (G == 1) {
                 if (cpt == 1) launch(k_scan_fast<1, 512, 1>, 512);

@@ -224,7 +224,9 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
 /* Copy a named intermediate buffer of the last query to host memory (parity tests).
  * Names: "box", "cells", "zrange", "list_counts", "cluster_counts", "probe_clusters",
  * "probe_lists", "range_start", "range_len", "cand_count", "budget", "sel_off", "scalars",
- * "qoff", "qstat", "distances" (the f32 ADC distance of every scanned candidate, query rows
+ * "qoff", "qstat", "morton_in" (candidates of the predicate pass whose labels were read),
+ * "morton_checked" (candidates of the predicate pass whose packed cell was read),
+ * "distances" (the f32 ADC distance of every scanned candidate, query rows
  * at the "qoff" offsets) and "cand_pool" (each query's selected candidates, rows at the
  * "sel_off" offsets, "cand_count" of them). */
 hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,
@@ -241,6 +243,8 @@ typedef struct hdg_index_info {
     int32_t morton_dims, morton_max_bits, morton_valid_map, diff_dim;
     uint64_t device_bytes;
     uint64_t prefix_entries;  /* change points of the compressed prefix rows; 0 = dense form */
+    uint64_t cell_pack_bytes; /* bytes per point of the packed cell coordinates that the predicate
+                               * pass reads (2, 4 or 8; 0 = too wide, not kept) */
 } hdg_index_info;
 hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out);
 

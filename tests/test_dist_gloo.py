@@ -53,17 +53,22 @@ def test_two_rank_max_timing_and_replica_value():
 
 
 def test_algorithmic_scan_bytes():
-    # post-filter query: M code bytes per candidate; predicate-first: 4*l label bytes per
-    # candidate plus M code bytes per survivor
+    # predicate inside the ADC scan: a post-filter query reads M code bytes per candidate, a
+    # predicate-first one 4*l label bytes per candidate plus M code bytes per survivor
     sys.path.insert(0, str(ROOT))
     import bench
     got = bench.algorithmic_scan_bytes([1000, 2000, 0], [900, 10, 0], [False, True, True], M=32, l=4)
-    assert got == 1000 * 32 + (2000 * 16 + 10 * 32)
+    assert got == (0.0, 1000 * 32 + (2000 * 16 + 10 * 32))
 
 
-def test_algorithmic_scan_bytes_with_morton_precheck():
+def test_algorithmic_scan_bytes_of_the_predicate_pass():
     import bench
-    # predicate-first query: 8 bytes of Morton code per candidate, labels only for the 300
-    # candidates inside the cell box, codes for the 10 survivors; post-filter unchanged
-    got = bench.algorithmic_scan_bytes([1000, 2000], [900, 10], [False, True], M=32, l=4, zin_q=[0, 300])
-    assert got == 1000 * 32 + (2000 * 8 + 300 * 16 + 10 * 32)
+    # the predicate pass reads the 2-byte packed cells of the 2000 checked candidates and the
+    # labels of the 300 inside the cell box; the ADC scan reads the codes of the 10 survivors
+    # and of every candidate of the post-filter query
+    got = bench.algorithmic_scan_bytes([1000, 2000], [900, 10], [False, True], M=32, l=4, read_q=[0, 300],
+                                       chk_q=[0, 2000], cbytes=2)
+    assert got == (2000 * 2 + 300 * 16, 1000 * 32 + 10 * 32)
+    # no cell check (most candidates in the box): labels for all, no cells
+    got = bench.algorithmic_scan_bytes([2000], [10], [True], M=32, l=4, read_q=[2000], chk_q=[0], cbytes=4)
+    assert got == (2000 * 16, 10 * 32)

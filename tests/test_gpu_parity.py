@@ -94,7 +94,7 @@ def test_gpu_bruteforce_matches_fp64_oracle(cuda):
 
 # ---- end-to-end parity on the GPU-built index --------------------------------------------
 
-def _parity(ws, cuda, min_recall=None, exact_ids=False, adc_rotated=False):
+def _parity(ws, cuda, min_recall=None, exact_ids=False, adc_rotated=False, layout=True):
     import hdgrid_b200 as hg
     import oracle
     k = ws["k"]
@@ -103,7 +103,9 @@ def _parity(ws, cuda, min_recall=None, exact_ids=False, adc_rotated=False):
     nq = ws["queries"].shape[0]
     tr = fetch_trace(idx, nq)
     ora, path = save_and_open_oracle(idx)
-    assert ora.check_layout() == 0, "pool layout / Morton codes / prefix counts differ from the labels"
+    # (the layout check recounts a dense [cells x lists] prefix table: small grids only)
+    if layout:
+        assert ora.check_layout() == 0, "pool layout / Morton codes / prefix counts differ from the labels"
     o_dist, o_ids, otr = ora.query(ws["queries"], ws["query_labels"], ws["base"], k, adc_rotated=adc_rotated)
     for name in ("box", "cells", "zrange", "list_counts", "probe_clusters", "probe_lists", "range_start",
                  "range_len"):
@@ -180,16 +182,43 @@ def test_parity_prefilter_rotated_adc(cuda):
 
 
 def test_parity_prefilter_compacted_scan(cuda):
-    # M = 32 (one subspace group): predicate-first queries run the compacting scan -- the
-    # survivors queue per lane and their ADC runs in full warps, each sum formed by the lane
-    # of its position -- so ids and ADC distances still equal the oracle's bit for bit
+    # M = 32 (one subspace group): the predicate pass lists each predicate-first query's
+    # survivors (Morton-code pre-check, then the labels) in arrival order, and the ADC scan sums
+    # each survivor from the subspace of its recorded position -- so ids and ADC distances
+    # still equal the oracle's bit for bit
     ws = datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
                           max_grids=4096, exps0=1)
-    _, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
+    idx, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
     valid = r["g_ids"] != INV
     assert valid.any()
     assert np.array_equal(r["g_ids"], r["o_ids"])
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+    # every candidate's labels or Morton code were read, and the Morton check skipped some labels
+    nq = ws["queries"].shape[0]
+    cand = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:nq, 0]
+    read = np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq]
+    chk = np.frombuffer(idx.debug_fetch("morton_checked").tobytes(), np.uint32)[:nq]
+    assert np.all((chk == cand) | ((chk == 0) & (read == cand)))
+    assert np.all(read <= cand) and read.sum() < cand.sum()
+
+
+def test_parity_prefilter_cell_pack_widths(cuda):
+    # the predicate pass tests each candidate's packed cell coordinates (one guarded field per
+    # dim, 2 or 4 bytes here) against the query's cell box; every width and grid gives the
+    # oracle's ids and distances bit for bit
+    seen = set()
+    for max_grids in (4096, 20_000, 30_000_000):
+        ws = datasets.config2(scale=0.01, n_queries=120, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                              max_grids=max_grids, exps0=1)
+        idx, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True, layout=max_grids <= 300_000)
+        info = idx.info()
+        bits = sum((d - 1).bit_length() + 1 for d in info["grid_dims"] if d > 1)
+        assert info["cell_pack_bytes"] == (2 if bits <= 16 else 4 if bits <= 32 else 8), (bits, info)
+        seen.add(info["cell_pack_bytes"])
+        valid = r["g_ids"] != INV
+        assert np.array_equal(r["g_ids"], r["o_ids"])
+        assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
+    assert seen == {2, 4}, seen
 
 
 def test_parity_prefilter_rotated_adc_fp16_lut(cuda):
