@@ -269,6 +269,98 @@ __device__ __forceinline__ void block_bitonic_sort(uint64_t* keys, int n) {
     }
 }
 
+// Stable in-place compaction of the keys that are not ~0 to the front of keys[0, n) (the
+// rest set to ~0); all threads of the block.  s_wc: 32 words of shared scratch.
+__device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32_t* s_wc) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    uint32_t base = 0;
+    for (int r = 0; r < n; r += blockDim.x) {
+        const int e = r + t;
+        const uint64_t v = e < n ? keys[e] : ~0ull;
+        const bool f = v != ~0ull;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) s_wc[warp] = __popc(bal);
+        __syncthreads();  // every read of this round is done before any write
+        uint32_t off = 0, tot = 0;
+        for (int i = 0; i < nw; i++) {
+            const uint32_t c = s_wc[i];
+            off += i < warp ? c : 0u;
+            tot += c;
+        }
+        // the destination is below r + blockDim.x: no later round's key is overwritten
+        if (f) keys[base + off + __popc(bal & ((1u << lane) - 1u))] = v;
+        __syncthreads();
+        base += tot;
+    }
+    for (int e = (int)base + t; e < n; e += blockDim.x) keys[e] = ~0ull;
+    __syncthreads();
+}
+
+// The k smallest keys of keys[0, n) (the keys other than ~0 distinct, at least k of them):
+// compacted to keys[0, k) in their original relative order, the rest set to ~0; returns the
+// k-th smallest.  A radix select over 8-bit digits from the most significant one, stopping
+// once one key is left in the chosen digit's bin, then one compaction.  All threads; s_hist:
+// 256 words, s_wc: 32 words, s_sel: 4 words of shared scratch.
+__device__ __forceinline__ uint64_t block_select_smallest(uint64_t* keys, int n, int k, uint32_t* s_hist, uint32_t* s_wc,
+                                          unsigned long long* s_sel) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    uint64_t prefix = 0, pmask = 0;
+    uint32_t need = (uint32_t)k, cnt = 0;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = t; i < 256; i += blockDim.x) s_hist[i] = 0;
+        __syncthreads();
+        for (int i = t; i < n; i += blockDim.x) {
+            const uint64_t v = keys[i];
+            if (v != ~0ull && (v & pmask) == prefix) atomicAdd(&s_hist[(v >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (warp == 0) {  // lane l scans bins 8l .. 8l + 7
+            uint32_t c[8], sum = 0;
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                c[b] = s_hist[8 * lane + b];
+                sum += c[b];
+            }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+            if (run < need && need <= incl) {
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    if (run < need && need <= run + c[b]) {
+                        s_sel[0] = (unsigned long long)(8 * lane + b);
+                        s_sel[1] = need - run;
+                        s_sel[2] = c[b];
+                    }
+                    run += c[b];
+                }
+            }
+        }
+        __syncthreads();
+        prefix |= (uint64_t)s_sel[0] << shift;
+        pmask |= 255ull << shift;
+        need = (uint32_t)s_sel[1];
+        cnt = (uint32_t)s_sel[2];
+        if (cnt == 1) break;  // one key left with this prefix: the k-th
+    }
+    __syncthreads();  // every thread has read s_sel
+    for (int i = t; i < n; i += blockDim.x) {
+        const uint64_t v = keys[i];
+        if (v != ~0ull && (v & pmask) == prefix) s_sel[3] = v;
+    }
+    __syncthreads();
+    const uint64_t kth = s_sel[3];
+    for (int i = t; i < n; i += blockDim.x)
+        if (keys[i] > kth) keys[i] = ~0ull;
+    __syncthreads();
+    block_compact_keys(keys, n, s_wc);
+    return kth;
+}
+
 __device__ __forceinline__ uint32_t next_pow2_dev(uint32_t x) {
     return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
 }

@@ -54,6 +54,8 @@ __global__ void __launch_bounds__(256) k_features(IndexDev D, GridMeta g, const 
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);         // [sort_n]
     float* s_q = reinterpret_cast<float*>(s_keys + sort_n);        // [d]
     __shared__ float s_f[kMlpFeatures];
+    __shared__ uint32_t s_hist[256], s_wc[32];
+    __shared__ unsigned long long s_sel[4];
     __shared__ unsigned long long s_tot;
     __shared__ unsigned s_nz;
     const uint64_t qi = blockIdx.x;
@@ -107,7 +109,10 @@ __global__ void __launch_bounds__(256) k_features(IndexDev D, GridMeta g, const 
     atomicAdd(&s_tot, tot);
     atomicAdd(&s_nz, nz);
     __syncthreads();
-    block_bitonic_sort(s_keys, sort_n);
+    // the 16 nearest centroids (keys distinct: the centroid index is their low word), in order
+    const int kn = min(16, C);
+    block_select_smallest(s_keys, sort_n, kn, s_hist, s_wc, s_sel);
+    block_bitonic_sort(s_keys, (int)next_pow2_dev((uint32_t)max(kn, 2)));
     const float lnN = logf(1.f + (float)D.n);
     if (t < 16) {
         const int j = min(t, C - 1);

@@ -361,46 +361,6 @@ __device__ __forceinline__ void lower_bound_u64_multi(const uint64_t* const (&a)
     for (int i = 0; i < N; i++) r[i] = lo[i];
 }
 
-// Stable in-place compaction of the keys that are not ~0 to the front of keys[0, n) (the
-// rest set to ~0); all threads of the block.  s_wc: 32 words of shared scratch.
-__device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32_t* s_wc) {
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    uint32_t base = 0;
-    for (int r = 0; r < n; r += blockDim.x) {
-        const int e = r + t;
-        const uint64_t v = e < n ? keys[e] : ~0ull;
-        const bool f = v != ~0ull;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) s_wc[warp] = __popc(bal);
-        __syncthreads();  // every read of this round is done before any write
-        uint32_t off = 0, tot = 0;
-        for (int i = 0; i < nw; i++) {
-            const uint32_t c = s_wc[i];
-            off += i < warp ? c : 0u;
-            tot += c;
-        }
-        // the destination is below r + blockDim.x: no later round's key is overwritten
-        if (f) keys[base + off + __popc(bal & ((1u << lane) - 1u))] = v;
-        __syncthreads();
-        base += tot;
-    }
-    for (int e = (int)base + t; e < n; e += blockDim.x) keys[e] = ~0ull;
-    __syncthreads();
-}
-
-// Sorts keys[0, n) (n a power of two) of which at most nvalid are not ~0: when a shorter sort
-// suffices, the valid keys are first compacted to the front (stably, the rest set to ~0) and
-// only next_pow2(nvalid) of them are sorted -- the same result as sorting all n.  All threads.
-__device__ __forceinline__ void block_sort_valid(uint64_t* keys, int n, int nvalid, uint32_t* s_wc) {
-    const int n2 = (int)next_pow2_dev((uint32_t)max(nvalid, 2));
-    if (n2 < n) {
-        block_compact_keys(keys, n, s_wc);
-        block_bitonic_sort(keys, n2);
-    } else {
-        block_bitonic_sort(keys, n);
-    }
-}
-
 // One sub-range of a probed list's Morton interval [lo, hi) when is_split = 1.
 // get_query_end_points_kernel (zorder.cu:596-654) cuts the interval into
 // min(len, n_split) near-equal parts; zorder_range_query_kernel (:474-594) then moves each
@@ -464,6 +424,8 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
     __shared__ uint32_t s_red[2];
     __shared__ uint32_t s_wc[32];
     __shared__ unsigned long long s_scan[32];
+    __shared__ uint32_t s_hist[256];
+    __shared__ unsigned long long s_sel[4];
     __shared__ int s_nvalid;
     __shared__ float s_bound;
     const uint64_t qi = blockIdx.x;
@@ -495,8 +457,8 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
             s_keys[c] = key;
         }
         __syncthreads();
-        block_sort_valid(s_keys, sort_n1, s_nvalid, s_wc);
-        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Pc - 1] >> 32));
+        const uint64_t kth = block_select_smallest(s_keys, sort_n1, Pc, s_hist, s_wc, s_sel);
+        if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
         __syncthreads();
     }
     for (int c = t; c < sort_n1; c += blockDim.x) {
@@ -516,9 +478,10 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
         s_keys[c] = key;
     }
     __syncthreads();
-    // with every non-empty cluster taken the keys hold no distance: cluster order, compacted
+    // with every non-empty cluster taken the keys hold no distance: cluster order, compacted;
+    // otherwise the n_list smallest (distance, cluster) keys, a set in no particular order
     if (all_c) block_compact_keys(s_keys, sort_n1, s_wc);
-    else block_sort_valid(s_keys, sort_n1, s_nvalid, s_wc);
+    else block_select_smallest(s_keys, sort_n1, Pc, s_hist, s_wc, s_sel);
     const int npc = min(Pc, s_nvalid);
     for (int i = t; i < Pc; i += blockDim.x) {
         const uint32_t c = i < npc ? (uint32_t)s_keys[i] : kInvalid;
@@ -555,8 +518,8 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
             s_keys[e] = key;
         }
         __syncthreads();
-        block_sort_valid(s_keys, sort_n2, s_nvalid, s_wc);
-        if (t == 0) s_bound = key_float((uint32_t)(s_keys[Psq - 1] >> 32));
+        const uint64_t kth = block_select_smallest(s_keys, sort_n2, Psq, s_hist, s_wc, s_sel);
+        if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
         __syncthreads();
     }
     for (int e = t; e < sort_n2; e += blockDim.x) {
@@ -582,14 +545,13 @@ __global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, con
         s_keys[e] = key;
     }
     __syncthreads();
-    // every list taken and every cluster taken (chosen clusters in cluster order): the keys are
-    // already in list-id order and only need compacting; otherwise the sort orders them
-    if (all_l && all_c) block_compact_keys(s_keys, sort_n2, s_wc);
-    else block_sort_valid(s_keys, sort_n2, s_nvalid, s_wc);
+    // every list taken: the keys carry no distance, compacted (in list-id order when the chosen
+    // clusters are in cluster order too); otherwise the sub_lists smallest (distance, list) keys
+    if (all_l) block_compact_keys(s_keys, sort_n2, s_wc);
+    else block_select_smallest(s_keys, sort_n2, Psq, s_hist, s_wc, s_sel);
     const int nps = min(Psq, s_nvalid);
     // the probed lists in list-id (= pool) order, so candidate positions follow pool order
-    // (with every list taken the keys carry no distance and are in list-id order already)
-    if (!all_l) {
+    if (!(all_l && all_c)) {
         const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
         for (int i = t; i < sort_n3; i += blockDim.x)
             s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
@@ -960,6 +922,7 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
 // The row's order depends on timing; the distance of each survivor does not (the ADC order
 // follows its position) and the select orders ties by position.
 constexpr int kPreThreads = 256;
+constexpr int kPreRingWords = 2 * 512 + 2 * 256;  // shared words per warp
 
 // Largest i in [0, n) with a[i] <= key (a nondecreasing, a[0] <= key), by 32-way rounds.
 // Every lane of the warp calls it and gets the answer.
@@ -978,56 +941,55 @@ __device__ __forceinline__ int warp_find_le(const uint32_t* a, int n, uint32_t k
     return lo;
 }
 
-// Appends (a, b) of the lanes where f holds to a per-warp buffer ([0, 64) first words, [64,
-// 128) second words) that holds n entries (warp-uniform, n < 32 on entry).
-__device__ __forceinline__ void warp_push(uint32_t* buf, int& n, bool f, uint32_t a, uint32_t b) {
+// Per-warp rings in shared memory: word i of entry s at ring[i * size + s], head h and tail t
+// warp-uniform and free-running (entries t - h).
+
+// Appends (a, b) of the lanes where f holds at the ring's tail.  All lanes.
+template <uint32_t SIZE>
+__device__ __forceinline__ void ring_push(uint32_t* ring, uint32_t& t, bool f, uint32_t a, uint32_t b) {
     const unsigned bal = __ballot_sync(0xffffffffu, f);
     if (f) {
-        const int s = n + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
-        buf[s] = a;
-        buf[64 + s] = b;
+        const uint32_t s = (t + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u))) & (SIZE - 1);
+        ring[s] = a;
+        ring[SIZE + s] = b;
     }
-    n += __popc(bal);
+    t += __popc(bal);
 }
 
-// Drops the first 32 of the buffer's n entries (32 <= n < 64).
-__device__ __forceinline__ void warp_drop32(uint32_t* buf, int& n) {
-    const int lane = threadIdx.x & 31;
-    __syncwarp();
-    const bool mv = lane < n - 32;
-    uint32_t a = 0, b = 0;
-    if (mv) {
-        a = buf[32 + lane];
-        b = buf[96 + lane];
-    }
-    __syncwarp();
-    if (mv) {
-        buf[lane] = a;
-        buf[64 + lane] = b;
-    }
-    __syncwarp();
-    n -= 32;
-}
-
-// One predicate-pass work item: positions [e0, e1) of one query.  PT: the packed cell type,
-// CHECK: test the cell box first (lo_f / hi_g / gd: the box's low fields, its high fields with
-// the guard bits set, the guard bits), LAB4: four 16-byte-aligned label dims in registers.
+// One predicate-pass work item: positions [e0, e1) of one query (R ranges, prefix pre, starts
+// start; r0 the range of e0).  PT: the packed cell type, CHECK: test the cell box first (lo_f /
+// hi_g / gd: the box's low fields, its high fields with the guard bits set, the guard bits),
+// LAB4: four 16-byte-aligned label dims in registers.  qr: [2][512] ring (cell-passed
+// candidates; without CHECK the survivors), sr: [2][256] survivor ring.  n_chk / n_read:
+// candidates whose cell / labels were read (warp totals).
 template <typename PT, bool CHECK, bool LAB4>
 __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float* bx_s, PT lo_f, PT hi_g, PT gd,
-                                         const uint32_t* pre, const uint32_t* start, int r0, uint32_t e0,
-                                         uint32_t e1, uint32_t* qb, uint32_t* sb, uint32_t* ctr, uint32_t* drow,
+                                         const uint32_t* pre, const uint32_t* start, int R, int r0, uint32_t e0,
+                                         uint32_t e1, uint32_t* qr, uint32_t* sr, uint32_t* ctr, uint32_t* drow,
                                          uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
-    constexpr int J = 8;  // positions per lane in one step
+    constexpr int J = 8;  // windows of 32 positions in one step
+    constexpr uint32_t QS = 512, SS = 256;
     const int lane = threadIdx.x & 31;
     float bx[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) bx[i] = LAB4 ? bx_s[i] : 0.f;
     const PT* cells = static_cast<const PT*>(D.cellpack);
     const float4* lab4 = reinterpret_cast<const float4*>(D.labels);
-    // the lane's walk over the query's ranges: positions only grow along it
-    int rr = r0;
-    uint32_t nb = pre[rr + 1], base = start[rr] - pre[rr];
-    int qn = 0, sn = 0;
+    // Position -> pool row (warp-uniform state): the current range rc holds positions up to
+    // nb1 (pool row = bc + position), the next non-empty range from nb1 up to nb2 (bn).  A
+    // window of 32 positions with at most one range start inside reads the two bases; a window
+    // with more (ranges shorter than 32) walks per lane.
+    int rc = r0, rn = r0;
+    uint32_t nb1 = pre[r0 + 1], bc = start[r0] - pre[r0], nb2 = 0xffffffffu, bn = 0;
+    auto find_next = [&]() {  // the first non-empty range after rc
+        int r = rc + 1;
+        while (r < R && pre[r + 1] == nb1) r++;
+        rn = r;
+        nb2 = r < R ? pre[r + 1] : 0xffffffffu;
+        bn = r < R ? start[r] - nb1 : 0u;
+    };
+    find_next();
+    uint32_t qh = 0, qt = 0, sh = 0, st = 0;
     // the label predicate of the candidate at pool row p (a NaN label passes, as in the reference)
     auto label_ok = [&](uint32_t p) -> bool {
         if (LAB4) {
@@ -1043,46 +1005,89 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         }
         return ok;
     };
-    // the first m (<= 32) staged survivors to the row
-    auto flush = [&](int m) {
+    // m (<= 32) entries from a ring's head to the query's row: position into spos, pool row
+    // into the distance slot
+    auto flush = [&](const uint32_t* ring, uint32_t size, uint32_t h, int m) {
         __syncwarp();
         uint32_t at = 0;
         if (lane == 0) at = atomicAdd(ctr, (uint32_t)m);
         at = __shfl_sync(0xffffffffu, at, 0);
         if (lane < m) {
-            prow[at + lane] = sb[lane];
-            drow[at + lane] = sb[64 + lane];
+            const uint32_t s = (h + lane) & (size - 1);
+            prow[at + lane] = ring[s];
+            drow[at + lane] = ring[size + s];
         }
+        __syncwarp();
     };
-    auto stage = [&](bool f, uint32_t e, uint32_t p) {
-        warp_push(sb, sn, f, e, p);
-        if (sn >= 32) {
-            flush(32);
-            warp_drop32(sb, sn);
-        }
-    };
-    // label tests of the first m (<= 32) queued candidates, one per lane
+    // label tests of m (<= 128) cell-passed candidates from qr's head, four per lane with their
+    // label loads in flight together; survivors to sr, which is flushed 32 at a time
     auto label_round = [&](int m) {
         __syncwarp();
-        const bool v = lane < m;
-        const uint32_t e = v ? qb[lane] : 0u, p = v ? qb[64 + lane] : 0u;
-        stage(v && label_ok(p), e, p);
+        uint32_t e[4], p[4];
+        bool v[4], ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            v[u] = lane + 32 * u < m;
+            const uint32_t s = (qh + lane + 32u * u) & (QS - 1);
+            e[u] = v[u] ? qr[s] : 0u;
+            p[u] = v[u] ? qr[QS + s] : 0u;
+        }
+        if (LAB4) {
+            float4 x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) x[u] = v[u] ? __ldg(lab4 + p[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                ok[u] = v[u] && !(x[u].x < bx[0] || x[u].x > bx[1]) && !(x[u].y < bx[2] || x[u].y > bx[3]) &&
+                        !(x[u].z < bx[4] || x[u].z > bx[5]) && !(x[u].w < bx[6] || x[u].w > bx[7]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; u++) ok[u] = v[u] && label_ok(p[u]);
+        }
+        qh += (uint32_t)m;
+#pragma unroll
+        for (int u = 0; u < 4; u++) ring_push<SS>(sr, st, ok[u], e[u], p[u]);
+        while (st - sh >= 32) {
+            flush(sr, SS, sh, 32);
+            sh += 32;
+        }
     };
     for (uint32_t eb = e0; eb < e1; eb += 32u * J) {
+        // label tests of the earlier steps' queue, 128 at a time
+        if (CHECK)
+            while (qt - qh >= 128) label_round(128);  // then fewer than 128 queued: room for a step
         uint32_t pp[J];
         bool pv[J];
+        const uint32_t last = min(e1, eb + 32u * J) - 1;  // the step's last position
+        if (last < nb1) {  // the whole step inside the current range
 #pragma unroll
-        for (int j = 0; j < J; j++) {
-            const uint32_t e = eb + lane + 32u * j;
-            pv[j] = e < e1;
-            pp[j] = 0;
-            if (pv[j]) {
-                while (nb <= e) {
-                    rr++;
-                    nb = pre[rr + 1];
-                    base = start[rr] - pre[rr];
+            for (int j = 0; j < J; j++) {
+                const uint32_t e = eb + 32u * j + lane;
+                pv[j] = e < e1;
+                pp[j] = pv[j] ? bc + e : 0u;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                const uint32_t p = eb + 32u * j, e = p + lane;  // the window [p, p + 32)
+                pv[j] = e < e1;
+                uint32_t base;
+                if (p + 31u < nb2) {
+                    base = e < nb1 ? bc : bn;
+                } else {  // two or more ranges start inside the window
+                    int r = rc;
+                    if (pv[j])
+                        while (pre[r + 1] <= e) r++;
+                    base = start[r] - pre[r];
                 }
-                pp[j] = base + e;
+                pp[j] = pv[j] ? base + e : 0u;
+                // on to the range of the next window's first position
+                while (nb1 <= p + 32u && nb1 < e1) {
+                    rc = rn;
+                    nb1 = nb2;
+                    bc = bn;
+                    find_next();
+                }
             }
         }
         if constexpr (CHECK) {
@@ -1091,52 +1096,59 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
             for (int j = 0; j < J; j++) c[j] = pv[j] ? __ldg(cells + pp[j]) : PT(0);
 #pragma unroll
             for (int j = 0; j < J; j++) {
-                n_chk += pv[j] ? 1u : 0u;
                 // every field at or above its low bound and at or below its high bound: the
                 // guard bit above a field survives both subtractions exactly then
                 const PT t = (PT)((PT)((c[j] | gd) - lo_f) & (PT)(hi_g - c[j]));
-                pv[j] = pv[j] && (PT)(t & gd) == gd;
-                n_read += pv[j] ? 1u : 0u;
-                warp_push(qb, qn, pv[j], eb + lane + 32u * j, pp[j]);
-                if (qn >= 32) {
-                    label_round(32);
-                    warp_drop32(qb, qn);
-                }
-            }
-        } else if (LAB4) {
-            // four 16-byte label loads in flight at a time
-#pragma unroll
-            for (int j0 = 0; j0 < J; j0 += 4) {
-                float4 v[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    v[j] = pv[j0 + j] ? __ldg(lab4 + pp[j0 + j]) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    n_read += pv[j0 + j] ? 1u : 0u;
-                    const bool ok = pv[j0 + j] && !(v[j].x < bx[0] || v[j].x > bx[1]) &&
-                                    !(v[j].y < bx[2] || v[j].y > bx[3]) && !(v[j].z < bx[4] || v[j].z > bx[5]) &&
-                                    !(v[j].w < bx[6] || v[j].w > bx[7]);
-                    stage(ok, eb + lane + 32u * (j0 + j), pp[j0 + j]);
-                }
+                ring_push<QS>(qr, qt, pv[j] && (PT)(t & gd) == gd, eb + 32u * j + lane, pp[j]);
             }
         } else {
+            if (LAB4) {
+                // four 16-byte label loads in flight at a time
 #pragma unroll
-            for (int j = 0; j < J; j++) {
-                n_read += pv[j] ? 1u : 0u;
-                stage(pv[j] && label_ok(pp[j]), eb + lane + 32u * j, pp[j]);
+                for (int j0 = 0; j0 < J; j0 += 4) {
+                    float4 v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        v[j] = pv[j0 + j] ? __ldg(lab4 + pp[j0 + j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const bool ok = pv[j0 + j] && !(v[j].x < bx[0] || v[j].x > bx[1]) &&
+                                        !(v[j].y < bx[2] || v[j].y > bx[3]) && !(v[j].z < bx[4] || v[j].z > bx[5]) &&
+                                        !(v[j].w < bx[6] || v[j].w > bx[7]);
+                        ring_push<QS>(qr, qt, ok, eb + 32u * (j0 + j) + lane, pp[j0 + j]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < J; j++)
+                    ring_push<QS>(qr, qt, pv[j] && label_ok(pp[j]), eb + 32u * j + lane, pp[j]);
+            }
+            while (qt - qh >= 32) {
+                flush(qr, QS, qh, 32);
+                qh += 32;
             }
         }
     }
-    if (CHECK && qn > 0) label_round(qn);
-    if (sn > 0) flush(sn);
+    if (CHECK) {
+        n_read += qt;  // every cell-passed candidate had its labels read
+        n_chk += e1 - e0;
+        while (qt != qh) label_round((int)min(128u, qt - qh));
+        if (st != sh) flush(sr, SS, sh, (int)(st - sh));
+    } else {
+        n_read += e1 - e0;
+        while (qt != qh) {
+            const int m = (int)min(32u, qt - qh);
+            flush(qr, QS, qh, m);
+            qh += (uint32_t)m;
+        }
+    }
 }
 
 template <typename PT, bool LAB4>
 __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMeta g, int R, int lbl, uint64_t q,
                                                              Workspace w) {
     constexpr int NW = kPreThreads / 32;
-    __shared__ uint32_t s_qb[NW][128], s_sb[NW][128];  // cell-passed queue, survivor staging
+    extern __shared__ uint32_t s_rings[];  // per warp: [2][512] queue ring, [2][256] survivor ring
     __shared__ float s_bx[NW][2 * kMaxDims];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t n_items = w.pitem_off[q];
@@ -1213,19 +1225,14 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMet
         uint32_t* prow = w.spos + w.qoff[qq];
         uint32_t n_read = 0, n_chk = 0;
         const float* bxs = s_bx[wp];
-        uint32_t* qb = s_qb[wp];
-        uint32_t* sb = s_sb[wp];
+        uint32_t* qr = s_rings + (size_t)wp * kPreRingWords;
+        uint32_t* sr = qr + 2 * 512;
         if (use)
-            pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, r0, e0, e1, qb, sb,
-                                     ctr, drow, prow, n_read, n_chk);
+            pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, R, r0, e0, e1, qr,
+                                     sr, ctr, drow, prow, n_read, n_chk);
         else
-            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, r0, e0, e1, qb, sb, ctr, drow,
-                                      prow, n_read, n_chk);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            n_read += __shfl_xor_sync(0xffffffffu, n_read, o);
-            n_chk += __shfl_xor_sync(0xffffffffu, n_chk, o);
-        }
+            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, ctr,
+                                      drow, prow, n_read, n_chk);
         if (lane == 0 && n_read) atomicAdd(&w.zin[qq], n_read);
         if (lane == 0 && n_chk) atomicAdd(&w.zchk[qq], n_chk);
     }
@@ -2587,8 +2594,10 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
             // follow from their survivors
             const bool lab4 = l == 4 && (reinterpret_cast<uintptr_t>(D.labels) & 15) == 0;
             auto launch_pre = [&](auto kern) {
-                const int blocks = sm_count() * occupancy_blocks(kern, kPreThreads, 0);
-                kern<<<blocks, kPreThreads, 0, st>>>(D, idx->grid, R, l, q, w);
+                const size_t smp = sizeof(uint32_t) * kPreRingWords * (kPreThreads / 32);
+                CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
+                const int blocks = sm_count() * occupancy_blocks(kern, kPreThreads, smp);
+                kern<<<blocks, kPreThreads, smp, st>>>(D, idx->grid, R, l, q, w);
             };
             if (D.pack_bytes == 2) {
                 if (lab4) launch_pre(k_pre_scan<uint16_t, true>);
