@@ -446,6 +446,14 @@ def run_hdgrid(args):
                                                    info["cell_pack_bytes"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
+    # the re-rank: every selected entry's pool -> id lookup (4 B) and, for a post-filter query,
+    # its labels (4*l B); every predicate survivor's full row (4*d B)
+    refine_bytes = None
+    if p0["exps0"] > 1:
+        # after the select, cand_count holds each query's selection size
+        sel_q = np.frombuffer(idx.debug_fetch("cand_count").tobytes(), np.uint32)[:nq].astype(np.float64)
+        rows_q = np.frombuffer(idx.debug_fetch("refine_rows").tobytes(), np.uint32)[:nq].astype(np.float64)
+        refine_bytes = float((sel_q * 4).sum() + (sel_q[~pre_q] * 4 * info["l"]).sum() + (rows_q * 4 * info["d"]).sum())
 
     # end to end through the public API with host buffers
     q_h = torch.from_numpy(ws["queries"]).pin_memory()
@@ -546,6 +554,11 @@ def run_hdgrid(args):
         "gpu_launches": args.steps * launches_per_step,
         "clocks": clk.summary(),
         "stage_ms": stage_ms,
+        "stage_rooflines": ({"refine": {"kernel": "k_refine", "algorithmic_bytes": refine_bytes,
+                                        "kernel_ms": stage_ms.get("refine"),
+                                        "achieved": refine_bytes / (stage_ms["refine"] / 1e3) / 1e9,
+                                        "frac": refine_bytes / (stage_ms["refine"] / 1e3) / 1e9 / peak}}
+                            if refine_bytes and stage_ms.get("refine") else {}),
     }
     if versus is not None:
         line["learned_vs_plain"] = versus

@@ -981,8 +981,9 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     // with more (ranges shorter than 32) walks per lane.
     int rc = r0, rn = r0;
     uint32_t nb1 = pre[r0 + 1], bc = start[r0] - pre[r0], nb2 = 0xffffffffu, bn = 0;
-    auto find_next = [&]() {  // the first non-empty range after rc
-        int r = rc + 1;
+    const uint32_t total = pre[R];
+    auto find_next = [&]() {  // the first non-empty range after rc (none past the last position)
+        int r = nb1 < total ? rc + 1 : R;
         while (r < R && pre[r + 1] == nb1) r++;
         rn = r;
         nb2 = r < R ? pre[r + 1] : 0xffffffffu;
