@@ -922,7 +922,7 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
 // The row's order depends on timing; the distance of each survivor does not (the ADC order
 // follows its position) and the select orders ties by position.
 constexpr int kPreThreads = 256;
-constexpr int kPreRingWords = 2 * 512 + 2 * 256;  // shared words per warp
+constexpr int kPreRingWords = 4 * 128 + 2 * 512 + 2 * 64;  // shared words per warp: labels, queue, survivors
 
 // Largest i in [0, n) with a[i] <= key (a nondecreasing, a[0] <= key), by 32-way rounds.
 // Every lane of the warp calls it and gets the answer.
@@ -956,19 +956,28 @@ __device__ __forceinline__ void ring_push(uint32_t* ring, uint32_t& t, bool f, u
     t += __popc(bal);
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, cached in L2 only) and its groups
+__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // One predicate-pass work item: positions [e0, e1) of one query (R ranges, prefix pre, starts
 // start; r0 the range of e0).  PT: the packed cell type, CHECK: test the cell box first (lo_f /
 // hi_g / gd: the box's low fields, its high fields with the guard bits set, the guard bits),
-// LAB4: four 16-byte-aligned label dims in registers.  qr: [2][512] ring (cell-passed
-// candidates; without CHECK the survivors), sr: [2][256] survivor ring.  n_chk / n_read:
-// candidates whose cell / labels were read (warp totals).
+// LAB4: four 16-byte-aligned label dims.  qr: [2][512] ring of cell-passed candidates (without
+// CHECK: of survivors), sr: [2][64] survivor ring, lst: [128] staged labels (LAB4).  n_chk /
+// n_read: candidates whose cell / labels were read (warp totals).
 template <typename PT, bool CHECK, bool LAB4>
 __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float* bx_s, PT lo_f, PT hi_g, PT gd,
                                          const uint32_t* pre, const uint32_t* start, int R, int r0, uint32_t e0,
-                                         uint32_t e1, uint32_t* qr, uint32_t* sr, uint32_t* ctr, uint32_t* drow,
-                                         uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
+                                         uint32_t e1, uint32_t* qr, uint32_t* sr, float4* lst, uint32_t* ctr,
+                                         uint32_t* drow, uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
     constexpr int J = 8;  // windows of 32 positions in one step
-    constexpr uint32_t QS = 512, SS = 256;
+    constexpr uint32_t QS = 512, SS = 64, LB = 128;
     const int lane = threadIdx.x & 31;
     float bx[8];
 #pragma unroll
@@ -976,9 +985,9 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     const PT* cells = static_cast<const PT*>(D.cellpack);
     const float4* lab4 = reinterpret_cast<const float4*>(D.labels);
     // Position -> pool row (warp-uniform state): the current range rc holds positions up to
-    // nb1 (pool row = bc + position), the next non-empty range from nb1 up to nb2 (bn).  A
-    // window of 32 positions with at most one range start inside reads the two bases; a window
-    // with more (ranges shorter than 32) walks per lane.
+    // nb1 (pool row = bc + position), the next non-empty range from nb1 up to nb2 (bn).  A step
+    // with at most one range start inside reads the two bases; a window with more (ranges
+    // shorter than 32) walks per lane.
     int rc = r0, rn = r0;
     uint32_t nb1 = pre[r0 + 1], bc = start[r0] - pre[r0], nb2 = 0xffffffffu, bn = 0;
     const uint32_t total = pre[R];
@@ -990,14 +999,21 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         bn = r < R ? start[r] - nb1 : 0u;
     };
     find_next();
-    uint32_t qh = 0, qt = 0, sh = 0, st = 0;
+    auto advance_to = [&](uint32_t p) {  // the state at the range of position p
+        while (nb1 <= p && nb1 < e1) {
+            rc = rn;
+            nb1 = nb2;
+            bc = bn;
+            find_next();
+        }
+    };
+    auto box4 = [&](const float4& v) {
+        return !(v.x < bx[0] || v.x > bx[1]) && !(v.y < bx[2] || v.y > bx[3]) && !(v.z < bx[4] || v.z > bx[5]) &&
+               !(v.w < bx[6] || v.w > bx[7]);
+    };
     // the label predicate of the candidate at pool row p (a NaN label passes, as in the reference)
     auto label_ok = [&](uint32_t p) -> bool {
-        if (LAB4) {
-            const float4 v = __ldg(lab4 + p);
-            return !(v.x < bx[0] || v.x > bx[1]) && !(v.y < bx[2] || v.y > bx[3]) && !(v.z < bx[4] || v.z > bx[5]) &&
-                   !(v.w < bx[6] || v.w > bx[7]);
-        }
+        if (LAB4) return box4(__ldg(lab4 + p));
         bool ok = true;
         const float* lab = D.labels + (uint64_t)p * lbl;
         for (int i = 0; i < lbl; i++) {
@@ -1020,53 +1036,66 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         }
         __syncwarp();
     };
-    // label tests of m (<= 128) cell-passed candidates from qr's head, four per lane with their
-    // label loads in flight together; survivors to sr, which is flushed 32 at a time
-    auto label_round = [&](int m) {
-        __syncwarp();
-        uint32_t e[4], p[4];
-        bool v[4], ok[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            v[u] = lane + 32 * u < m;
-            const uint32_t s = (qh + lane + 32u * u) & (QS - 1);
-            e[u] = v[u] ? qr[s] : 0u;
-            p[u] = v[u] ? qr[QS + s] : 0u;
-        }
-        if (LAB4) {
-            float4 x[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = v[u] ? __ldg(lab4 + p[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                ok[u] = v[u] && !(x[u].x < bx[0] || x[u].x > bx[1]) && !(x[u].y < bx[2] || x[u].y > bx[3]) &&
-                        !(x[u].z < bx[4] || x[u].z > bx[5]) && !(x[u].w < bx[6] || x[u].w > bx[7]);
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; u++) ok[u] = v[u] && label_ok(p[u]);
-        }
-        qh += (uint32_t)m;
-#pragma unroll
-        for (int u = 0; u < 4; u++) ring_push<SS>(sr, st, ok[u], e[u], p[u]);
-        while (st - sh >= 32) {
+    uint32_t sh = 0, st = 0;
+    auto stage_surv = [&](bool f, uint32_t e, uint32_t p) {
+        ring_push<SS>(sr, st, f, e, p);
+        if (st - sh >= 32) {
             flush(sr, SS, sh, 32);
             sh += 32;
         }
     };
+    // Label batches (CHECK): qr holds [qh, qi) whose labels are on their way into lst, then
+    // [qi, qt) queued.  issue() starts the next batch's 16-byte label copies (cp.async: no
+    // registers held while they fly), consume() tests a batch once its copies have landed.
+    uint32_t qh = 0, qi = 0, qt = 0;
+    auto issue = [&](uint32_t m) {
+        __syncwarp();  // the pushes of every lane are visible
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = lane + 32u * u;
+            if (LAB4 && k < m) cp16_async(lst + k, lab4 + qr[QS + ((qi + k) & (QS - 1))]);
+        }
+        if (LAB4) cp_commit();
+        qi += m;
+    };
+    auto consume = [&]() {
+        const uint32_t m = qi - qh;
+        if (LAB4) cp_wait<0>();
+        __syncwarp();  // every lane's copies have landed
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = lane + 32u * u;
+            const bool v = k < m;
+            const uint32_t s = (qh + k) & (QS - 1);
+            const uint32_t e = v ? qr[s] : 0u, p = v ? qr[QS + s] : 0u;
+            bool ok = false;
+            if (v) ok = LAB4 ? box4(lst[k]) : label_ok(p);
+            stage_surv(ok, e, p);
+        }
+        qh = qi;
+        __syncwarp();  // lst and the consumed ring slots are free again
+    };
     for (uint32_t eb = e0; eb < e1; eb += 32u * J) {
-        // label tests of the earlier steps' queue, 128 at a time
-        if (CHECK)
-            while (qt - qh >= 128) label_round(128);  // then fewer than 128 queued: room for a step
+        if (CHECK) {
+            // test the batch in flight, start the next one; drain more only when the ring has no
+            // room for this step's pushes
+            for (;;) {
+                if (qi != qh) consume();
+                if (qt - qh >= LB) issue(LB);
+                if (qt - qh <= QS - 32u * J) break;
+            }
+        }
         uint32_t pp[J];
         bool pv[J];
         const uint32_t last = min(e1, eb + 32u * J) - 1;  // the step's last position
-        if (last < nb1) {  // the whole step inside the current range
+        if (last < nb2) {  // at most one range starts inside the step
 #pragma unroll
             for (int j = 0; j < J; j++) {
                 const uint32_t e = eb + 32u * j + lane;
                 pv[j] = e < e1;
-                pp[j] = pv[j] ? bc + e : 0u;
+                pp[j] = pv[j] ? (e < nb1 ? bc : bn) + e : 0u;
             }
+            advance_to(eb + 32u * J);
         } else {
 #pragma unroll
             for (int j = 0; j < J; j++) {
@@ -1082,13 +1111,7 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
                     base = start[r] - pre[r];
                 }
                 pp[j] = pv[j] ? base + e : 0u;
-                // on to the range of the next window's first position
-                while (nb1 <= p + 32u && nb1 < e1) {
-                    rc = rn;
-                    nb1 = nb2;
-                    bc = bn;
-                    find_next();
-                }
+                advance_to(p + 32u);
             }
         }
         if constexpr (CHECK) {
@@ -1112,12 +1135,8 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
                     for (int j = 0; j < 4; j++)
                         v[j] = pv[j0 + j] ? __ldg(lab4 + pp[j0 + j]) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const bool ok = pv[j0 + j] && !(v[j].x < bx[0] || v[j].x > bx[1]) &&
-                                        !(v[j].y < bx[2] || v[j].y > bx[3]) && !(v[j].z < bx[4] || v[j].z > bx[5]) &&
-                                        !(v[j].w < bx[6] || v[j].w > bx[7]);
-                        ring_push<QS>(qr, qt, ok, eb + 32u * (j0 + j) + lane, pp[j0 + j]);
-                    }
+                    for (int j = 0; j < 4; j++)
+                        ring_push<QS>(qr, qt, pv[j0 + j] && box4(v[j]), eb + 32u * (j0 + j) + lane, pp[j0 + j]);
                 }
             } else {
 #pragma unroll
@@ -1133,7 +1152,11 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     if (CHECK) {
         n_read += qt;  // every cell-passed candidate had its labels read
         n_chk += e1 - e0;
-        while (qt != qh) label_round((int)min(128u, qt - qh));
+        for (;;) {
+            if (qi != qh) consume();
+            if (qt == qh) break;
+            issue(min(LB, qt - qh));
+        }
         if (st != sh) flush(sr, SS, sh, (int)(st - sh));
     } else {
         n_read += e1 - e0;
@@ -1149,7 +1172,7 @@ template <typename PT, bool LAB4>
 __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMeta g, int R, int lbl, uint64_t q,
                                                              Workspace w) {
     constexpr int NW = kPreThreads / 32;
-    extern __shared__ uint32_t s_rings[];  // per warp: [2][512] queue ring, [2][256] survivor ring
+    extern __shared__ __align__(16) uint32_t s_rings[];  // per warp: staged labels, queue ring, survivor ring
     __shared__ float s_bx[NW][2 * kMaxDims];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t n_items = w.pitem_off[q];
@@ -1226,14 +1249,15 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMet
         uint32_t* prow = w.spos + w.qoff[qq];
         uint32_t n_read = 0, n_chk = 0;
         const float* bxs = s_bx[wp];
-        uint32_t* qr = s_rings + (size_t)wp * kPreRingWords;
+        float4* lst = reinterpret_cast<float4*>(s_rings + (size_t)wp * kPreRingWords);
+        uint32_t* qr = reinterpret_cast<uint32_t*>(lst + 128);
         uint32_t* sr = qr + 2 * 512;
         if (use)
             pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, R, r0, e0, e1, qr,
-                                     sr, ctr, drow, prow, n_read, n_chk);
+                                     sr, lst, ctr, drow, prow, n_read, n_chk);
         else
-            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, ctr,
-                                      drow, prow, n_read, n_chk);
+            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, lst,
+                                      ctr, drow, prow, n_read, n_chk);
         if (lane == 0 && n_read) atomicAdd(&w.zin[qq], n_read);
         if (lane == 0 && n_chk) atomicAdd(&w.zchk[qq], n_chk);
     }
@@ -1860,6 +1884,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
 // a query with one item writes its output row directly, otherwise every item leaves its
 // best k in the partial buffer and the last item of the query to finish merges them.
 constexpr uint32_t kRefChunk = 4096;
+
 
 __global__ void __launch_bounds__(1024) k_refine_plan(uint64_t q, Workspace w) {
     __shared__ unsigned long long s_w[32];
