@@ -442,8 +442,14 @@ def run_hdgrid(args):
     if pred_pass:
         read_q = np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq].astype(np.uint64)
         chk_q = np.frombuffer(idx.debug_fetch("morton_checked").tobytes(), np.uint32)[:nq].astype(np.uint64)
-    pred_bytes, adc_bytes = algorithmic_scan_bytes(cand_q, pass_q, pre_q, info["M"], info["l"], read_q, chk_q,
-                                                   info["cell_pack_bytes"])
+    # a predicate-first query whose budget takes every survivor needs no ADC (the re-rank
+    # orders them): only the others' survivors are summed
+    adc_q = pre_q.copy()
+    if pred_pass and p0["exps0"] > 1:
+        bud_q = np.frombuffer(idx.debug_fetch("budget").tobytes(), np.uint32)[:nq].astype(np.uint64)
+        adc_q = pre_q & (pass_q > bud_q)
+    pred_bytes, adc_bytes = algorithmic_scan_bytes(cand_q, np.where(pre_q & ~adc_q, 0, pass_q), pre_q, info["M"],
+                                                   info["l"], read_q, chk_q, info["cell_pack_bytes"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
     # the re-rank: every selected entry's pool -> id lookup (4 B) and, for a post-filter query,

@@ -796,7 +796,11 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_z = reserve(H.zcodes.size() * 8), o_id = reserve(H.ids.size() * 4);
     const size_t o_pk = reserve(H.zcodes.size() * pack_bytes);
     const size_t o_code = reserve(H.codes.size() + 64), o_lab = reserve(H.labels.size() * 4);
-    const size_t o_pq = reserve(H.pq_centers.size() * 4), o_pre = reserve(H.prefix.size() * 4);
+    // a dense prefix count never exceeds its list's size: 16 bits suffice when no list passes 65535
+    uint32_t max_list = 0;
+    for (uint64_t j = 0; j + 1 < H.list_off.size(); j++) max_list = std::max(max_list, H.list_off[j + 1] - H.list_off[j]);
+    const bool pre16 = !H.prefix.empty() && max_list <= 0xffffu;
+    const size_t o_pq = reserve(H.pq_centers.size() * 4), o_pre = reserve(H.prefix.size() * (pre16 ? 2 : 4));
     const size_t o_poff = reserve(H.prefix_off.size() * 8), o_prow = reserve(H.prefix_rows.size() * 8);
     idx->arena.reset();
     idx->arena.ensure(total);
@@ -844,10 +848,21 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.pq_centers = (const float*)up(o_pq, H.pq_centers.data(), H.pq_centers.size() * 4);
     if (!H.prefix_off.empty()) {  // the compressed rows form
         D.prefix = nullptr;
+        D.prefix16 = nullptr;
         D.prefix_off = (const uint64_t*)up(o_poff, H.prefix_off.data(), H.prefix_off.size() * 8);
         D.prefix_rows = (const uint64_t*)up(o_prow, H.prefix_rows.data(), H.prefix_rows.size() * 8);
     } else {
-        D.prefix = (const uint32_t*)up(o_pre, H.prefix.data(), H.prefix.size() * 4);
+        D.prefix = nullptr;
+        D.prefix16 = nullptr;
+        if (pre16) {
+            std::vector<uint16_t> p16(H.prefix.size());
+#pragma omp parallel for
+            for (int64_t i = 0; i < (int64_t)H.prefix.size(); i++) p16[i] = (uint16_t)H.prefix[i];
+            D.prefix16 = (const uint16_t*)up(o_pre, p16.data(), p16.size() * 2);
+            CK(cudaStreamSynchronize(st));  // p16 is read by the copy
+        } else {
+            D.prefix = (const uint32_t*)up(o_pre, H.prefix.data(), H.prefix.size() * 4);
+        }
         D.prefix_off = D.prefix_rows = nullptr;
     }
     k_to_bf16<<<blocks_for(H.centers.size(), 256), 256, 0, st>>>(D.centers, H.centers.size(),

@@ -304,9 +304,38 @@ __device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32
 __device__ __forceinline__ uint64_t block_select_smallest(uint64_t* keys, int n, int k, uint32_t* s_hist, uint32_t* s_wc,
                                           unsigned long long* s_sel) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    uint64_t prefix = 0, pmask = 0;
+    // the bytes above the highest one where the smallest and largest key differ are common to
+    // every key: the select starts below them
+    if (t == 0) {
+        s_sel[0] = ~0ull;
+        s_sel[1] = 0ull;
+    }
+    __syncthreads();
+    unsigned long long kmin = ~0ull, kmax = 0ull;
+    for (int i = t; i < n; i += blockDim.x) {
+        const uint64_t v = keys[i];
+        if (v != ~0ull) {
+            kmin = min(kmin, (unsigned long long)v);
+            kmax = max(kmax, (unsigned long long)v);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    }
+    if (lane == 0) {
+        atomicMin(&s_sel[0], kmin);
+        atomicMax(&s_sel[1], kmax);
+    }
+    __syncthreads();
+    const uint64_t lo_all = s_sel[0], diff = lo_all ^ s_sel[1];
+    const int top = diff ? (63 - __clzll((long long)diff)) / 8 * 8 : 0;  // shift of the highest differing byte
+    uint64_t pmask = top >= 56 ? 0ull : ~0ull << (top + 8);
+    uint64_t prefix = lo_all & pmask;
+    __syncthreads();  // every thread has read s_sel before it is reused
     uint32_t need = (uint32_t)k, cnt = 0;
-    for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int shift = top; shift >= 0; shift -= 8) {
         for (int i = t; i < 256; i += blockDim.x) s_hist[i] = 0;
         __syncthreads();
         for (int i = t; i < n; i += blockDim.x) {

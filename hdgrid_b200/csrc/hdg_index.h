@@ -127,7 +127,8 @@ struct IndexDev {
     const uint8_t* codes;
     const float* labels;
     const float* pq_centers;
-    const uint32_t* prefix;        // dense prefix counts (nullptr when the rows form is used)
+    const uint32_t* prefix;        // dense prefix counts (nullptr when the rows form or prefix16 is used)
+    const uint16_t* prefix16;      // the dense counts in 16 bits, kept when no list exceeds 65535 points
     const uint64_t* prefix_off;    // compressed rows (nullptr when dense)
     const uint64_t* prefix_rows;
 };

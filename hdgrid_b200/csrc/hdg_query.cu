@@ -134,6 +134,18 @@ __device__ __forceinline__ uint64_t budget_of(const Workspace& w, uint64_t qi, f
 }
 __device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) { return w.qbud[qi]; }
 
+// Warp-wide sum / maximum of a u64 (every lane gets it)
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
 // Slot of this lane among the lanes of its warp where f holds, taken from the counter *ctr
 // with one atomic per warp (~0u where f is false).  Every lane of the warp must call it.
 __device__ __forceinline__ uint32_t warp_reserve(bool f, uint32_t* ctr) {
@@ -246,7 +258,34 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
         s_sign[mask] = zero ? 0 : sign;
     }
     __syncthreads();
-    if (D.prefix) {  // dense: one coalesced row of L counts per corner
+    if (D.prefix16) {  // dense in 16 bits: two lists per 4-byte load when L is even
+        if ((L & 1) == 0) {
+            for (uint32_t jp = t; 2 * jp < L; jp += blockDim.x) {
+                long long a0 = 0, a1 = 0;
+                for (int m = 0; m < n_corner; m++) {
+                    const int sg = s_sign[m];
+                    if (!sg) continue;
+                    const uint32_t v = reinterpret_cast<const uint32_t*>(D.prefix16 + s_corner[m] * L)[jp];
+                    a0 += (long long)sg * (long long)(v & 0xffffu);
+                    a1 += (long long)sg * (long long)(v >> 16);
+                }
+                s_counts[2 * jp] = (uint32_t)a0;
+                s_counts[2 * jp + 1] = (uint32_t)a1;
+                w.list_counts[qi * L + 2 * jp] = (uint32_t)a0;
+                w.list_counts[qi * L + 2 * jp + 1] = (uint32_t)a1;
+            }
+        } else {
+            for (uint32_t j = t; j < L; j += blockDim.x) {
+                long long acc = 0;
+                for (int m = 0; m < n_corner; m++) {
+                    const int sg = s_sign[m];
+                    if (sg) acc += (long long)sg * (long long)D.prefix16[s_corner[m] * L + j];
+                }
+                s_counts[j] = (uint32_t)acc;
+                w.list_counts[qi * L + j] = (uint32_t)acc;
+            }
+        }
+    } else if (D.prefix) {  // dense: one coalesced row of L counts per corner
         for (uint32_t j = t; j < L; j += blockDim.x) {
             long long acc = 0;
             for (int m = 0; m < n_corner; m++) {
@@ -704,9 +743,15 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         w.item_off[q] = (uint32_t)ri;
         w.pitem_off[q] = (uint32_t)rp;
     }
-    atomicAdd(&s_red[0], cand);
-    atomicAdd(&s_red[1], exact);
-    atomicMax(&s_red[2], mx);
+    // one shared atomic per warp (1,024 threads on one word would serialise)
+    cand = warp_sum_u64(cand);
+    exact = warp_sum_u64(exact);
+    mx = warp_max_u64(mx);
+    if ((t & 31) == 0) {
+        atomicAdd(&s_red[0], cand);
+        atomicAdd(&s_red[1], exact);
+        atomicMax(&s_red[2], mx);
+    }
     __syncthreads();
     if (t == 0) {
         w.scal[0] = s_red[0];
@@ -745,8 +790,12 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         rs += si;
     }
     if (e == q && b < e) w.soff[q] = rs;
-    atomicAdd(&s_drop[0], dropped);
-    atomicAdd(&s_drop[1], kept);
+    dropped = warp_sum_u64(dropped);
+    kept = warp_sum_u64(kept);
+    if ((t & 31) == 0) {
+        atomicAdd(&s_drop[0], dropped);
+        atomicAdd(&s_drop[1], kept);
+    }
     __syncthreads();
     if (t == 0) {
         w.scal[5] = s_drop[0];
@@ -1088,7 +1137,14 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         uint32_t pp[J];
         bool pv[J];
         const uint32_t last = min(e1, eb + 32u * J) - 1;  // the step's last position
-        if (last < nb2) {  // at most one range starts inside the step
+        if (last < nb1 && eb + 32u * J <= e1) {  // a whole step inside the current range
+#pragma unroll
+            for (int j = 0; j < J; j++) {
+                pv[j] = true;
+                pp[j] = bc + eb + 32u * j + lane;
+            }
+            advance_to(eb + 32u * J);
+        } else if (last < nb2) {  // at most one range starts inside the step
 #pragma unroll
             for (int j = 0; j < J; j++) {
                 const uint32_t e = eb + 32u * j + lane;
@@ -1271,9 +1327,16 @@ __global__ void __launch_bounds__(1024) k_scan_plan(uint64_t q, Workspace w) {
     const uint64_t per = (q + blockDim.x - 1) / blockDim.x;
     const uint64_t b = t * per, e = min(q, b + per);
     auto n_items = [&](uint64_t i) {
-        const uint32_t c = compacts(w, i) ? w.cand_count[i] : w.qstat[i * 4];
+        uint32_t c = compacts(w, i) ? w.cand_count[i] : w.qstat[i * 4];
+        // a compact row that its budget takes whole needs no ADC distance (the select takes
+        // every survivor and the re-rank orders them), unless the distances are the output
+        // (the reference's pre-filter schedule)
+        if (compacts(w, i) && w.mode != kPre && c <= w.qbud[i]) c = 0;
         return (c + w.chunk - 1) / w.chunk;
     };
+    // such a row's survivors all count as passed (the ADC scan counts them for the others)
+    for (uint64_t i = b; i < e; i++)
+        if (compacts(w, i) && w.mode != kPre && w.cand_count[i] <= w.qbud[i]) w.nfin[i] = w.cand_count[i];
     unsigned long long items = 0;
     for (uint64_t i = b; i < e; i++) items += n_items(i);
     unsigned long long tot = 0;
@@ -1680,7 +1743,15 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             }
         }
     };
-    if (need0 > 0 && nfin <= (uint32_t)K) {
+    if (compact && !sorted_out && total <= q_budget(w, qi)) {
+        // the budget takes the whole compact row: every survivor, with no ADC distance read
+        // (the ADC scan left this row alone)
+        for (uint32_t base = 0; base < total; base += blockDim.x) {
+            const uint32_t e = base + t;
+            warp_append(e < total, e < total ? posof(e) : 0u, &s_out, sel_dst);
+        }
+        __syncthreads();
+    } else if (need0 > 0 && nfin <= (uint32_t)K) {
         // every finite candidate is selected (the loop bound is block-uniform so that every
         // lane reaches the warp appends)
         for (uint32_t base = 0; base < total; base += blockDim.x) {
