@@ -46,7 +46,8 @@ struct Params {
 };
 
 // ---- features --------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_features(IndexDev D, GridMeta g, const float* __restrict__ queries,
+// One 128-thread block per query (its phases are serial; small blocks keep more queries in flight)
+__global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const float* __restrict__ queries,
                                                   const float* __restrict__ box, const uint32_t* __restrict__ cc,
                                                   const uint32_t* __restrict__ qk, uint32_t k_max, int sort_n,
                                                   float* __restrict__ feats) {
@@ -380,7 +381,7 @@ void learned_features(hdg_index* idx, const float* d_queries, uint64_t q, const 
     const size_t sm = sizeof(uint64_t) * sort_n + sizeof(float) * D.d;
     HDG_REQUIRE(sm <= 200 * 1024, HDG_ERR_UNSUPPORTED, "feature kernel does not fit shared memory");
     CK(cudaFuncSetAttribute(k_features, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_features<<<(unsigned)q, 256, sm, st>>>(D, idx->grid, d_queries, box, cc, qk, k_max, sort_n, feats);
+    k_features<<<(unsigned)q, 128, sm, st>>>(D, idx->grid, d_queries, box, cc, qk, k_max, sort_n, feats);
     CK_LAUNCH();
 }
 

@@ -454,7 +454,10 @@ __device__ __forceinline__ void approx_band(const IndexDev& D, const Workspace& 
     *hi = a + e;
 }
 
-__global__ void __launch_bounds__(kThreads) k_coarse(IndexDev D, GridMeta g, const float* __restrict__ queries,
+// One block of kCoarseThreads per query: the query's phases are serial (selections, searches),
+// so smaller blocks keep more queries in flight per SM
+constexpr int kCoarseThreads = 128;
+__global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta g, const float* __restrict__ queries,
                                                      int Pc, int Ps, int sort_n1, int sort_n2,
                                                      Workspace w) {
     extern __shared__ uint64_t s_keys[];  // [max(sort_n1, sort_n2)] then query vector
@@ -2627,7 +2630,7 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     } else {
         w.S = nullptr;
     }
-    k_coarse<<<(unsigned)q, kThreads, sm_co, st>>>(D, idx->grid, c.queries, Pc, Ps, sort_n1, sort_n2, w);
+    k_coarse<<<(unsigned)q, kCoarseThreads, sm_co, st>>>(D, idx->grid, c.queries, Pc, Ps, sort_n1, sort_n2, w);
     CK_LAUNCH();
     launches++;
     tm.mark("coarse");
