@@ -1691,9 +1691,14 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     const uint32_t total = compact ? w.cand_count[qi] : w.qstat[qi * 4];
     const float* dist = w.dist + w.qoff[qi];
     const uint32_t* prow = compact ? w.spos + w.qoff[qi] : nullptr;
-    const uint32_t* rpre = w.range_pre + qi * (Ps + 1);
-    for (int i = t; i <= Ps; i += blockDim.x) s_pre[i] = rpre[i];
-    for (int i = t; i < Ps; i += blockDim.x) s_start[i] = w.range_start[qi * Ps + i];
+    // a compact row that its budget takes whole: every survivor, and the distance slots still
+    // hold the survivors' pool rows (the ADC scan left the row alone), so no range table either
+    const bool take_all = compact && !sorted_out && total <= q_budget(w, qi);
+    if (!take_all) {
+        const uint32_t* rpre = w.range_pre + qi * (Ps + 1);
+        for (int i = t; i <= Ps; i += blockDim.x) s_pre[i] = rpre[i];
+        for (int i = t; i < Ps; i += blockDim.x) s_start[i] = w.range_start[qi * Ps + i];
+    }
     if (t == 0) s_out = 0;
     __syncthreads();
     const uint32_t nfin = w.nfin[qi];
@@ -1746,13 +1751,10 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             }
         }
     };
-    if (compact && !sorted_out && total <= q_budget(w, qi)) {
-        // the budget takes the whole compact row: every survivor, with no ADC distance read
-        // (the ADC scan left this row alone)
-        for (uint32_t base = 0; base < total; base += blockDim.x) {
-            const uint32_t e = base + t;
-            warp_append(e < total, e < total ? posof(e) : 0u, &s_out, sel_dst);
-        }
+    if (take_all) {
+        const uint32_t* rows = reinterpret_cast<const uint32_t*>(dist);
+        for (uint32_t e = t; e < total; e += blockDim.x) sel_dst[e] = rows[e];
+        if (t == 0) s_out = total;
         __syncthreads();
     } else if (need0 > 0 && nfin <= (uint32_t)K) {
         // every finite candidate is selected (the loop bound is block-uniform so that every
@@ -1928,7 +1930,8 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     const uint32_t nsel = s_out;
     if (!sorted_out) {
         uint32_t* pool = w.cand_pool + w.soff[qi];
-        for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
+        if (!take_all)  // positions to pool rows (a whole compact row holds pool rows already)
+            for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
         if (t == 0) w.cand_count[qi] = nsel;
         return;
     }
