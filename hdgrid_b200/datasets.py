@@ -106,8 +106,10 @@ def config2(scale: float = 1.0, n_queries: int = 10_000, **conf):
             f"filter1:\n\ttype = 1\n\tinterval_map = [{table}]\n"
             "filter2:\n\ttype = 2\n\tdiv_value = [10]\n")
     # n_list / sub_lists / exps0: the recall@100 >= 0.95 operating point of the plain schedule
-    # on this workload (selectivity <= 2 % spreads the filtered neighbours over every list)
-    c = dict(clusters=64, sub_clusters=8, pq_dim=96, max_grids=30_000, n_list=64, sub_lists=512, exps0=10, topk=100)
+    # on this workload (selectivity <= 2 % spreads the filtered neighbours over every list);
+    # max_grids 3e7: the 74 x 74 x 5477 grid, whose counts the compressed prefix rows hold
+    c = dict(clusters=64, sub_clusters=8, pq_dim=96, max_grids=30_000_000, n_list=64, sub_lists=512, exps0=10,
+             topk=100)
     c.update(conf)
     return dict(name="config2", base=base, labels=labels, queries=queries, query_labels=qlabels,
                 hdgrid_conf=hdgrid_conf(**c), filter_conf=filt, k=int(c["topk"]), selectivity=sel)
