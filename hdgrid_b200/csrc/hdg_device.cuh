@@ -390,6 +390,17 @@ __device__ __forceinline__ uint64_t block_select_smallest(uint64_t* keys, int n,
     return kth;
 }
 
+// Band [lo, hi] around the exact f32 squared distance between a query and a centroid from
+// their squared norms qn, cn and a BF16 tensor-core dot product s: |(qn + cn - 2 s) - exact| is
+// below 2 * 2^-8 sqrt(qn cn) for BF16-rounded inputs, plus f32 rounding of the norms and sums;
+// the band doubles both terms.
+__device__ __forceinline__ void coarse_band(float qn, float cn, float s, float* lo, float* hi) {
+    const float a = qn + cn - 2.f * s;
+    const float e = 0.015625f * sqrtf(qn * cn) + 1e-4f * (qn + cn);
+    *lo = a - e;
+    *hi = a + e;
+}
+
 __device__ __forceinline__ uint32_t next_pow2_dev(uint32_t x) {
     return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
 }

@@ -54,8 +54,11 @@ constexpr int kMlpB2 = kMlpW2 + kMlpHidden * kMlpHidden;
 constexpr int kMlpW3 = kMlpB2 + kMlpHidden;
 constexpr int kMlpB3 = kMlpW3 + kMlpOut * kMlpHidden;
 constexpr int kMlpParams = kMlpB3 + kMlpOut;
+// S / ldS / qnorm: the coarse stage's tensor-core products and the queries' squared norms,
+// which narrow the exact centroid distances to the candidates of the 16 nearest (nullptr: all)
 void learned_features(hdg_index* idx, const float* d_queries, uint64_t q, const float* box, const uint32_t* cc,
-                      const uint32_t* qk, uint32_t k_max, float* feats, cudaStream_t st);
+                      const uint32_t* qk, uint32_t k_max, float* feats, cudaStream_t st, const float* S = nullptr,
+                      uint64_t ldS = 0, const float* qnorm = nullptr);
 void learned_infer(hdg_index* idx, const float* feats, uint64_t q, uint32_t* nprobe, uint8_t* sched, int allow_sched,
                    uint32_t max_probe, float* z, cudaStream_t st);
 void mlp_init(hdg_index* idx, uint64_t seed);

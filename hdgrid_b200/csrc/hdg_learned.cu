@@ -50,10 +50,14 @@ struct Params {
 __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const float* __restrict__ queries,
                                                   const float* __restrict__ box, const uint32_t* __restrict__ cc,
                                                   const uint32_t* __restrict__ qk, uint32_t k_max, int sort_n,
-                                                  float* __restrict__ feats) {
+                                                  const float* __restrict__ S, uint64_t ldS,
+                                                  const float* __restrict__ qnorm, float* __restrict__ feats) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);         // [sort_n]
-    float* s_q = reinterpret_cast<float*>(s_keys + sort_n);        // [d]
+    uint32_t* s_cand = reinterpret_cast<uint32_t*>(s_keys + sort_n);  // [sort_n]
+    float* s_q = reinterpret_cast<float*>(s_cand + sort_n);        // [d]
+    __shared__ int s_ncand;
+    __shared__ float s_bound;
     __shared__ float s_f[kMlpFeatures];
     __shared__ uint32_t s_hist[256], s_wc[32];
     __shared__ unsigned long long s_sel[4];
@@ -83,13 +87,46 @@ __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const 
     // Four centroids per warp and step keep four independent row loads in flight; each
     // centroid's sum is formed exactly as with one per step (per-lane FMA chain, warp sum).
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+    // With the coarse stage's tensor-core products S, only a centroid whose lower bound lies
+    // within the 16th smallest upper bound can be among the 16 nearest (the 16 with the
+    // smallest upper bounds are at or below it), so only those get exact distances: the same
+    // 16 keys, each computed the same way
+    const int kn = min(16, C);
+    int n_ex = C;
+    if (S) {
+        for (int c = t; c < sort_n; c += blockDim.x) {
+            uint64_t key = ~0ull;
+            if (c < C) {
+                float lo, hi;
+                coarse_band(qnorm[qi], D.cnorm[c], S[qi * ldS + c], &lo, &hi);
+                key = ((uint64_t)float_key(hi) << 32) | (uint32_t)c;
+            }
+            s_keys[c] = key;
+        }
+        if (t == 0) s_ncand = 0;
+        __syncthreads();
+        const uint64_t kth = block_select_smallest(s_keys, sort_n, kn, s_hist, s_wc, s_sel);
+        if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
+        __syncthreads();
+        for (int c = t; c < sort_n; c += blockDim.x) {
+            if (c < C) {
+                float lo, hi;
+                coarse_band(qnorm[qi], D.cnorm[c], S[qi * ldS + c], &lo, &hi);
+                if (lo <= s_bound) s_cand[atomicAdd(&s_ncand, 1)] = (uint32_t)c;
+            }
+            s_keys[c] = ~0ull;
+        }
+        __syncthreads();
+        n_ex = s_ncand;
+    }
+    auto cid = [&](int k) { return S ? (int)s_cand[k] : k; };
     constexpr int kCU = 4;
-    for (int c0 = warp; c0 < C; c0 += kCU * nw) {
+    for (int c0 = warp; c0 < n_ex; c0 += kCU * nw) {
         const float* row[kCU];
         float sq[kCU];
 #pragma unroll
         for (int u = 0; u < kCU; u++) {
-            row[u] = D.centers + (uint64_t)min(c0 + u * nw, C - 1) * d;
+            row[u] = D.centers + (uint64_t)cid(min(c0 + u * nw, n_ex - 1)) * d;
             sq[u] = 0.f;
         }
         for (int i = lane; i < d; i += 32) {
@@ -103,15 +140,16 @@ __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const 
 #pragma unroll
         for (int u = 0; u < kCU; u++) {
             const float v = warp_sum(sq[u]);
-            const int c = c0 + u * nw;
-            if (lane == 0 && c < C) s_keys[c] = ((uint64_t)float_key(v) << 32) | (uint32_t)c;
+            if (lane == 0 && c0 + u * nw < n_ex) {
+                const int c = cid(c0 + u * nw);
+                s_keys[c] = ((uint64_t)float_key(v) << 32) | (uint32_t)c;
+            }
         }
     }
     atomicAdd(&s_tot, tot);
     atomicAdd(&s_nz, nz);
     __syncthreads();
     // the 16 nearest centroids (keys distinct: the centroid index is their low word), in order
-    const int kn = min(16, C);
     block_select_smallest(s_keys, sort_n, kn, s_hist, s_wc, s_sel);
     block_bitonic_sort(s_keys, (int)next_pow2_dev((uint32_t)max(kn, 2)));
     const float lnN = logf(1.f + (float)D.n);
@@ -375,13 +413,15 @@ __global__ void k_round_rows(const float* __restrict__ x, uint64_t n, float* __r
 }  // namespace
 
 void learned_features(hdg_index* idx, const float* d_queries, uint64_t q, const float* box, const uint32_t* cc,
-                      const uint32_t* qk, uint32_t k_max, float* feats, cudaStream_t st) {
+                      const uint32_t* qk, uint32_t k_max, float* feats, cudaStream_t st, const float* S, uint64_t ldS,
+                      const float* qnorm) {
     const IndexDev& D = idx->dev;
     const int sort_n = (int)next_pow2(std::max<uint32_t>(D.C, 16));
-    const size_t sm = sizeof(uint64_t) * sort_n + sizeof(float) * D.d;
+    const size_t sm = (sizeof(uint64_t) + sizeof(uint32_t)) * sort_n + sizeof(float) * D.d;
     HDG_REQUIRE(sm <= 200 * 1024, HDG_ERR_UNSUPPORTED, "feature kernel does not fit shared memory");
     CK(cudaFuncSetAttribute(k_features, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_features<<<(unsigned)q, 128, sm, st>>>(D, idx->grid, d_queries, box, cc, qk, k_max, sort_n, feats);
+    k_features<<<(unsigned)q, 128, sm, st>>>(D, idx->grid, d_queries, box, cc, qk, k_max, sort_n, S, ldS, qnorm,
+                                             feats);
     CK_LAUNCH();
 }
 

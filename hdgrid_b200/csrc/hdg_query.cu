@@ -447,11 +447,7 @@ __device__ void split_subrange(const uint64_t* __restrict__ z, uint32_t off, uin
 // doubles both terms.
 __device__ __forceinline__ void approx_band(const IndexDev& D, const Workspace& w, uint64_t qi, uint32_t col,
                                             float* lo, float* hi) {
-    const float qn = w.qnorm[qi], cn = D.cnorm[col];
-    const float a = qn + cn - 2.f * w.S[qi * w.ldS + col];
-    const float e = 0.015625f * sqrtf(qn * cn) + 1e-4f * (qn + cn);
-    *lo = a - e;
-    *hi = a + e;
+    coarse_band(w.qnorm[qi], D.cnorm[col], w.S[qi * w.ldS + col], lo, hi);
 }
 
 // One block of kCoarseThreads per query: the query's phases are serial (selections, searches),
@@ -2603,17 +2599,6 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     CK_LAUNCH();
     launches++;
     tm.mark("prologue");
-    if (P.learned && !c.qps && !c.qsched) {
-        // the learned schedule: per-query lists to probe and predicate-first flag
-        HDG_REQUIRE(idx->mlp_ready, HDG_ERR_STATE, "LEARNED=1 but the index holds no trained model");
-        learned_features(idx, c.queries, q, w.box, w.cluster_counts, c.qk, k, w.feats, st);
-        learned_infer(idx, w.feats, q, w.lq_ps, w.lq_sched, mode != kPre, (uint32_t)Ps, nullptr, st);
-        w.qps = w.lq_ps;
-        w.qsched = mode != kPre ? w.lq_sched : nullptr;
-        launches += 2;
-        tm.mark("learned");
-    }
-
     const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
     const int sort_n2 = (int)next_pow2(std::max<uint32_t>((uint32_t)Pc * D.S_max, 2));
     const size_t sm_co = sizeof(uint64_t) * std::max(sort_n1, sort_n2) + sizeof(float) * D.d;
@@ -2633,6 +2618,18 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     } else {
         w.S = nullptr;
     }
+    if (P.learned && !c.qps && !c.qsched) {
+        // the learned schedule: per-query lists to probe and predicate-first flag
+        HDG_REQUIRE(idx->mlp_ready, HDG_ERR_STATE, "LEARNED=1 but the index holds no trained model");
+        // the features' 16 nearest centroids are pruned by the tensor-core products when present
+        learned_features(idx, c.queries, q, w.box, w.cluster_counts, c.qk, k, w.feats, st, w.S, w.ldS, w.qnorm);
+        learned_infer(idx, w.feats, q, w.lq_ps, w.lq_sched, mode != kPre, (uint32_t)Ps, nullptr, st);
+        w.qps = w.lq_ps;
+        w.qsched = mode != kPre ? w.lq_sched : nullptr;
+        launches += 2;
+        tm.mark("learned");
+    }
+
     k_coarse<<<(unsigned)q, kCoarseThreads, sm_co, st>>>(D, idx->grid, c.queries, Pc, Ps, sort_n1, sort_n2, w);
     CK_LAUNCH();
     launches++;
