@@ -1978,11 +1978,32 @@ __global__ void __launch_bounds__(1024) k_refine_plan(uint64_t q, Workspace w) {
     if (t == 0) w.counter[1] = 0;
 }
 
-// Adds the keys below the running k-th to s_keys in rounds of at most cap - kq keys; the
-// buffer is sorted and cut to kq between rounds.  get(i) gives key i of n; all threads.
+// Scratch of the re-rank's selections (shared memory)
+struct RefSel {
+    uint32_t* hist;            // [256]
+    uint32_t* wc;              // [32]
+    unsigned long long* sel;   // [4]
+};
+
+// Keeps the kq smallest of the c keys in s_keys (c > kq) in s_keys[0, kq), in no order, and
+// returns the kq-th smallest; the rest of [0, c) becomes ~0.  All threads.
+__device__ __forceinline__ uint64_t keep_smallest(uint64_t* s_keys, int c, int kq, const RefSel& rs) {
+    return block_select_smallest(s_keys, c, kq, rs.hist, rs.wc, rs.sel);
+}
+
+// Sorts s_keys[0, m) ascending (padding to the next power of two with ~0).  All threads.
+__device__ __forceinline__ void sort_prefix(uint64_t* s_keys, int m) {
+    const int n2 = (int)next_pow2_dev((uint32_t)max(m, 2));
+    for (int i = m + threadIdx.x; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(s_keys, n2);
+}
+
+// Adds the keys below the running k-th to s_keys in rounds of at most cap - kq keys; between
+// rounds the buffer keeps its kq smallest.  get(i) gives key i of n; all threads.
 template <typename Get>
 __device__ __forceinline__ void topk_rounds(uint64_t* s_keys, int cap, int kq, int n, int* s_cnt, uint64_t* s_th,
-                                            Get get) {
+                                            const RefSel& rs, Get get) {
     const int per_round = max(cap - kq, 1);
     for (int r0 = 0; r0 < n; r0 += per_round) {
         const int r1 = min(n, r0 + per_round);
@@ -1994,20 +2015,17 @@ __device__ __forceinline__ void topk_rounds(uint64_t* s_keys, int cap, int kq, i
         const int c = *s_cnt;
         __syncthreads();
         if (r1 < n && c > kq) {
-            const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
-            for (int i = c + threadIdx.x; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
-            __syncthreads();
-            block_bitonic_sort(s_keys, n2);
+            const uint64_t kth = keep_smallest(s_keys, c, kq, rs);
             if (threadIdx.x == 0) {
                 *s_cnt = kq;
-                *s_th = s_keys[kq - 1];
+                *s_th = kth;
             }
             __syncthreads();
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __restrict__ queries,
+__global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float* __restrict__ queries,
                                                      const float* __restrict__ data, int cap, int apply_pred,
                                                      int lbl, uint64_t q, Workspace w, float* __restrict__ out_dist,
                                                      uint64_t* __restrict__ out_ids, int k_out) {
@@ -2018,6 +2036,9 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
     __shared__ int s_wsum[kThreads / 32];
     __shared__ int s_cnt, s_ns, s_item, s_qi, s_last;
     __shared__ uint64_t s_th;
+    __shared__ uint32_t s_rhist[256], s_rwc[32];
+    __shared__ unsigned long long s_rsel[4];
+    const RefSel rs{s_rhist, s_rwc, s_rsel};
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = kThreads / 32;
     const int d = D.d;
     const uint32_t n_items = w.ritem_off[q];
@@ -2162,25 +2183,18 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
             const int c = s_cnt;
             __syncthreads();
             if (r1 < ns && c > kq) {  // more rows follow: keep the kq best
-                const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
-                for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
-                __syncthreads();
-                block_bitonic_sort(s_keys, n2);
+                const uint64_t kth = keep_smallest(s_keys, c, kq, rs);
                 if (t == 0) {
                     s_cnt = kq;
-                    s_th = s_keys[kq - 1];
+                    s_th = kth;
                 }
                 __syncthreads();
             }
         }
         int c = s_cnt;
         __syncthreads();
-        {
-            const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
-            for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
-            __syncthreads();
-            block_bitonic_sort(s_keys, n2);
-        }
+        if (c > kq) keep_smallest(s_keys, c, kq, rs);
+        sort_prefix(s_keys, min(c, kq));
         bool write_out = nq_items == 1;
         if (!write_out) {
             // this item's best kq keys go to its partial row; the query's last item merges
@@ -2198,13 +2212,12 @@ __global__ void __launch_bounds__(kThreads) k_refine(IndexDev D, const float* __
                 }
                 __syncthreads();
                 const uint64_t* rows = w.rpart + (uint64_t)it0 * k_out;
-                topk_rounds(s_keys, cap, kq, (int)nq_items * kq, &s_cnt, &s_th,
+                topk_rounds(s_keys, cap, kq, (int)nq_items * kq, &s_cnt, &s_th, rs,
                             [&](int i) { return __ldcg(rows + (uint64_t)(i / kq) * k_out + (i % kq)); });
                 c = s_cnt;
-                const int n2 = (int)next_pow2_dev((uint32_t)max(c, 2));  // the filled prefix only (c <= cap)
-                for (int i = c + t; i < n2; i += blockDim.x) s_keys[i] = ~0ull;
                 __syncthreads();
-                block_bitonic_sort(s_keys, n2);
+                if (c > kq) keep_smallest(s_keys, c, kq, rs);
+                sort_prefix(s_keys, min(c, kq));
                 write_out = true;
             }
         }
