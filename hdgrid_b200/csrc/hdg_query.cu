@@ -497,8 +497,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     __syncthreads();
     // clusters with a non-zero filtered count (filter_none_zero_data :1027-1028).  When all
     // of them fit in n_list the ranking cannot change the chosen set: no distances needed.
-    for (int c = t; c < (int)D.C; c += blockDim.x)
-        if (w.cluster_counts[qi * D.C + c] > 0) atomicAdd(&s_nvalid, 1);
+    {
+        uint32_t nz = 0;
+        for (int c = t; c < (int)D.C; c += blockDim.x) nz += w.cluster_counts[qi * D.C + c] > 0 ? 1u : 0u;
+        nz = __reduce_add_sync(0xffffffffu, nz);  // one shared atomic per warp
+        if ((t & 31) == 0 && nz) atomicAdd(&s_nvalid, (int)nz);
+    }
     __syncthreads();
     const bool all_c = s_nvalid <= Pc;
     // With the tensor-core estimates, only clusters whose lower bound is below the n_list-th
@@ -551,9 +555,18 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     __syncthreads();
     // the non-empty lists of the chosen clusters (again no distances when all are taken)
     const uint32_t Smax = D.S_max;
-    for (int e = t; e < npc * (int)Smax; e += blockDim.x) {
-        const uint32_t c = s_chosen[e / Smax], j = D.cluster_off[c] + e % Smax;
-        if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) atomicAdd(&s_nvalid, 1);
+    // list slot e = chosen cluster e / Smax, its list e % Smax (shifts when Smax is a power of two)
+    const bool sm_pow2 = (Smax & (Smax - 1)) == 0;
+    const int sm_shift = __ffs((int)Smax) - 1;
+    {
+        uint32_t nzl = 0;
+        for (int e = t; e < npc * (int)Smax; e += blockDim.x) {
+            const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
+            const uint32_t c = s_chosen[i], j = D.cluster_off[c] + jj;
+            if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) nzl++;
+        }
+        nzl = __reduce_add_sync(0xffffffffu, nzl);  // one shared atomic per warp
+        if ((t & 31) == 0 && nzl) atomicAdd(&s_nvalid, (int)nzl);
     }
     __syncthreads();
     // lists probed by this query: sub_lists, or the query's own n_probe when given
@@ -563,7 +576,7 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     if (prune_l) {
         for (int e = t; e < sort_n2; e += blockDim.x) {
             uint64_t key = ~0ull;
-            const int i = e / Smax, jj = e % Smax;
+            const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
             if (i < npc) {
                 const uint32_t c = s_chosen[i];
                 const uint32_t j = D.cluster_off[c] + jj;
@@ -582,7 +595,7 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     }
     for (int e = t; e < sort_n2; e += blockDim.x) {
         uint64_t key = ~0ull;
-        const int i = e / Smax, jj = e % Smax;
+        const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
         if (i < npc) {
             const uint32_t c = s_chosen[i];
             const uint32_t j = D.cluster_off[c] + jj;
@@ -844,7 +857,7 @@ __device__ __forceinline__ void store_lut(float* lut, int f16, uint64_t i, float
 // conflict-free lane reads); lane = subspace column j, so a warp stores one contiguous
 // 128-byte LUT row per codeword.
 __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict__ queries, uint64_t q, int G,
-                                             float* __restrict__ lut, int f16) {
+                                             float* __restrict__ lut, int f16, const uint32_t* __restrict__ item_off) {
     extern __shared__ float smem_lut[];
     const int g = blockIdx.y, pq_len = D.pq_len, d = D.d, M = D.M;
     float* s_cb = smem_lut;                          // [(c * pq_len + t) * 33 + j]
@@ -862,6 +875,7 @@ __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict
     for (int qq = warp; qq < kLutQ; qq += nw) {
         const uint64_t qi = (uint64_t)blockIdx.x * kLutQ + qq;
         if (qi >= q) break;
+        if (item_off[qi + 1] == item_off[qi]) continue;  // no ADC work: no LUT
         float qv[kLutMaxPqLen];
 #pragma unroll
         for (int t = 0; t < kLutMaxPqLen; t++)
@@ -883,10 +897,12 @@ __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict
 
 // Fallback for long subspaces: one query per block, thread = codeword, transposed store.
 __global__ void __launch_bounds__(256) k_lut_plain(IndexDev D, const float* __restrict__ queries, int G,
-                                                   float* __restrict__ lut, int f16) {
+                                                   float* __restrict__ lut, int f16,
+                                                   const uint32_t* __restrict__ item_off) {
     extern __shared__ float s_q[];     // [d]
     __shared__ float s_t[kCodes][33];  // [c][j]
     const uint64_t qi = blockIdx.x;
+    if (item_off[qi + 1] == item_off[qi]) return;  // no ADC work: no LUT (block-uniform)
     const int g = blockIdx.y, d = D.d, pq_len = D.pq_len, c = threadIdx.x;
     for (int i = threadIdx.x; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
     __syncthreads();
@@ -2702,21 +2718,6 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     w.rpart = static_cast<uint64_t*>(cx.part_buf.ptr);
     tm.mark("budget");
 
-    {
-        if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
-            const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
-            CK(cudaFuncSetAttribute(k_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, c.queries, q, (int)G, w.lut,
-                                                                                w.lut16);
-        } else {
-            k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, c.queries, (int)G, w.lut,
-                                                                              w.lut16);
-        }
-        CK_LAUNCH();
-        launches++;
-        tm.mark("lut");
-    }
-
     const int pre = mode == kPre ? 1 : 0;
     // candidate ranges per query: one per probed list, or n_split per list when is_split
     const int R = Ps * w.nsplit;
@@ -2747,6 +2748,22 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
             CK_LAUNCH();
             launches += 2;
             tm.mark("predicate");
+        }
+        {
+            // the LUTs of the queries that have ADC work items (a predicate-first query whose
+            // budget takes every survivor has none)
+            if (D.pq_len <= (uint32_t)kLutMaxPqLen) {
+                const size_t sm = sizeof(float) * kCodes * D.pq_len * 33;
+                CK(cudaFuncSetAttribute(k_lut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_lut<<<dim3((unsigned)((q + kLutQ - 1) / kLutQ), G), 512, sm, st>>>(D, c.queries, q, (int)G, w.lut,
+                                                                                    w.lut16, w.item_off);
+            } else {
+                k_lut_plain<<<dim3((unsigned)q, G), 256, sizeof(float) * D.d, st>>>(D, c.queries, (int)G, w.lut,
+                                                                                  w.lut16, w.item_off);
+            }
+            CK_LAUNCH();
+            launches++;
+            tm.mark("lut");
         }
         if (fast) {
             // threads x candidates-per-thread (SCAN_CPT, chosen by the autotuner; 0 = 1)
