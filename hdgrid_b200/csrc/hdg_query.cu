@@ -859,6 +859,12 @@ __device__ __forceinline__ void store_lut(float* lut, int f16, uint64_t i, float
 __global__ void __launch_bounds__(512) k_lut(IndexDev D, const float* __restrict__ queries, uint64_t q, int G,
                                              float* __restrict__ lut, int f16, const uint32_t* __restrict__ item_off) {
     extern __shared__ float smem_lut[];
+    // a block none of whose queries has ADC work stages nothing
+    {
+        const uint64_t qt = (uint64_t)blockIdx.x * kLutQ + threadIdx.x;
+        const bool need = threadIdx.x < kLutQ && qt < q && item_off[qt + 1] != item_off[qt];
+        if (!__syncthreads_or(need)) return;
+    }
     const int g = blockIdx.y, pq_len = D.pq_len, d = D.d, M = D.M;
     float* s_cb = smem_lut;                          // [(c * pq_len + t) * 33 + j]
     const int n = 32 * kCodes * pq_len;
@@ -1259,6 +1265,18 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     }
 }
 
+// The pass without the cell test (queries with most candidates inside the cell box, or an index
+// with NaN labels) is called out of line, so that the hot loop with the test stays compact in
+// the instruction cache
+template <typename PT, bool LAB4>
+__device__ __noinline__ void pre_span_labels(const IndexDev& D, int lbl, const float* bx_s, const uint32_t* pre,
+                                             const uint32_t* start, int R, int r0, uint32_t e0, uint32_t e1,
+                                             uint32_t* qr, uint32_t* sr, float4* lst, uint32_t* ctr, uint32_t* drow,
+                                             uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
+    pre_span<PT, false, LAB4>(D, lbl, bx_s, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow,
+                              prow, n_read, n_chk);
+}
+
 template <typename PT, bool LAB4>
 __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMeta g, int R, int lbl, uint64_t q,
                                                              Workspace w) {
@@ -1347,8 +1365,8 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMet
             pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, R, r0, e0, e1, qr,
                                      sr, lst, ctr, drow, prow, n_read, n_chk);
         else
-            pre_span<PT, false, LAB4>(D, lbl, bxs, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, lst,
-                                      ctr, drow, prow, n_read, n_chk);
+            pre_span_labels<PT, LAB4>(D, lbl, bxs, pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow, prow, n_read,
+                                      n_chk);
         if (lane == 0 && n_read) atomicAdd(&w.zin[qq], n_read);
         if (lane == 0 && n_chk) atomicAdd(&w.zchk[qq], n_chk);
     }
