@@ -1165,16 +1165,20 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         qh = qi;
         __syncwarp();  // lst and the consumed ring slots are free again
     };
-    for (uint32_t eb = e0; eb < e1; eb += 32u * J) {
+    // one pass past the last step drains the queue (a single copy of the label-batch code)
+    for (uint32_t eb = e0;; eb += 32u * J) {
+        const bool last_pass = eb >= e1;
         if (CHECK) {
             // test the batch in flight, start the next one; drain more only when the ring has no
-            // room for this step's pushes
+            // room for this step's pushes (or, after the last step, until it is empty)
             for (;;) {
                 if (qi != qh) consume();
-                if (qt - qh >= LB) issue(LB);
-                if (qt - qh <= QS - 32u * J) break;
+                const uint32_t pend = qt - qh;
+                if (pend >= LB || (last_pass && pend > 0)) issue(min(LB, pend));
+                if (last_pass ? qi == qh : qt - qh <= QS - 32u * J) break;
             }
         }
+        if (last_pass) break;
         uint32_t pp[J];
         bool pv[J];
         const uint32_t last = min(e1, eb + 32u * J) - 1;  // the step's last position
