@@ -304,7 +304,7 @@ def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int, read_q=None, c
     A post-filter query: M code bytes per candidate, in the ADC scan.  A predicate-first query
     with the predicate inside the ADC scan (read_q None): 4*l label bytes per candidate plus M
     code bytes per candidate that passes, all in the ADC scan.  A predicate-first query of the
-    predicate pass: cbytes of packed cell coordinates per candidate whose cell it tested (chk_q)
+    predicate pass: cbytes of packed label ranks per candidate whose ranks it tested (chk_q)
     and 4*l label bytes per candidate whose labels it read (read_q), then M code bytes per
     survivor in the ADC scan."""
     cand_q = np.asarray(cand_q, np.float64)
@@ -436,12 +436,12 @@ def run_hdgrid(args):
         pre_q = np.frombuffer(idx.debug_fetch("learned_schedule").tobytes(), np.uint8)[:nq] == 1
     pass_q = np.frombuffer(idx.debug_fetch("nfin").tobytes(), np.uint32)[:nq].astype(np.uint64)
     # the predicate pass (the fast ADC path: M a multiple of 32, at most 96) counts the packed
-    # cells and labels it read per query
+    # label ranks and labels it read per query
     pred_pass = info["M"] % 32 == 0 and info["M"] <= 96
     read_q = chk_q = None
     if pred_pass:
-        read_q = np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq].astype(np.uint64)
-        chk_q = np.frombuffer(idx.debug_fetch("morton_checked").tobytes(), np.uint32)[:nq].astype(np.uint64)
+        read_q = np.frombuffer(idx.debug_fetch("labels_read").tobytes(), np.uint32)[:nq].astype(np.uint64)
+        chk_q = np.frombuffer(idx.debug_fetch("ranks_read").tobytes(), np.uint32)[:nq].astype(np.uint64)
     # a predicate-first query whose budget takes every survivor needs no ADC (the re-rank
     # orders them): only the others' survivors are summed
     adc_q = pre_q.copy()
@@ -449,7 +449,7 @@ def run_hdgrid(args):
         bud_q = np.frombuffer(idx.debug_fetch("budget").tobytes(), np.uint32)[:nq].astype(np.uint64)
         adc_q = pre_q & (pass_q > bud_q)
     pred_bytes, adc_bytes = algorithmic_scan_bytes(cand_q, np.where(pre_q & ~adc_q, 0, pass_q), pre_q, info["M"],
-                                                   info["l"], read_q, chk_q, info["cell_pack_bytes"])
+                                                   info["l"], read_q, chk_q, info["rank_pack_bytes"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
     # the re-rank: every selected entry's pool -> id lookup (4 B) and, for a post-filter query,

@@ -54,7 +54,7 @@ class hdg_index_info(C.Structure):
         ("label_left", C.c_uint64 * MAX_DIMS), ("label_span", C.c_uint64 * MAX_DIMS),
         ("morton_dims", C.c_int32), ("morton_max_bits", C.c_int32), ("morton_valid_map", C.c_int32),
         ("diff_dim", C.c_int32), ("device_bytes", C.c_uint64), ("prefix_entries", C.c_uint64),
-        ("cell_pack_bytes", C.c_uint64)]
+        ("rank_pack_bytes", C.c_uint64), ("rank_bits", C.c_uint64)]
 
 
 class HDGError(RuntimeError):
@@ -268,7 +268,7 @@ class SuperGridIndex:
                 "label_span": list(i.label_span[:l]), "morton_dims": i.morton_dims,
                 "morton_max_bits": i.morton_max_bits, "morton_valid_map": i.morton_valid_map,
                 "diff_dim": i.diff_dim, "device_bytes": i.device_bytes, "prefix_entries": i.prefix_entries,
-                "cell_pack_bytes": i.cell_pack_bytes}
+                "rank_pack_bytes": i.rank_pack_bytes, "rank_bits": i.rank_bits}
 
     def build(self, build_in: build_input_t, stream=None) -> None:
         ds, lb = build_in.dataset, build_in.data_labels

@@ -372,7 +372,8 @@ hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out) {
         out->diff_dim = H.grid.diff_dim;
         out->device_bytes = index->arena.bytes;
         out->prefix_entries = index->host.prefix_off.empty() ? 0 : index->host.prefix_rows.size();
-        out->cell_pack_bytes = index->dev.pack_bytes;
+        out->rank_pack_bytes = index->dev.rankpack ? 4 : 0;
+        out->rank_bits = index->dev.rank_bits;
     });
 }
 

@@ -297,21 +297,25 @@ __global__ void k_scan_axis(uint32_t* __restrict__ prefix, uint64_t n_lines, uin
     }
 }
 
-// Packed cell coordinates of every point from its Morton code: dim i's coordinate is the
-// code's bits under zmask[i] in ascending order (morton_dim_masks), placed at pack_off[i].
-template <typename T>
-__global__ void k_pack_cells(const uint64_t* __restrict__ z, uint64_t n, GridMeta g, T* __restrict__ out) {
+// Every point's label ranks packed into 32 bits: dim i's rank (thresholds at or below the
+// label, by binary search) at bit i * (bits + 1).
+__global__ void k_pack_ranks(const float* __restrict__ labels, uint64_t n, int l, const float* __restrict__ thr,
+                             uint32_t stride, IndexDev D, uint32_t* __restrict__ out) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
-    const uint64_t code = z[r];
-    uint64_t packed = 0;
-    for (int i = 0; i < g.l; i++) {
-        if (!g.pack_w[i]) continue;
-        uint64_t m = g.zmask[i], c = 0;
-        for (int k = 0; m; k++, m &= m - 1) c |= ((code >> (__ffsll((long long)m) - 1)) & 1ull) << k;
-        packed |= c << g.pack_off[i];
+    uint32_t packed = 0;
+    for (int i = 0; i < l; i++) {
+        const float x = labels[r * l + i];
+        const float* t = thr + (uint64_t)i * stride;
+        uint32_t lo = 0, hi = D.rank_n[i];
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (t[mid] <= x) lo = mid + 1;
+            else hi = mid;
+        }
+        packed |= lo << (i * (D.rank_bits + 1));
     }
-    out[r] = (T)packed;
+    out[r] = packed;
 }
 
 // codes [n][chunks] (16-byte chunks, row-major) -> [chunks][n]: chunk j of point p at j*n + p
@@ -791,10 +795,40 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_co = reserve(H.cluster_off.size() * 4), o_lo = reserve(H.list_off.size() * 4);
     GridMeta gp = H.grid;
     morton_dim_masks(gp);
-    cell_pack_layout(gp);
-    const uint32_t pack_bytes = gp.pack_bits <= 16 ? 2u : gp.pack_bits <= 32 ? 4u : gp.pack_bits <= 64 ? 8u : 0u;
+    // label-rank thresholds: per dim, the distinct values of a strided sample when they fit,
+    // else its quantiles (equal counts per rank), so a rank box is about as tight as the labels
+    const int rbits = H.n && !H.labels.empty() ? rank_bits_for((int)H.l) : 0;
+    const uint32_t rstride = rbits ? (1u << rbits) - 1u : 0u;
+    std::vector<float> rthr((size_t)H.l * rstride);
+    uint32_t rn[kMaxDims] = {0};
+    if (rbits) {
+        const uint64_t step = std::max<uint64_t>(1, H.n / 262144);
+#pragma omp parallel for
+        for (int i = 0; i < (int)H.l; i++) {
+            std::vector<float> v;
+            v.reserve(H.n / step + 1);
+            for (uint64_t r = 0; r < H.n; r += step) {
+                const float x = H.labels[r * H.l + i];
+                if (!std::isnan(x)) v.push_back(x);
+            }
+            std::sort(v.begin(), v.end());
+            std::vector<float> u(v);
+            u.erase(std::unique(u.begin(), u.end()), u.end());
+            float* t = rthr.data() + (size_t)i * rstride;
+            uint32_t m = 0;
+            if (u.size() <= rstride + 1) {
+                for (size_t k = 1; k < u.size(); k++) t[m++] = u[k];  // one rank per distinct value
+            } else {
+                for (uint32_t k = 1; k <= rstride; k++) {
+                    const float x = v[(size_t)((uint64_t)k * v.size() / (rstride + 1))];
+                    if (m == 0 || x > t[m - 1]) t[m++] = x;
+                }
+            }
+            rn[i] = m;
+        }
+    }
     const size_t o_z = reserve(H.zcodes.size() * 8), o_id = reserve(H.ids.size() * 4);
-    const size_t o_pk = reserve(H.zcodes.size() * pack_bytes);
+    const size_t o_pk = reserve(rbits ? H.n * 4 : 0), o_rt = reserve(rthr.size() * 4);
     const size_t o_code = reserve(H.codes.size() + 64), o_lab = reserve(H.labels.size() * 4);
     // a dense prefix count never exceeds its list's size: 16 bits suffice when no list passes 65535
     uint32_t max_list = 0;
@@ -818,19 +852,7 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.list_off = (const uint32_t*)up(o_lo, H.list_off.data(), H.list_off.size() * 4);
     D.zcodes = (const uint64_t*)up(o_z, H.zcodes.data(), H.zcodes.size() * 8);
     D.ids = (const uint32_t*)up(o_id, H.ids.data(), H.ids.size() * 4);
-    D.pack_bytes = pack_bytes;
     D.labels_nan = std::any_of(H.labels.begin(), H.labels.end(), [](float v) { return std::isnan(v); }) ? 1u : 0u;
-    D.cellpack = pack_bytes ? base + o_pk : nullptr;
-    if (pack_bytes && H.n) {
-        const unsigned nb = blocks_for(H.n, 256);
-        if (pack_bytes == 2)
-            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint16_t*>(base + o_pk));
-        else if (pack_bytes == 4)
-            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint32_t*>(base + o_pk));
-        else
-            k_pack_cells<<<nb, 256, 0, st>>>(D.zcodes, H.n, gp, reinterpret_cast<uint64_t*>(base + o_pk));
-        CK_LAUNCH();
-    }
     {
         // pool-ordered rows -> 16-byte chunk planes (the scan's coalesced layout)
         DevMem<uint8_t> rows(std::max<size_t>(H.codes.size(), 16));
@@ -845,6 +867,19 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
         D.codes = (const uint8_t*)(base + o_code);
     }
     D.labels = (const float*)up(o_lab, H.labels.data(), H.labels.size() * 4);
+    D.rank_bits = (uint32_t)rbits;
+    D.rank_stride = rstride;
+    D.rank_guard = 0;
+    for (int i = 0; i < kMaxDims; i++) D.rank_n[i] = i < (int)H.l ? rn[i] : 0u;
+    for (int i = 0; rbits && i < (int)H.l; i++) D.rank_guard |= 1u << (i * (rbits + 1) + rbits);
+    D.rank_thr = rbits ? (const float*)up(o_rt, rthr.data(), rthr.size() * 4) : nullptr;
+    D.rankpack = rbits ? reinterpret_cast<const uint32_t*>(base + o_pk) : nullptr;
+    if (rbits) {
+        k_pack_ranks<<<blocks_for(H.n, 256), 256, 0, st>>>(D.labels, H.n, (int)H.l, D.rank_thr, rstride, D,
+                                                         reinterpret_cast<uint32_t*>(base + o_pk));
+        CK_LAUNCH();
+        CK(cudaStreamSynchronize(st));  // rthr is read by the copy
+    }
     D.pq_centers = (const float*)up(o_pq, H.pq_centers.data(), H.pq_centers.size() * 4);
     if (!H.prefix_off.empty()) {  // the compressed rows form
         D.prefix = nullptr;

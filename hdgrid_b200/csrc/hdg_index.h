@@ -55,31 +55,17 @@ struct GridMeta {
     // bits of each (shuffled) dim inside a Morton code (0 for a masked dim); derived from the
     // Morton configuration by morton_dim_masks, not stored in the index file
     uint64_t zmask[kMaxDims] = {0};
-    // packed cell coordinates (derived by cell_pack_layout, not stored in the index file): the
-    // coordinate of dim i in bits [pack_off[i], pack_off[i] + pack_w[i]) with a zero guard bit
-    // above it (pack_w[i] = 0: a dim of one cell, no field); pack_bits = total width
-    int pack_off[kMaxDims] = {0};
-    int pack_w[kMaxDims] = {0};
-    int pack_bits = 0;
 };
 
 // The Morton-code bit positions of every dim (zorder.cu:3-15 interleaves MSB first over the
 // valid dims): masking a code with zmask[i] keeps dim i's bits in their order, so comparing
 // two masked codes compares the two cells' coordinates of dim i.
-// Field layout of the packed cell coordinates: the bits of grid_dims[i] - 1 per dim of more
-// than one cell, each followed by a guard bit (used by the range test of the predicate pass).
-inline void cell_pack_layout(GridMeta& g) {
-    int off = 0;
-    for (int i = 0; i < kMaxDims; i++) {
-        g.pack_off[i] = off;
-        g.pack_w[i] = 0;
-        if (i >= g.l || g.grid_dims[i] <= 1) continue;
-        int w = 0;
-        while (w < 31 && (1u << w) < (uint32_t)g.grid_dims[i]) w++;
-        g.pack_w[i] = w;
-        off += w + 1;
-    }
-    g.pack_bits = off;
+// Bits per label-rank field: l fields of b bits, each with its guard bit, in 32 bits; at most
+// 12 (4095 thresholds per dim); 0 when l fields do not fit.
+inline int rank_bits_for(int l) {
+    if (l <= 0) return 0;
+    const int b = (32 - l) / l;
+    return b < 1 ? 0 : (b > 12 ? 12 : b);
 }
 
 inline void morton_dim_masks(GridMeta& g) {
@@ -118,10 +104,17 @@ struct IndexDev {
     const uint32_t* cluster_off;
     const uint32_t* list_off;
     const uint64_t* zcodes;
-    // every point's cell coordinates packed in pack_bytes (2, 4 or 8; 0 = too wide, none kept)
-    // in the fields of GridMeta::pack_off / pack_w: the predicate pass tests the cell box on these
-    const void* cellpack;
-    uint32_t pack_bytes;
+    // Label ranks (derived at upload, not stored in the index file): per label dim i, up to
+    // 2^rank_bits - 1 ascending thresholds rank_thr[i * rank_stride + k], k < rank_n[i]; a
+    // label's rank is the number of thresholds at or below it.  rankpack holds every point's
+    // ranks in pool order, dim i in bits [i * (rank_bits + 1), +rank_bits) with a zero guard bit
+    // above (rank_guard = the guard bits).  A rank outside the query's rank box proves the label
+    // test fails, so the predicate pass reads labels only for candidates inside it.
+    // rankpack = nullptr when the label dims do not fit 32 bits.
+    const uint32_t* rankpack;
+    const float* rank_thr;
+    uint32_t rank_n[kMaxDims];
+    uint32_t rank_bits, rank_stride, rank_guard;
     uint32_t labels_nan;           // some label is NaN (passes every label test, in any cell)
     const uint32_t* ids;
     const uint8_t* codes;

@@ -2,7 +2,7 @@
 // (src/index/2-level_index/Super-Grid-IVF_PQ.cu:985-1249) as B200 kernels.
 //
 //   k_prologue   per query: filter recovery (preprocessing.cu:3-32) -> f32 box, cell box
-//                (:930-961), Morton corners (:903-928, zorder.cu:3-15), per-list filtered
+//                (:930-961), label-rank box, Morton corners (:903-928, zorder.cu:3-15), per-list filtered
 //                counts by 2^d-corner inclusion-exclusion over the dense prefix counts
 //                (:693-765) and per-cluster sums (:767-790).
 //   k_coarse     per query: exact f32 L2 to the non-empty clusters, top n_list
@@ -11,6 +11,8 @@
 //                [lower_bound(zlo), lower_bound(zhi+1)) inside every probed list (zorder.cu:656-685).
 //   k_batch      candidate offsets, work items and the batch sums of the post-filter budget
 //                beta (:1198-1222).
+//   k_pre_scan   predicate-first queries: label-rank box test, then the label predicate
+//                (filter.cu:30-64), survivors listed for the ADC (prefiltering.cu:36-51).
 //   k_lut        per query PQ lookup table (build_pq_lut_kernel, product-quantization.cu:4-35).
 //   k_scan       persistent streaming ADC over the contiguous Z-ordered candidate ranges
 //                (compute_batched_L2_distance_kernel, :37-77) with the LUT in shared memory,
@@ -43,6 +45,7 @@ constexpr uint32_t kPreChunk = 8192; // candidates per work item of the predicat
 struct Workspace {
     float* box;              // [q x 2l]
     int* cells;              // [q x 2l]
+    uint32_t* rank_box;      // [q x 2] rank box: low ranks, high ranks | guard bits (0: rejects nothing)
     uint64_t* zrange;        // [q x 2]
     uint32_t* list_counts;   // [q x L]
     uint32_t* cluster_counts;// [q x C]
@@ -59,8 +62,8 @@ struct Workspace {
     uint32_t* pitem_off;     // [q + 1] work-item offsets of the predicate pass (predicate-first queries)
     uint32_t* mm;            // [q x 2] min / max finite distance key
     uint32_t* nfin;          // [q] finite distances (predicate passed)
-    uint32_t* zin;           // [q] candidates of the predicate pass whose labels were read
-    uint32_t* zchk;          // [q] candidates of the predicate pass whose Morton code was read
+    uint32_t* lab_read;      // [q] candidates of the predicate pass whose labels were read
+    uint32_t* rank_read;     // [q] candidates of the predicate pass whose label ranks were read
     uint32_t* counter;       // [4] work counters: ADC scan, refine, predicate pass
     float* lut;              // [q x G x 256 x 32] f32, or __half when lut16
     int lut16;               // LUT stored in FP16 (LUT_FP16=1); the scan sums in FP32
@@ -201,10 +204,12 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
     __shared__ int s_cells[2 * kMaxDims];
     __shared__ uint64_t s_corner[1 << kMaxDims];
     __shared__ int s_sign[1 << kMaxDims];
+    __shared__ uint32_t s_rank[3];
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
     const int l = g.l;
     const uint32_t L = D.n_lists;
+    if (t < 3) s_rank[t] = 0;
     if (t < l) {
         float lo, hi;
         recover_dim(f, qlabels + qi * label_cols, t, &lo, &hi);
@@ -214,6 +219,27 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
         w.box[qi * 2 * l + 2 * t + 1] = hi;
     }
     __syncthreads();
+    if (t < l && D.rankpack) {
+        // the rank box of label dim t: a rank below that of lo means a label below a threshold
+        // <= lo, a rank above that of hi a label above a threshold > hi (NaN bounds reject nothing)
+        const float blo = s_box[2 * t], bhi = s_box[2 * t + 1];
+        const float* thr = D.rank_thr + (uint64_t)t * D.rank_stride;
+        const uint32_t n = D.rank_n[t];
+        auto rank = [&](float x) {
+            uint32_t a = 0, b = n;
+            while (a < b) {
+                const uint32_t m = (a + b) >> 1;
+                if (thr[m] <= x) a = m + 1;
+                else b = m;
+            }
+            return a;
+        };
+        const uint32_t rlo = isnan(blo) ? 0u : rank(blo), rhi = isnan(bhi) ? n : rank(bhi);
+        const int off = t * (int)(D.rank_bits + 1);
+        if (rlo) atomicOr(&s_rank[0], rlo << off);
+        atomicOr(&s_rank[1], rhi << off);
+        if (rlo > 0 || rhi < n) s_rank[2] = 1;
+    }
     if (t < l) {
         const int od = g.shuffle[t];
         int lo, hi;
@@ -232,6 +258,8 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
         }
         w.zrange[qi * 2] = morton_encode(clo, g.morton_dims, g.morton_max_bits, g.morton_valid_map);
         w.zrange[qi * 2 + 1] = morton_encode(chi, g.morton_dims, g.morton_max_bits, g.morton_valid_map);
+        w.rank_box[qi * 2] = s_rank[0];
+        w.rank_box[qi * 2 + 1] = s_rank[2] ? s_rank[1] | D.rank_guard : 0u;
     }
     // corners of the cell box over the valid (unmasked) dims (get_prefix_sum_device :693-724)
     const int dv = __popc(g.morton_valid_map);
@@ -766,8 +794,8 @@ __global__ void __launch_bounds__(1024) k_batch(uint64_t q, Workspace w) {
         w.mm[2 * i] = 0xffffffffu;
         w.mm[2 * i + 1] = 0u;
         w.nfin[i] = 0;
-        w.zin[i] = 0;
-        w.zchk[i] = 0;
+        w.lab_read[i] = 0;
+        w.rank_read[i] = 0;
         w.cand_count[i] = 0;
     }
     if (e == q && b < e) {
@@ -999,13 +1027,13 @@ __device__ __forceinline__ void scan_load_query(const Workspace& w, int Ps, int 
 // predicate-first flag) keeps only its candidates that pass the label predicate
 // (filter.cu:30-64), and only those need an ADC distance.  This pass runs before the ADC scan:
 // one warp per work item (kPreChunk consecutive candidate positions of one query), no
-// shared-memory LUT, so it runs at full occupancy and streams the candidates' packed cell
-// coordinates and labels.  A lane tests positions lane, lane + 32, ... of every step of 32 * J:
-//   1. the candidate's cell against the query's cell box, all dims in one guarded-field range
-//      test: a cell outside the box on a side where that proves the label test fails rejects
-//      the candidate without reading its labels;
-//   2. the labels of the other candidates against the query's f32 box, 32 per round from a
-//      per-warp queue, so that a round's label loads are all useful;
+// shared-memory LUT, so it runs at full occupancy and streams the candidates' packed label
+// ranks and labels.  A lane tests positions lane, lane + 32, ... of every step of 32 * J:
+//   1. the candidate's label ranks against the query's rank box, all dims in one guarded-field
+//      range test: a rank outside the box proves that the label test fails, so the candidate
+//      is rejected without reading its labels;
+//   2. the labels of the other candidates against the query's f32 box, 128 per batch from a
+//      per-warp queue, so that a batch's label loads are all useful;
 //   3. the survivors are staged per warp and appended to the query's row 32 at a time -- the
 //      candidate position into spos and the pool row into the distance slot, which the ADC
 //      scan then overwrites with the survivor's distance.
@@ -1056,13 +1084,14 @@ template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // One predicate-pass work item: positions [e0, e1) of one query (R ranges, prefix pre, starts
-// start; r0 the range of e0).  PT: the packed cell type, CHECK: test the cell box first (lo_f /
-// hi_g / gd: the box's low fields, its high fields with the guard bits set, the guard bits),
-// LAB4: four 16-byte-aligned label dims.  qr: [2][512] ring of cell-passed candidates (without
-// CHECK: of survivors), sr: [2][64] survivor ring, lst: [128] staged labels (LAB4).  n_chk /
-// n_read: candidates whose cell / labels were read (warp totals).
-template <typename PT, bool CHECK, bool LAB4>
-__device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float* bx_s, PT lo_f, PT hi_g, PT gd,
+// start; r0 the range of e0).  CHECK: test the rank box first (lo_f / hi_g / gd: the box's low
+// ranks, its high ranks with the guard bits set, the guard bits), LAB4: four 16-byte-aligned
+// label dims.  qr: [2][512] ring of rank-passed candidates (without CHECK: of survivors), sr:
+// [2][64] survivor ring, lst: [128] staged labels (LAB4).  n_chk / n_read: candidates whose
+// ranks / labels were read (warp totals).
+template <bool CHECK, bool LAB4>
+__device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float* bx_s, uint32_t lo_f, uint32_t hi_g,
+                                         uint32_t gd,
                                          const uint32_t* pre, const uint32_t* start, int R, int r0, uint32_t e0,
                                          uint32_t e1, uint32_t* qr, uint32_t* sr, float4* lst, uint32_t* ctr,
                                          uint32_t* drow, uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
@@ -1072,7 +1101,7 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     float bx[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) bx[i] = LAB4 ? bx_s[i] : 0.f;
-    const PT* cells = static_cast<const PT*>(D.cellpack);
+    const uint32_t* ranks = D.rankpack;
     const float4* lab4 = reinterpret_cast<const float4*>(D.labels);
     // Position -> pool row (warp-uniform state): the current range rc holds positions up to
     // nb1 (pool row = bc + position), the next non-empty range from nb1 up to nb2 (bn).  A step
@@ -1216,15 +1245,15 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
             }
         }
         if constexpr (CHECK) {
-            PT c[J];
+            uint32_t c[J];
 #pragma unroll
-            for (int j = 0; j < J; j++) c[j] = pv[j] ? __ldg(cells + pp[j]) : PT(0);
+            for (int j = 0; j < J; j++) c[j] = pv[j] ? __ldg(ranks + pp[j]) : 0u;
 #pragma unroll
             for (int j = 0; j < J; j++) {
                 // every field at or above its low bound and at or below its high bound: the
                 // guard bit above a field survives both subtractions exactly then
-                const PT t = (PT)((PT)((c[j] | gd) - lo_f) & (PT)(hi_g - c[j]));
-                ring_push<QS>(qr, qt, pv[j] && (PT)(t & gd) == gd, eb + 32u * j + lane, pp[j]);
+                const uint32_t t = ((c[j] | gd) - lo_f) & (hi_g - c[j]);
+                ring_push<QS>(qr, qt, pv[j] && (t & gd) == gd, eb + 32u * j + lane, pp[j]);
             }
         } else {
             if (LAB4) {
@@ -1269,27 +1298,25 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     }
 }
 
-// The pass without the cell test (queries with most candidates inside the cell box, or an index
+// The pass without the rank test (queries with most candidates inside the cell box, or an index
 // with NaN labels) is called out of line, so that the hot loop with the test stays compact in
 // the instruction cache
-template <typename PT, bool LAB4>
+template <bool LAB4>
 __device__ __noinline__ void pre_span_labels(const IndexDev& D, int lbl, const float* bx_s, const uint32_t* pre,
                                              const uint32_t* start, int R, int r0, uint32_t e0, uint32_t e1,
                                              uint32_t* qr, uint32_t* sr, float4* lst, uint32_t* ctr, uint32_t* drow,
                                              uint32_t* prow, uint32_t& n_read, uint32_t& n_chk) {
-    pre_span<PT, false, LAB4>(D, lbl, bx_s, PT(0), PT(0), PT(0), pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow,
-                              prow, n_read, n_chk);
+    pre_span<false, LAB4>(D, lbl, bx_s, 0u, 0u, 0u, pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow, prow, n_read,
+                          n_chk);
 }
 
-template <typename PT, bool LAB4>
-__global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMeta g, int R, int lbl, uint64_t q,
-                                                             Workspace w) {
+template <bool LAB4>
+__global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, int R, int lbl, uint64_t q, Workspace w) {
     constexpr int NW = kPreThreads / 32;
     extern __shared__ __align__(16) uint32_t s_rings[];  // per warp: staged labels, queue ring, survivor ring
     __shared__ float s_bx[NW][2 * kMaxDims];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t n_items = w.pitem_off[q];
-    const int l = g.l;
     for (;;) {
         __syncwarp();  // the previous item's reads of the warp's tables are done
         uint32_t item = 0;
@@ -1302,58 +1329,14 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMet
         if (e0 >= total) continue;  // a query cut by a capacity
         const uint32_t e1 = min(total, e0 + kPreChunk);
         if (lane < 2 * lbl) s_bx[wp][lane] = w.box[(uint64_t)qq * 2 * lbl + lane];
-        // The cell box as packed fields, per dim (shuffled order) and side that can reject: a
-        // cell below the low cell means a label below l = (float)max(trunc(lo), left), as cells
-        // grow with the label (get_grid_id_device, Super-Grid-IVF_PQ.cu:24-26), which rejects
-        // exactly when l <= lo; above the high cell only proves the label exceeds
-        // r = (float)min(trunc(hi), left + span) (:947-960), exact when r >= hi.  The other
-        // sides take every cell.  Skipped when the index holds NaN labels (a NaN passes the
-        // label test in any cell) or when the query's count of points in its cell box over the
-        // probed lists says the codes would cost more label bytes than they save.
+        // The query's rank box (label ranks: see IndexDev) rejects a candidate whose labels
+        // must fail without reading them.  Skipped when it rejects nothing, when the index holds
+        // NaN labels (a NaN passes the label test), or when the query's count of points in its
+        // cell box over the probed lists says that most candidates pass anyway.
         const uint32_t inbox = w.qstat[(uint64_t)qq * 4 + 1];
-        const bool check = D.pack_bytes && !D.labels_nan &&
-                           (uint64_t)inbox * 16 < (uint64_t)total * (16 - D.pack_bytes);
-        uint64_t lo_f = 0, hi_f = 0, gd = 0;
-        bool act = false;
-        {
-            // lane i < l takes dim i of the grid (selected by unrolled compares: no local copy of g)
-            uint64_t left = 0, top = 0;
-            int shf = 0, gdim = 0, off = 0, wd = 0;
-#pragma unroll
-            for (int i = 0; i < kMaxDims; i++)
-                if (i == lane) {
-                    left = g.left[i];
-                    top = g.left[i] + g.span[i];
-                    shf = g.shuffle[i];
-                    gdim = g.grid_dims[i];
-                    off = g.pack_off[i];
-                    wd = g.pack_w[i];
-                }
-            if (check && lane < l && wd > 0) {
-                const int clo = w.cells[(uint64_t)qq * 2 * l + 2 * lane];
-                const int chi = w.cells[(uint64_t)qq * 2 * l + 2 * lane + 1];
-                const float blo = w.box[(uint64_t)qq * 2 * lbl + 2 * shf];
-                const float bhi = w.box[(uint64_t)qq * 2 * lbl + 2 * shf + 1];
-                const uint64_t tlo = (uint64_t)blo, thi = (uint64_t)bhi;  // saturating, as in cell_range
-                const float lf = (float)(tlo > left ? tlo : left);
-                const float rf = (float)(thi < top ? thi : top);
-                const bool lo_rej = clo > 0 && lf <= blo;
-                const bool hi_rej = chi < gdim - 1 && rf >= bhi;
-                act = lo_rej || hi_rej;
-                lo_f = (uint64_t)(lo_rej ? clo : 0) << off;
-                hi_f = (uint64_t)(hi_rej ? (uint32_t)chi : (1u << wd) - 1u) << off;
-                gd = 1ull << (off + wd);
-            }
-        }
-        // every field's bounds to every lane (fields are disjoint: OR them together)
-        const bool use = __any_sync(0xffffffffu, act);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            lo_f |= __shfl_xor_sync(0xffffffffu, lo_f, o);
-            hi_f |= __shfl_xor_sync(0xffffffffu, hi_f, o);
-            gd |= __shfl_xor_sync(0xffffffffu, gd, o);
-        }
-        __syncwarp();
+        const uint32_t rlo = w.rank_box[2 * qq], rhi = w.rank_box[2 * qq + 1];
+        const bool use = rhi != 0 && D.rankpack && !D.labels_nan && (uint64_t)inbox * 16 < (uint64_t)total * 12;
+        __syncwarp();  // s_bx is written
         const uint32_t* pre = w.range_pre + (uint64_t)qq * (R + 1);
         const uint32_t* start = w.range_start + (uint64_t)qq * R;
         const int r0 = warp_find_le(pre, R, e0);
@@ -1366,13 +1349,13 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, GridMet
         uint32_t* qr = reinterpret_cast<uint32_t*>(lst + 128);
         uint32_t* sr = qr + 2 * 512;
         if (use)
-            pre_span<PT, true, LAB4>(D, lbl, bxs, (PT)lo_f, (PT)(hi_f | gd), (PT)gd, pre, start, R, r0, e0, e1, qr,
-                                     sr, lst, ctr, drow, prow, n_read, n_chk);
+            pre_span<true, LAB4>(D, lbl, bxs, rlo, rhi, D.rank_guard, pre, start, R, r0, e0, e1, qr, sr, lst, ctr,
+                                 drow, prow, n_read, n_chk);
         else
-            pre_span_labels<PT, LAB4>(D, lbl, bxs, pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow, prow, n_read,
-                                      n_chk);
-        if (lane == 0 && n_read) atomicAdd(&w.zin[qq], n_read);
-        if (lane == 0 && n_chk) atomicAdd(&w.zchk[qq], n_chk);
+            pre_span_labels<LAB4>(D, lbl, bxs, pre, start, R, r0, e0, e1, qr, sr, lst, ctr, drow, prow, n_read,
+                                  n_chk);
+        if (lane == 0 && n_read) atomicAdd(&w.lab_read[qq], n_read);
+        if (lane == 0 && n_chk) atomicAdd(&w.rank_read[qq], n_chk);
     }
 }
 
@@ -2316,6 +2299,7 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     Workspace w{};
     w.box = (float*)take("box", q * 2 * l * 4);
     w.cells = (int*)take("cells", q * 2 * l * 4);
+    w.rank_box = (uint32_t*)take("rank_box", q * 2 * 4);
     w.zrange = (uint64_t*)take("zrange", q * 2 * 8);
     w.list_counts = (uint32_t*)take("list_counts", q * L * 4);
     w.cluster_counts = (uint32_t*)take("cluster_counts", q * C * 4);
@@ -2334,8 +2318,8 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     w.pitem_off = (uint32_t*)take("pre_items", (q + 1) * 4);
     w.mm = (uint32_t*)take("minmax", q * 2 * 4);
     w.nfin = (uint32_t*)take("nfin", q * 4);
-    w.zin = (uint32_t*)take("morton_in", q * 4);
-    w.zchk = (uint32_t*)take("morton_checked", q * 4);
+    w.lab_read = (uint32_t*)take("labels_read", q * 4);
+    w.rank_read = (uint32_t*)take("ranks_read", q * 4);
     w.counter = (uint32_t*)take("counter", 16);
     w.lut16 = P.lut_fp16 != 0;
     w.lut = (float*)take("lut", q * G * kCodes * 32 * (w.lut16 ? 2 : 4));
@@ -2753,18 +2737,10 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
                 const size_t smp = sizeof(uint32_t) * kPreRingWords * (kPreThreads / 32);
                 CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp));
                 const int blocks = sm_count() * occupancy_blocks(kern, kPreThreads, smp);
-                kern<<<blocks, kPreThreads, smp, st>>>(D, idx->grid, R, l, q, w);
+                kern<<<blocks, kPreThreads, smp, st>>>(D, R, l, q, w);
             };
-            if (D.pack_bytes == 2) {
-                if (lab4) launch_pre(k_pre_scan<uint16_t, true>);
-                else launch_pre(k_pre_scan<uint16_t, false>);
-            } else if (D.pack_bytes == 8) {
-                if (lab4) launch_pre(k_pre_scan<uint64_t, true>);
-                else launch_pre(k_pre_scan<uint64_t, false>);
-            } else {  // 4 bytes, or no packed cells (the pass then reads labels only)
-                if (lab4) launch_pre(k_pre_scan<uint32_t, true>);
-                else launch_pre(k_pre_scan<uint32_t, false>);
-            }
+            if (lab4) launch_pre(k_pre_scan<true>);
+            else launch_pre(k_pre_scan<false>);
             CK_LAUNCH();
             k_scan_plan<<<1, 1024, 0, st>>>(q, w);
             CK_LAUNCH();

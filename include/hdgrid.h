@@ -224,8 +224,8 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
 /* Copy a named intermediate buffer of the last query to host memory (parity tests).
  * Names: "box", "cells", "zrange", "list_counts", "cluster_counts", "probe_clusters",
  * "probe_lists", "range_start", "range_len", "cand_count", "budget", "sel_off", "scalars",
- * "qoff", "qstat", "morton_in" (candidates of the predicate pass whose labels were read),
- * "morton_checked" (candidates of the predicate pass whose packed cell was read),
+ * "qoff", "qstat", "labels_read" (candidates of the predicate pass whose labels were read),
+ * "ranks_read" (candidates of the predicate pass whose packed label ranks were read),
  * "distances" (the f32 ADC distance of every scanned candidate, query rows
  * at the "qoff" offsets) and "cand_pool" (each query's selected candidates, rows at the
  * "sel_off" offsets, "cand_count" of them). */
@@ -243,8 +243,9 @@ typedef struct hdg_index_info {
     int32_t morton_dims, morton_max_bits, morton_valid_map, diff_dim;
     uint64_t device_bytes;
     uint64_t prefix_entries;  /* change points of the compressed prefix rows; 0 = dense form */
-    uint64_t cell_pack_bytes; /* bytes per point of the packed cell coordinates that the predicate
-                               * pass reads (2, 4 or 8; 0 = too wide, not kept) */
+    uint64_t rank_pack_bytes; /* bytes per point of the packed label ranks that the predicate pass
+                               * reads before the labels (4; 0 = not kept) */
+    uint64_t rank_bits;       /* bits per label dim of a packed rank (2^bits - 1 thresholds at most) */
 } hdg_index_info;
 hdg_status hdg_get_info(const hdg_index* index, hdg_index_info* out);
 

@@ -183,7 +183,7 @@ def test_parity_prefilter_rotated_adc(cuda):
 
 def test_parity_prefilter_compacted_scan(cuda):
     # M = 32 (one subspace group): the predicate pass lists each predicate-first query's
-    # survivors (Morton-code pre-check, then the labels) in arrival order, and the ADC scan sums
+    # survivors (label-rank pre-check, then the labels) in arrival order, and the ADC scan sums
     # each survivor from the subspace of its recorded position -- so ids and ADC distances
     # still equal the oracle's bit for bit
     ws = datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
@@ -193,32 +193,50 @@ def test_parity_prefilter_compacted_scan(cuda):
     assert valid.any()
     assert np.array_equal(r["g_ids"], r["o_ids"])
     assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
-    # every candidate's labels or Morton code were read, and the Morton check skipped some labels
+    # every candidate's labels or label ranks were read, and the rank check skipped some labels
     nq = ws["queries"].shape[0]
     cand = np.frombuffer(idx.debug_fetch("qstat").tobytes(), np.uint32).reshape(-1, 4)[:nq, 0]
-    read = np.frombuffer(idx.debug_fetch("morton_in").tobytes(), np.uint32)[:nq]
-    chk = np.frombuffer(idx.debug_fetch("morton_checked").tobytes(), np.uint32)[:nq]
+    read = np.frombuffer(idx.debug_fetch("labels_read").tobytes(), np.uint32)[:nq]
+    chk = np.frombuffer(idx.debug_fetch("ranks_read").tobytes(), np.uint32)[:nq]
     assert np.all((chk == cand) | ((chk == 0) & (read == cand)))
     assert np.all(read <= cand) and read.sum() < cand.sum()
 
 
-def test_parity_prefilter_cell_pack_widths(cuda):
-    # the predicate pass tests each candidate's packed cell coordinates (one guarded field per
-    # dim, 2 or 4 bytes here) against the query's cell box; every width and grid gives the
-    # oracle's ids and distances bit for bit
-    seen = set()
-    for max_grids in (4096, 20_000, 30_000_000):
-        ws = datasets.config2(scale=0.01, n_queries=120, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
-                              max_grids=max_grids, exps0=1)
-        idx, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True, layout=max_grids <= 300_000)
+def test_parity_prefilter_label_ranks(cuda):
+    # the predicate pass tests each candidate's packed label ranks (a guarded field per label dim:
+    # the number of the index's per-dim thresholds at or below the label) against the query's
+    # rank box before it reads the labels.  Quantile thresholds (config2's three dims, 9 bits;
+    # config4's four dims, 7 bits) and one rank per distinct value (a dim of 5 values, a
+    # constant dim) with box bounds equal to label values all give the oracle's ids and
+    # distances bit for bit, and the ranks spare label reads
+    cases = [datasets.config2(scale=0.01, n_queries=120, clusters=16, sub_clusters=4, n_list=8, sub_lists=24,
+                              max_grids=20_000, exps0=1)]
+    ws = datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
+                          max_grids=4096, exps0=1)
+    cases.append(ws)
+    ws = dict(ws)
+    lab = ws["labels"].copy()
+    lab[:, 1] = (lab[:, 1] // 200_000) * 200_000  # 5 distinct values
+    lab[:, 3] = 500_000                             # one value
+    ql = ws["query_labels"].copy()
+    ql[::3, 2] = 200_000                            # box bounds on the values themselves
+    ql[::3, 3] = 400_000
+    ws["labels"], ws["query_labels"] = lab, ql
+    cases.append(ws)
+    for ws in cases:
+        idx, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
         info = idx.info()
-        bits = sum((d - 1).bit_length() + 1 for d in info["grid_dims"] if d > 1)
-        assert info["cell_pack_bytes"] == (2 if bits <= 16 else 4 if bits <= 32 else 8), (bits, info)
-        seen.add(info["cell_pack_bytes"])
+        l = info["l"]
+        assert info["rank_pack_bytes"] == 4, info
+        assert info["rank_bits"] == min(12, (32 - l) // l), info
         valid = r["g_ids"] != INV
+        assert valid.any()
         assert np.array_equal(r["g_ids"], r["o_ids"])
         assert np.array_equal(r["g_dist"][valid].view(np.uint32), r["o_dist"][valid].view(np.uint32))
-    assert seen == {2, 4}, seen
+        nq = ws["queries"].shape[0]
+        read = np.frombuffer(idx.debug_fetch("labels_read").tobytes(), np.uint32)[:nq]
+        chk = np.frombuffer(idx.debug_fetch("ranks_read").tobytes(), np.uint32)[:nq]
+        assert read.sum() < chk.sum(), (read.sum(), chk.sum())
 
 
 def test_parity_prefilter_rotated_adc_fp16_lut(cuda):
