@@ -1098,9 +1098,6 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
     constexpr int J = 8;  // windows of 32 positions in one step
     constexpr uint32_t QS = 512, SS = 64, LB = 128;
     const int lane = threadIdx.x & 31;
-    float bx[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) bx[i] = LAB4 ? bx_s[i] : 0.f;
     const uint32_t* ranks = D.rankpack;
     const float4* lab4 = reinterpret_cast<const float4*>(D.labels);
     // Position -> pool row (warp-uniform state): the current range rc holds positions up to
@@ -1126,9 +1123,11 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
             find_next();
         }
     };
+    // (the box stays in shared memory: the label tests are rare and the registers go to loads in flight)
     auto box4 = [&](const float4& v) {
-        return !(v.x < bx[0] || v.x > bx[1]) && !(v.y < bx[2] || v.y > bx[3]) && !(v.z < bx[4] || v.z > bx[5]) &&
-               !(v.w < bx[6] || v.w > bx[7]);
+        const float4 b0 = reinterpret_cast<const float4*>(bx_s)[0], b1 = reinterpret_cast<const float4*>(bx_s)[1];
+        return !(v.x < b0.x || v.x > b0.y) && !(v.y < b0.z || v.y > b0.w) && !(v.z < b1.x || v.z > b1.y) &&
+               !(v.w < b1.z || v.w > b1.w);
     };
     // the label predicate of the candidate at pool row p (a NaN label passes, as in the reference)
     auto label_ok = [&](uint32_t p) -> bool {
@@ -1314,7 +1313,7 @@ template <bool LAB4>
 __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, int R, int lbl, uint64_t q, Workspace w) {
     constexpr int NW = kPreThreads / 32;
     extern __shared__ __align__(16) uint32_t s_rings[];  // per warp: staged labels, queue ring, survivor ring
-    __shared__ float s_bx[NW][2 * kMaxDims];
+    __shared__ __align__(16) float s_bx[NW][2 * kMaxDims];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t n_items = w.pitem_off[q];
     for (;;) {
