@@ -452,14 +452,19 @@ def run_hdgrid(args):
                                                    info["l"], read_q, chk_q, info["rank_pack_bytes"])
     pass_share = float(pass_q[pre_q].sum() / max(1, cand_q[pre_q].sum())) if pre_q.any() else None
     launches_per_step = int(stats["launches"])
-    # the re-rank: every selected entry's pool -> id lookup (4 B) and, for a post-filter query,
-    # its labels (4*l B); every predicate survivor's full row (4*d B)
-    refine_bytes = None
+    # the re-rank: every selected entry's pool -> id lookup (4 B); for a post-filter query, its
+    # packed label ranks (4 B when kept) and the labels (4*l B) of the entries the ranks leave
+    # open; every predicate survivor's full row (4*d B)
+    refine_bytes = refine_entries = None
     if p0["exps0"] > 1:
         # after the select, cand_count holds each query's selection size
         sel_q = np.frombuffer(idx.debug_fetch("cand_count").tobytes(), np.uint32)[:nq].astype(np.float64)
         rows_q = np.frombuffer(idx.debug_fetch("refine_rows").tobytes(), np.uint32)[:nq].astype(np.float64)
-        refine_bytes = float((sel_q * 4).sum() + (sel_q[~pre_q] * 4 * info["l"]).sum() + (rows_q * 4 * info["d"]).sum())
+        lab_q = np.frombuffer(idx.debug_fetch("refine_labels_read").tobytes(), np.uint32)[:nq].astype(np.float64)
+        refine_bytes = float((sel_q * 4).sum() + (sel_q[~pre_q] * info["rank_pack_bytes"]).sum()
+                             + (lab_q * 4 * info["l"]).sum() + (rows_q * 4 * info["d"]).sum())
+        refine_entries = {"selected": int(sel_q.sum()), "selected_post_filter": int(sel_q[~pre_q].sum()),
+                          "labels_read": int(lab_q.sum()), "rows": int(rows_q.sum())}
 
     # end to end through the public API with host buffers
     q_h = torch.from_numpy(ws["queries"]).pin_memory()
@@ -544,6 +549,7 @@ def run_hdgrid(args):
         "config": workload_config(ws, args) | {"recall_at_k": rec, "build_s": round(t_build, 2),
                                                "candidates_per_step": cand,
                                                "predicate_pass_share": pass_share,
+                                               "refine_entries": refine_entries,
                                                "max_rel_dist_err_vs_fp64": max_rel}
                   | ({"schedule": "learned (LEARNED=1)"} if learned else {})
                   | ({"cuda_graph": True, "autotuned": tuned} if graph_mode else {}),

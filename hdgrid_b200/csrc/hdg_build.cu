@@ -801,6 +801,7 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const uint32_t rstride = rbits ? (1u << rbits) - 1u : 0u;
     std::vector<float> rthr((size_t)H.l * rstride);
     uint32_t rn[kMaxDims] = {0};
+    float rmin[kMaxDims] = {0.f}, rmax[kMaxDims] = {0.f};
     if (rbits) {
         const uint64_t step = std::max<uint64_t>(1, H.n / 262144);
 #pragma omp parallel for
@@ -812,6 +813,14 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
                 if (!std::isnan(x)) v.push_back(x);
             }
             std::sort(v.begin(), v.end());
+            float mn = INFINITY, mx = -INFINITY;  // over every label, not the sample
+            for (uint64_t r = 0; r < H.n; r++) {
+                const float x = H.labels[r * H.l + i];
+                mn = std::min(mn, x);
+                mx = std::max(mx, x);
+            }
+            rmin[i] = mn;
+            rmax[i] = mx;
             std::vector<float> u(v);
             u.erase(std::unique(u.begin(), u.end()), u.end());
             float* t = rthr.data() + (size_t)i * rstride;
@@ -869,9 +878,16 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     D.labels = (const float*)up(o_lab, H.labels.data(), H.labels.size() * 4);
     D.rank_bits = (uint32_t)rbits;
     D.rank_stride = rstride;
-    D.rank_guard = 0;
-    for (int i = 0; i < kMaxDims; i++) D.rank_n[i] = i < (int)H.l ? rn[i] : 0u;
-    for (int i = 0; rbits && i < (int)H.l; i++) D.rank_guard |= 1u << (i * (rbits + 1) + rbits);
+    D.rank_guard = D.rank_full = 0;
+    for (int i = 0; i < kMaxDims; i++) {
+        D.rank_n[i] = i < (int)H.l ? rn[i] : 0u;
+        D.rank_min[i] = i < (int)H.l ? rmin[i] : 0.f;
+        D.rank_max[i] = i < (int)H.l ? rmax[i] : 0.f;
+    }
+    for (int i = 0; rbits && i < (int)H.l; i++) {
+        D.rank_guard |= 1u << (i * (rbits + 1) + rbits);
+        D.rank_full |= rn[i] << (i * (rbits + 1));
+    }
     D.rank_thr = rbits ? (const float*)up(o_rt, rthr.data(), rthr.size() * 4) : nullptr;
     D.rankpack = rbits ? reinterpret_cast<const uint32_t*>(base + o_pk) : nullptr;
     if (rbits) {

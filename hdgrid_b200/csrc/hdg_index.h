@@ -108,13 +108,16 @@ struct IndexDev {
     // 2^rank_bits - 1 ascending thresholds rank_thr[i * rank_stride + k], k < rank_n[i]; a
     // label's rank is the number of thresholds at or below it.  rankpack holds every point's
     // ranks in pool order, dim i in bits [i * (rank_bits + 1), +rank_bits) with a zero guard bit
-    // above (rank_guard = the guard bits).  A rank outside the query's rank box proves the label
-    // test fails, so the predicate pass reads labels only for candidates inside it.
-    // rankpack = nullptr when the label dims do not fit 32 bits.
+    // above (rank_guard = the guard bits; rank_full = every rank_n[i] in its field).  The labels
+    // of rank r lie in [thr[r - 1], thr[r]), with rank_min / rank_max (the smallest and largest
+    // label of the dim) closing the two ends.  A rank outside the query's rank box proves that
+    // the label test fails; a rank inside its inner box proves that it passes.  Only the others
+    // need their labels read.  rankpack = nullptr when the label dims do not fit 32 bits.
     const uint32_t* rankpack;
     const float* rank_thr;
     uint32_t rank_n[kMaxDims];
-    uint32_t rank_bits, rank_stride, rank_guard;
+    float rank_min[kMaxDims], rank_max[kMaxDims];
+    uint32_t rank_bits, rank_stride, rank_guard, rank_full;
     uint32_t labels_nan;           // some label is NaN (passes every label test, in any cell)
     const uint32_t* ids;
     const uint8_t* codes;

@@ -45,7 +45,7 @@ constexpr uint32_t kPreChunk = 8192; // candidates per work item of the predicat
 struct Workspace {
     float* box;              // [q x 2l]
     int* cells;              // [q x 2l]
-    uint32_t* rank_box;      // [q x 2] rank box: low ranks, high ranks | guard bits (0: rejects nothing)
+    uint32_t* rank_box;      // [q x 4] rank box (low ranks, high ranks | guard bits), inner box (same)
     uint64_t* zrange;        // [q x 2]
     uint32_t* list_counts;   // [q x L]
     uint32_t* cluster_counts;// [q x C]
@@ -75,6 +75,7 @@ struct Workspace {
     uint32_t* ritem_off;     // [q + 1] refine work-item offsets (k_refine_plan)
     uint32_t* rdone;         // [q] refine items finished per query
     uint32_t* rsurv;         // [q] rows re-ranked exactly per query (predicate survivors of the selection)
+    uint32_t* rlab;          // [q] selected entries whose labels the re-rank read (the ranks left them open)
     uint64_t* rpart;         // [refine items x k_max] best keys of each refine item
     int surv_list;           // 1: the predicate pass lists each predicate-first query's survivors
     float* dist;             // [sum of candidates]
@@ -204,12 +205,12 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
     __shared__ int s_cells[2 * kMaxDims];
     __shared__ uint64_t s_corner[1 << kMaxDims];
     __shared__ int s_sign[1 << kMaxDims];
-    __shared__ uint32_t s_rank[3];
+    __shared__ uint32_t s_rank[4];
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
     const int l = g.l;
     const uint32_t L = D.n_lists;
-    if (t < 3) s_rank[t] = 0;
+    if (t < 4) s_rank[t] = 0;
     if (t < l) {
         float lo, hi;
         recover_dim(f, qlabels + qi * label_cols, t, &lo, &hi);
@@ -220,25 +221,32 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
     }
     __syncthreads();
     if (t < l && D.rankpack) {
-        // the rank box of label dim t: a rank below that of lo means a label below a threshold
-        // <= lo, a rank above that of hi a label above a threshold > hi (NaN bounds reject nothing)
+        // The rank box of label dim t: a rank below that of lo holds labels below a threshold
+        // <= lo, a rank above that of hi labels at or above a threshold > hi.  The inner box:
+        // ranks whose labels all lie in [lo, hi] -- above the rank of the largest threshold
+        // below lo (or every rank when the dim's smallest label is >= lo), and below the rank
+        // of hi (or every rank when its largest label is <= hi).  NaN bounds reject nothing.
         const float blo = s_box[2 * t], bhi = s_box[2 * t + 1];
         const float* thr = D.rank_thr + (uint64_t)t * D.rank_stride;
         const uint32_t n = D.rank_n[t];
-        auto rank = [&](float x) {
+        auto count = [&](float x, bool le) {  // thresholds <= x (le) or < x
             uint32_t a = 0, b = n;
             while (a < b) {
                 const uint32_t m = (a + b) >> 1;
-                if (thr[m] <= x) a = m + 1;
+                if (le ? thr[m] <= x : thr[m] < x) a = m + 1;
                 else b = m;
             }
             return a;
         };
-        const uint32_t rlo = isnan(blo) ? 0u : rank(blo), rhi = isnan(bhi) ? n : rank(bhi);
+        const uint32_t rlo = isnan(blo) ? 0u : count(blo, true), rhi = isnan(bhi) ? n : count(bhi, true);
+        const int ilo = isnan(blo) || D.rank_min[t] >= blo ? 0 : (int)count(blo, false) + 1;
+        const int ihi = isnan(bhi) || D.rank_max[t] <= bhi ? (int)n : (int)rhi - 1;
+        const bool empty = ilo > ihi;  // no rank is sure to pass: the field's box [1, 0]
         const int off = t * (int)(D.rank_bits + 1);
         if (rlo) atomicOr(&s_rank[0], rlo << off);
         atomicOr(&s_rank[1], rhi << off);
-        if (rlo > 0 || rhi < n) s_rank[2] = 1;
+        if (empty || ilo) atomicOr(&s_rank[2], (empty ? 1u : (uint32_t)ilo) << off);
+        if (!empty && ihi) atomicOr(&s_rank[3], (uint32_t)ihi << off);
     }
     if (t < l) {
         const int od = g.shuffle[t];
@@ -258,8 +266,10 @@ __global__ void __launch_bounds__(kThreads) k_prologue(IndexDev D, GridMeta g, F
         }
         w.zrange[qi * 2] = morton_encode(clo, g.morton_dims, g.morton_max_bits, g.morton_valid_map);
         w.zrange[qi * 2 + 1] = morton_encode(chi, g.morton_dims, g.morton_max_bits, g.morton_valid_map);
-        w.rank_box[qi * 2] = s_rank[0];
-        w.rank_box[qi * 2 + 1] = s_rank[2] ? s_rank[1] | D.rank_guard : 0u;
+        w.rank_box[qi * 4] = s_rank[0];
+        w.rank_box[qi * 4 + 1] = s_rank[1] | D.rank_guard;
+        w.rank_box[qi * 4 + 2] = s_rank[2];
+        w.rank_box[qi * 4 + 3] = s_rank[3] | D.rank_guard;
     }
     // corners of the cell box over the valid (unmasked) dims (get_prefix_sum_device :693-724)
     const int dv = __popc(g.morton_valid_map);
@@ -1333,8 +1343,9 @@ __global__ void __launch_bounds__(kPreThreads, 4) k_pre_scan(IndexDev D, int R, 
         // NaN labels (a NaN passes the label test), or when the query's count of points in its
         // cell box over the probed lists says that most candidates pass anyway.
         const uint32_t inbox = w.qstat[(uint64_t)qq * 4 + 1];
-        const uint32_t rlo = w.rank_box[2 * qq], rhi = w.rank_box[2 * qq + 1];
-        const bool use = rhi != 0 && D.rankpack && !D.labels_nan && (uint64_t)inbox * 16 < (uint64_t)total * 12;
+        const uint32_t rlo = w.rank_box[4 * qq], rhi = w.rank_box[4 * qq + 1];
+        const bool use = D.rankpack && !D.labels_nan && (rlo != 0 || rhi != (D.rank_full | D.rank_guard)) &&
+                         (uint64_t)inbox * 16 < (uint64_t)total * 12;
         __syncwarp();  // s_bx is written
         const uint32_t* pre = w.range_pre + (uint64_t)qq * (R + 1);
         const uint32_t* start = w.range_start + (uint64_t)qq * R;
@@ -2013,6 +2024,7 @@ __global__ void __launch_bounds__(1024) k_refine_plan(uint64_t q, Workspace w) {
         r += max(1u, (w.cand_count[i] + kRefChunk - 1) / kRefChunk);
         w.rdone[i] = 0;
         w.rsurv[i] = 0;
+        w.rlab[i] = 0;
     }
     if (e == q && b < e) w.ritem_off[q] = (uint32_t)r;
     if (t == 0) w.counter[1] = 0;
@@ -2076,6 +2088,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
     __shared__ int s_wsum[kThreads / 32];
     __shared__ int s_cnt, s_ns, s_item, s_qi, s_last;
     __shared__ uint64_t s_th;
+    __shared__ uint32_t s_rb[4];
     __shared__ uint32_t s_rhist[256], s_rwc[32];
     __shared__ unsigned long long s_rsel[4];
     const RefSel rs{s_rhist, s_rwc, s_rsel};
@@ -2104,6 +2117,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
         if ((int)qi != cur) {
             for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
             if (t < 2 * lbl) s_box[t] = w.box[qi * 2 * lbl + t];
+            if (t < 4) s_rb[t] = w.rank_box[qi * 4 + t];
             cur = (int)qi;
         }
         if (t == 0) {
@@ -2117,9 +2131,13 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
         const int nc = (int)(min(w.cand_count[qi], c0 + kRefChunk) - min(w.cand_count[qi], c0));
         const int kq = (int)q_k(w, qi);
         const bool pred_q = apply_pred && q_sched(w, qi) == 0;  // predicate-first queries already passed it
+        // label ranks decide most entries: outside the rank box fails, inside the inner box passes
+        const bool ranks = D.rankpack && !D.labels_nan;
+        const uint32_t gd = D.rank_guard;
         uint32_t* list = w.cand_pool + w.soff[qi] + c0;
         // 1. the predicate survivors, compacted in place as original ids (each chunk is read
         //    before the barrier and written at or below its own start)
+        uint32_t n_lab = 0;
         for (int base = 0; base < nc; base += kThreads) {
             const int e = base + t;
             bool keep = false;
@@ -2128,10 +2146,21 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
                 pool = list[e];
                 keep = pool != kInvalid;
                 if (keep && pred_q) {
-                    const float* lab = D.labels + (uint64_t)pool * lbl;
-                    for (int i = 0; i < lbl; i++) {
-                        const float v = lab[i];
-                        if (v < s_box[2 * i] || v > s_box[2 * i + 1]) keep = false;
+                    bool sure = false;
+                    if (ranks) {
+                        const uint32_t c = __ldg(D.rankpack + pool);
+                        const uint32_t to = ((c | gd) - s_rb[0]) & (s_rb[1] - c);
+                        const uint32_t ti = ((c | gd) - s_rb[2]) & (s_rb[3] - c);
+                        keep = (to & gd) == gd;
+                        sure = (ti & gd) == gd;
+                    }
+                    if (keep && !sure) {
+                        n_lab++;
+                        const float* lab = D.labels + (uint64_t)pool * lbl;
+                        for (int i = 0; i < lbl; i++) {
+                            const float v = lab[i];
+                            if (v < s_box[2 * i] || v > s_box[2 * i + 1]) keep = false;
+                        }
                     }
                 }
             }
@@ -2147,6 +2176,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
             __syncthreads();
             if (t == 0) s_ns += tot;
         }
+        n_lab = __reduce_add_sync(0xffffffffu, n_lab);
+        if (lane == 0 && n_lab) atomicAdd(&w.rlab[qi], n_lab);
         __syncthreads();
         const int ns = s_ns;
         if (t == 0 && ns) atomicAdd(&w.rsurv[qi], (uint32_t)ns);
@@ -2298,7 +2329,7 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     Workspace w{};
     w.box = (float*)take("box", q * 2 * l * 4);
     w.cells = (int*)take("cells", q * 2 * l * 4);
-    w.rank_box = (uint32_t*)take("rank_box", q * 2 * 4);
+    w.rank_box = (uint32_t*)take("rank_box", q * 4 * 4);
     w.zrange = (uint64_t*)take("zrange", q * 2 * 8);
     w.list_counts = (uint32_t*)take("list_counts", q * L * 4);
     w.cluster_counts = (uint32_t*)take("cluster_counts", q * C * 4);
@@ -2328,6 +2359,7 @@ static Workspace carve(hdg_index* idx, QueryCtx& cx, uint64_t q, bool record) {
     w.ritem_off = (uint32_t*)take("refine_items", (q + 1) * 4);
     w.rdone = (uint32_t*)take("refine_done", q * 4);
     w.rsurv = (uint32_t*)take("refine_rows", q * 4);
+    w.rlab = (uint32_t*)take("refine_labels_read", q * 4);
     w.ldS = C + L;
     w.S = (float*)take("gemm_s", q * (C + L) * 4);
     w.qnorm = (float*)take("qnorm", q * 4);

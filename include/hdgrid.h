@@ -226,7 +226,9 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
  * "probe_lists", "range_start", "range_len", "cand_count", "budget", "sel_off", "scalars",
  * "qoff", "qstat", "labels_read" (candidates of the predicate pass whose labels were read),
  * "ranks_read" (candidates of the predicate pass whose packed label ranks were read),
- * "distances" (the f32 ADC distance of every scanned candidate, query rows
+ * "rank_box" (per query: the label-rank box and its inner box, four words), "refine_rows"
+ * (rows the re-rank computed exactly), "refine_labels_read" (selected entries whose labels
+ * the re-rank read), "distances" (the f32 ADC distance of every scanned candidate, query rows
  * at the "qoff" offsets) and "cand_pool" (each query's selected candidates, rows at the
  * "sel_off" offsets, "cand_count" of them). */
 hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,

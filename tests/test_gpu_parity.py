@@ -202,6 +202,20 @@ def test_parity_prefilter_compacted_scan(cuda):
     assert np.all(read <= cand) and read.sum() < cand.sum()
 
 
+def _few_values(ws):
+    # dim 1 holds 5 distinct values, dim 3 one; every third query's dim-1 box has bounds equal
+    # to two of the values
+    ws = dict(ws)
+    lab = ws["labels"].copy()
+    lab[:, 1] = (lab[:, 1] // 200_000) * 200_000
+    lab[:, 3] = 500_000
+    ql = ws["query_labels"].copy()
+    ql[::3, 2] = 200_000
+    ql[::3, 3] = 400_000
+    ws["labels"], ws["query_labels"] = lab, ql
+    return ws
+
+
 def test_parity_prefilter_label_ranks(cuda):
     # the predicate pass tests each candidate's packed label ranks (a guarded field per label dim:
     # the number of the index's per-dim thresholds at or below the label) against the query's
@@ -213,16 +227,7 @@ def test_parity_prefilter_label_ranks(cuda):
                               max_grids=20_000, exps0=1)]
     ws = datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
                           max_grids=4096, exps0=1)
-    cases.append(ws)
-    ws = dict(ws)
-    lab = ws["labels"].copy()
-    lab[:, 1] = (lab[:, 1] // 200_000) * 200_000  # 5 distinct values
-    lab[:, 3] = 500_000                             # one value
-    ql = ws["query_labels"].copy()
-    ql[::3, 2] = 200_000                            # box bounds on the values themselves
-    ql[::3, 3] = 400_000
-    ws["labels"], ws["query_labels"] = lab, ql
-    cases.append(ws)
+    cases += [ws, _few_values(ws)]
     for ws in cases:
         idx, r = _parity(ws, cuda, exact_ids=True, adc_rotated=True)
         info = idx.info()
@@ -237,6 +242,20 @@ def test_parity_prefilter_label_ranks(cuda):
         read = np.frombuffer(idx.debug_fetch("labels_read").tobytes(), np.uint32)[:nq]
         chk = np.frombuffer(idx.debug_fetch("ranks_read").tobytes(), np.uint32)[:nq]
         assert read.sum() < chk.sum(), (read.sum(), chk.sum())
+
+
+def test_parity_postfilter_label_ranks(cuda):
+    # post-filter: the re-rank reads an entry's labels only when its ranks sit on the rank box's
+    # edge (outside the box fails, inside the inner box passes); each query's ids equal the
+    # oracle's
+    for ws in (datasets.config4(scale=0.004, n_queries=300, clusters=16, sub_clusters=4, n_list=8, sub_lists=32,
+                                max_grids=4096, exps0=32),):
+        for w in (ws, _few_values(ws)):
+            idx, r = _parity(w, cuda, exact_ids=True, adc_rotated=True)  # every query's id set equal
+            nq = w["queries"].shape[0]
+            sel = np.frombuffer(idx.debug_fetch("cand_count").tobytes(), np.uint32)[:nq]
+            lab = np.frombuffer(idx.debug_fetch("refine_labels_read").tobytes(), np.uint32)[:nq]
+            assert 0 < lab.sum() < sel.sum(), (lab.sum(), sel.sum())
 
 
 def test_parity_prefilter_rotated_adc_fp16_lut(cuda):
