@@ -137,6 +137,18 @@ __device__ __forceinline__ uint64_t budget_of(const Workspace& w, uint64_t qi, f
     return max((uint64_t)1, min(K, (uint64_t)0xffffffffu));
 }
 __device__ __forceinline__ uint32_t q_budget(const Workspace& w, uint64_t qi) { return w.qbud[qi]; }
+// A compact row (predicate survivors) that its budget takes whole: the selection is the row
+// itself -- its distance slots still hold the survivors' pool rows, as the ADC scan leaves such
+// a row alone -- so the select skips it and the re-rank reads the row in place.  (nfin: the
+// row's survivors, which the select does not change, unlike cand_count.)
+__device__ __forceinline__ bool takes_row(const Workspace& w, uint64_t qi) {
+    return compacts(w, qi) && w.nfin[qi] <= q_budget(w, qi);
+}
+// The selected candidates (pool rows) of query qi: its row of the selection buffer, or its
+// distance row when it takes the row whole
+__device__ __forceinline__ uint32_t* sel_row(const Workspace& w, uint64_t qi) {
+    return takes_row(w, qi) ? reinterpret_cast<uint32_t*>(w.dist + w.qoff[qi]) : w.cand_pool + w.soff[qi];
+}
 
 // Warp-wide sum / maximum of a u64 (every lane gets it)
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
@@ -1735,13 +1747,11 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     // in arrival order with their candidate positions beside them (cand_count entries); any
     // other query's row holds one distance per candidate position.
     const bool compact = compacts(w, qi);
+    if (!sorted_out && takes_row(w, qi)) return;  // the selection is the row (cand_count entries)
     const uint32_t total = compact ? w.cand_count[qi] : w.qstat[qi * 4];
     const float* dist = w.dist + w.qoff[qi];
     const uint32_t* prow = compact ? w.spos + w.qoff[qi] : nullptr;
-    // a compact row that its budget takes whole: every survivor, and the distance slots still
-    // hold the survivors' pool rows (the ADC scan left the row alone), so no range table either
-    const bool take_all = compact && !sorted_out && total <= q_budget(w, qi);
-    if (!take_all) {
+    {
         const uint32_t* rpre = w.range_pre + qi * (Ps + 1);
         for (int i = t; i <= Ps; i += blockDim.x) s_pre[i] = rpre[i];
         for (int i = t; i < Ps; i += blockDim.x) s_start[i] = w.range_start[qi * Ps + i];
@@ -1798,12 +1808,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
             }
         }
     };
-    if (take_all) {
-        const uint32_t* rows = reinterpret_cast<const uint32_t*>(dist);
-        for (uint32_t e = t; e < total; e += blockDim.x) sel_dst[e] = rows[e];
-        if (t == 0) s_out = total;
-        __syncthreads();
-    } else if (need0 > 0 && nfin <= (uint32_t)K) {
+    if (need0 > 0 && nfin <= (uint32_t)K) {
         // every finite candidate is selected (the loop bound is block-uniform so that every
         // lane reaches the warp appends)
         for (uint32_t base = 0; base < total; base += blockDim.x) {
@@ -1977,8 +1982,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(IndexDev D, int Ps, int 
     const uint32_t nsel = s_out;
     if (!sorted_out) {
         uint32_t* pool = w.cand_pool + w.soff[qi];
-        if (!take_all)  // positions to pool rows (a whole compact row holds pool rows already)
-            for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
+        for (uint32_t i = t; i < nsel; i += blockDim.x) pool[i] = pos_to_pool(s_pre, s_start, Ps, pool[i]);
         if (t == 0) w.cand_count[qi] = nsel;
         return;
     }
@@ -2134,7 +2138,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
         // label ranks decide most entries: outside the rank box fails, inside the inner box passes
         const bool ranks = D.rankpack && !D.labels_nan;
         const uint32_t gd = D.rank_guard;
-        uint32_t* list = w.cand_pool + w.soff[qi] + c0;
+        uint32_t* list = sel_row(w, qi) + c0;
         // 1. the predicate survivors, compacted in place as original ids (each chunk is read
         //    before the barrier and written at or below its own start)
         uint32_t n_lab = 0;

@@ -230,7 +230,8 @@ int hdg_last_stage_times(const hdg_index* index, float* ms, const char** names, 
  * (rows the re-rank computed exactly), "refine_labels_read" (selected entries whose labels
  * the re-rank read), "distances" (the f32 ADC distance of every scanned candidate, query rows
  * at the "qoff" offsets) and "cand_pool" (each query's selected candidates, rows at the
- * "sel_off" offsets, "cand_count" of them). */
+ * "sel_off" offsets, "cand_count" of them; a predicate-first query whose budget takes all its
+ * survivors keeps them, as pool rows, in its "distances" row instead). */
 hdg_status hdg_debug_fetch(const hdg_index* index, const char* name, void* host_dst,
                            size_t bytes, size_t* bytes_needed);
 
