@@ -44,6 +44,7 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
                uint32_t label_cols, const float* d_data, uint32_t k, float* d_dist, uint64_t* d_ids,
                cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,
                const uint8_t* d_sched = nullptr);
+int sm_count();  // SMs of the current device
 // learned per-query schedule (hdg_learned.cu): 48 features -> 128 -> 128 -> 2 BF16 MLP,
 // parameters W1 [128 x 48], b1, W2 [128 x 128], b2, W3 [2 x 128], b3 in one f32 vector
 constexpr int kMlpFeatures = 48, kMlpHidden = 128, kMlpOut = 2;

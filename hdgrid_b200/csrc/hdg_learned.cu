@@ -189,8 +189,10 @@ __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const 
 }
 
 // ---- forward ---------------------------------------------------------------------------
-// Block = kTile samples, 128 threads (one hidden unit each).  Weights staged transposed in
-// shared memory (thread o reads column o: conflict-free), inputs broadcast.
+// 128 threads (one hidden unit each), persistent over tiles of kTile samples: the weights are
+// staged once per block, unit-major with rows padded by one word (49 and 129), so that both
+// the staging writes and the reads of unit t's row across the threads are conflict-free;
+// inputs are broadcast.
 struct FwdOut {
     float* z;            // [n x 2]
     float* a1;           // [n x 128] hidden 1 (bf16-rounded), training only
@@ -203,73 +205,79 @@ struct FwdOut {
 
 __global__ void __launch_bounds__(kMlpHidden) k_mlp_forward(Params P, const float* __restrict__ x, uint64_t n,
                                                             FwdOut o) {
+    constexpr int S1 = kMlpFeatures + 1, S2 = kMlpHidden + 1;  // padded weight rows
+    constexpr int SH = kTile + 4;  // activation rows: 16-byte aligned, 4-way conflicts at most on the writes
     extern __shared__ __align__(16) float sm[];
-    float* w1t = sm;                                   // [48][128]
-    float* w2t = w1t + kMlpFeatures * kMlpHidden;      // [128][128]
-    float* w3 = w2t + kMlpHidden * kMlpHidden;         // [2][128]
-    float* xs = w3 + kMlpOut * kMlpHidden;             // [kTile][48]
-    float* h1 = xs + kTile * kMlpFeatures;             // [kTile][128]
-    float* h2 = h1 + kTile * kMlpHidden;               // [kTile][128]
+    float* w1p = sm;                                   // [128][49]: unit-major W1
+    float* w2p = w1p + kMlpHidden * S1;                // [128][129]
+    float* w3 = w2p + kMlpHidden * S2;                 // [2][128]
+    float* xs = w3 + kMlpOut * kMlpHidden;             // [48][kTile]: feature-major inputs
+    float* h1 = xs + kMlpFeatures * kTile;             // [128][SH]: unit-major activations
+    float* h2 = h1 + kMlpHidden * SH;                  // [128][SH]
     const int t = threadIdx.x;
-    for (int e = t; e < kMlpHidden * kMlpFeatures; e += blockDim.x) {
-        const int oo = e / kMlpFeatures, i = e % kMlpFeatures;
-        w1t[i * kMlpHidden + oo] = __bfloat162float(P.w[kMlpW1 + e]);
-    }
-    for (int e = t; e < kMlpHidden * kMlpHidden; e += blockDim.x) {
-        const int oo = e / kMlpHidden, j = e % kMlpHidden;
-        w2t[j * kMlpHidden + oo] = __bfloat162float(P.w[kMlpW2 + e]);
-    }
+    for (int e = t; e < kMlpHidden * kMlpFeatures; e += blockDim.x)
+        w1p[(e / kMlpFeatures) * S1 + e % kMlpFeatures] = __bfloat162float(P.w[kMlpW1 + e]);
+    for (int e = t; e < kMlpHidden * kMlpHidden; e += blockDim.x)
+        w2p[(e / kMlpHidden) * S2 + e % kMlpHidden] = __bfloat162float(P.w[kMlpW2 + e]);
     for (int e = t; e < kMlpOut * kMlpHidden; e += blockDim.x) w3[e] = __bfloat162float(P.w[kMlpW3 + e]);
-    const uint64_t b0 = (uint64_t)blockIdx.x * kTile;
-    for (int e = t; e < kTile * kMlpFeatures; e += blockDim.x) {
-        const uint64_t b = b0 + e / kMlpFeatures;
-        xs[e] = b < n ? bf16r(x[b0 * kMlpFeatures + e]) : 0.f;
-    }
-    __syncthreads();
-    float acc[kTile];
     const float bias1 = P.master[kMlpB1 + t], bias2 = P.master[kMlpB2 + t];
+    // one hidden layer: acc[b] = sum over r of w[r] * in[r][b], in order r = 0, 1, ... (the
+    // sample's inputs read four at a time as broadcasts)
+    auto layer = [&](const float* wrow, const float* in, int rows, int ld, float (&acc)[kTile]) {
 #pragma unroll
-    for (int b = 0; b < kTile; b++) acc[b] = 0.f;
-    for (int i = 0; i < kMlpFeatures; i++) {
-        const float wv = w1t[i * kMlpHidden + t];
+        for (int b = 0; b < kTile; b++) acc[b] = 0.f;
+        for (int r = 0; r < rows; r++) {
+            const float wv = wrow[r];
+            const float4* v = reinterpret_cast<const float4*>(in + r * ld);
 #pragma unroll
-        for (int b = 0; b < kTile; b++) acc[b] = fmaf(wv, xs[b * kMlpFeatures + i], acc[b]);
-    }
-#pragma unroll
-    for (int b = 0; b < kTile; b++) h1[b * kMlpHidden + t] = bf16r(fmaxf(acc[b] + bias1, 0.f));
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < kTile; b++) acc[b] = 0.f;
-    for (int j = 0; j < kMlpHidden; j++) {
-        const float wv = w2t[j * kMlpHidden + t];
-#pragma unroll
-        for (int b = 0; b < kTile; b++) acc[b] = fmaf(wv, h1[b * kMlpHidden + j], acc[b]);
-    }
-#pragma unroll
-    for (int b = 0; b < kTile; b++) h2[b * kMlpHidden + t] = bf16r(fmaxf(acc[b] + bias2, 0.f));
-    __syncthreads();
-    if (o.a1) {
-        for (int e = t; e < kTile * kMlpHidden; e += blockDim.x) {
-            const uint64_t b = b0 + e / kMlpHidden;
-            if (b < n) {
-                o.a1[b0 * kMlpHidden + e] = h1[e];
-                o.a2[b0 * kMlpHidden + e] = h2[e];
+            for (int b4 = 0; b4 < kTile / 4; b4++) {
+                const float4 a = v[b4];
+                acc[4 * b4] = fmaf(wv, a.x, acc[4 * b4]);
+                acc[4 * b4 + 1] = fmaf(wv, a.y, acc[4 * b4 + 1]);
+                acc[4 * b4 + 2] = fmaf(wv, a.z, acc[4 * b4 + 2]);
+                acc[4 * b4 + 3] = fmaf(wv, a.w, acc[4 * b4 + 3]);
             }
         }
-    }
-    if (t < kTile * kMlpOut) {
-        const int b = t >> 1, c = t & 1;
-        float z = 0.f;
-        for (int j = 0; j < kMlpHidden; j++) z = fmaf(w3[c * kMlpHidden + j], h2[b * kMlpHidden + j], z);
-        z += P.master[kMlpB3 + c];
-        const uint64_t bi = b0 + b;
-        if (bi < n) {
-            if (o.z) o.z[bi * kMlpOut + c] = z;
-            if (c == 0 && o.nprobe) {
-                const float p = exp2f(fminf(fmaxf(z, 0.f), 20.f));
-                o.nprobe[bi] = (uint32_t)min((float)o.max_probe, fmaxf(1.f, rintf(p)));
+    };
+    for (uint64_t b0 = (uint64_t)blockIdx.x * kTile; b0 < n; b0 += (uint64_t)gridDim.x * kTile) {
+        __syncthreads();  // the weights are staged; the previous tile's reads are done
+        for (int e = t; e < kTile * kMlpFeatures; e += blockDim.x) {
+            const int i = e / kTile, b = e % kTile;
+            xs[e] = b0 + b < n ? bf16r(x[(b0 + b) * kMlpFeatures + i]) : 0.f;
+        }
+        __syncthreads();
+        float acc[kTile];
+        layer(w1p + t * S1, xs, kMlpFeatures, kTile, acc);
+#pragma unroll
+        for (int b = 0; b < kTile; b++) h1[t * SH + b] = bf16r(fmaxf(acc[b] + bias1, 0.f));
+        __syncthreads();
+        layer(w2p + t * S2, h1, kMlpHidden, SH, acc);
+#pragma unroll
+        for (int b = 0; b < kTile; b++) h2[t * SH + b] = bf16r(fmaxf(acc[b] + bias2, 0.f));
+        __syncthreads();
+        if (o.a1) {
+            for (int e = t; e < kTile * kMlpHidden; e += blockDim.x) {
+                const int b = e / kMlpHidden, u = e % kMlpHidden;
+                if (b0 + b < n) {
+                    o.a1[(b0 + b) * kMlpHidden + u] = h1[u * SH + b];
+                    o.a2[(b0 + b) * kMlpHidden + u] = h2[u * SH + b];
+                }
             }
-            if (c == 1 && o.sched) o.sched[bi] = (o.allow_sched && z > 0.f) ? 1 : 0;
+        }
+        if (t < kTile * kMlpOut) {
+            const int b = t >> 1, c = t & 1;
+            float z = 0.f;
+            for (int j2 = 0; j2 < kMlpHidden; j2++) z = fmaf(w3[c * kMlpHidden + j2], h2[j2 * SH + b], z);
+            z += P.master[kMlpB3 + c];
+            const uint64_t bi = b0 + b;
+            if (bi < n) {
+                if (o.z) o.z[bi * kMlpOut + c] = z;
+                if (c == 0 && o.nprobe) {
+                    const float p = exp2f(fminf(fmaxf(z, 0.f), 20.f));
+                    o.nprobe[bi] = (uint32_t)min((float)o.max_probe, fmaxf(1.f, rintf(p)));
+                }
+                if (c == 1 && o.sched) o.sched[bi] = (o.allow_sched && z > 0.f) ? 1 : 0;
+            }
         }
     }
 }
@@ -375,14 +383,19 @@ ModelPtrs model_ptrs(hdg_index* idx) {
 }
 
 size_t forward_smem() {
-    return sizeof(float) * (kMlpFeatures * kMlpHidden + kMlpHidden * kMlpHidden + kMlpOut * kMlpHidden +
-                            kTile * kMlpFeatures + 2 * kTile * kMlpHidden);
+    return sizeof(float) * ((kMlpFeatures + 1) * kMlpHidden + (kMlpHidden + 1) * kMlpHidden + kMlpOut * kMlpHidden +
+                            kTile * kMlpFeatures + 2 * (kTile + 4) * kMlpHidden);
 }
 
 void launch_forward(const ModelPtrs& mp, const float* x, uint64_t n, const FwdOut& o, cudaStream_t st) {
     const size_t sm = forward_smem();
     CK(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_mlp_forward<<<(unsigned)((n + kTile - 1) / kTile), kMlpHidden, sm, st>>>(Params{mp.master, mp.w}, x, n, o);
+    // persistent over the tiles: as many blocks as fit at once (each stages the weights once)
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_forward, kMlpHidden, sm));
+    const uint64_t tiles = (n + kTile - 1) / kTile;
+    const uint64_t blocks = std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)sm_count() * std::max(per_sm, 1)));
+    k_mlp_forward<<<(unsigned)blocks, kMlpHidden, sm, st>>>(Params{mp.master, mp.w}, x, n, o);
     CK_LAUNCH();
 }
 

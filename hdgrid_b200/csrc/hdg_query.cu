@@ -2524,6 +2524,8 @@ int occupancy_blocks(K kernel, int threads, size_t smem) {
     return std::max(nb, 1);
 }
 
+}  // namespace
+
 int sm_count() {
     static int n = 0;
     if (!n) {
@@ -2533,7 +2535,6 @@ int sm_count() {
     }
     return n;
 }
-}  // namespace
 
 struct QueryCall {
     const float* queries;
