@@ -298,11 +298,11 @@ __device__ __forceinline__ void block_compact_keys(uint64_t* keys, int n, uint32
 
 // The k smallest keys of keys[0, n) (the keys other than ~0 distinct, at least k of them):
 // compacted to keys[0, k) in their original relative order, the rest set to ~0; returns the
-// k-th smallest.  A radix select over 8-bit digits from the most significant one, stopping
+// k-th smallest (compact = false: only returns it, the keys stay as they are).  A radix select over 8-bit digits from the most significant one, stopping
 // once one key is left in the chosen digit's bin, then one compaction.  All threads; s_hist:
 // 256 words, s_wc: 32 words, s_sel: 4 words of shared scratch.
 __device__ __forceinline__ uint64_t block_select_smallest(uint64_t* keys, int n, int k, uint32_t* s_hist, uint32_t* s_wc,
-                                          unsigned long long* s_sel) {
+                                          unsigned long long* s_sel, bool compact = true) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     // the bytes above the highest one where the smallest and largest key differ are common to
     // every key: the select starts below them
@@ -383,6 +383,7 @@ __device__ __forceinline__ uint64_t block_select_smallest(uint64_t* keys, int n,
     }
     __syncthreads();
     const uint64_t kth = s_sel[3];
+    if (!compact) return kth;
     for (int i = t; i < n; i += blockDim.x)
         if (keys[i] > kth) keys[i] = ~0ull;
     __syncthreads();

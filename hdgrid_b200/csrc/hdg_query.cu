@@ -526,8 +526,9 @@ constexpr int kCoarseThreads = 128;
 __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta g, const float* __restrict__ queries,
                                                      int Pc, int Ps, int sort_n1, int sort_n2,
                                                      Workspace w) {
-    extern __shared__ uint64_t s_keys[];  // [max(sort_n1, sort_n2)] then query vector
-    float* s_q = reinterpret_cast<float*>(s_keys + max(sort_n1, sort_n2));
+    extern __shared__ uint64_t s_keys[];  // [max(sort_n1, sort_n2)], then the bands' lows, the query vector
+    float* s_lo = reinterpret_cast<float*>(s_keys + max(sort_n1, sort_n2));
+    float* s_q = s_lo + max(sort_n1, sort_n2);
     __shared__ uint32_t s_chosen[1024];
     __shared__ uint32_t s_red[2];
     __shared__ uint32_t s_wc[32];
@@ -539,17 +540,30 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     const uint64_t qi = blockIdx.x;
     const int t = threadIdx.x;
     const int d = D.d;
+    const bool est = w.S != nullptr;  // tensor-core estimates of the centroid distances
     for (int i = t; i < d; i += blockDim.x) s_q[i] = queries[qi * d + i];
     if (t == 0) {
         s_nvalid = 0;
         s_red[0] = s_red[1] = 0;
     }
     __syncthreads();
-    // clusters with a non-zero filtered count (filter_none_zero_data :1027-1028).  When all
-    // of them fit in n_list the ranking cannot change the chosen set: no distances needed.
+    // One pass over the clusters: those with a non-zero filtered count (filter_none_zero_data
+    // :1027-1028) get a key -- the upper end of their estimate band and the cluster -- and the
+    // band's lower end; the others ~0.  When all of them fit in n_list the ranking cannot change
+    // the chosen set: no distances needed.
     {
         uint32_t nz = 0;
-        for (int c = t; c < (int)D.C; c += blockDim.x) nz += w.cluster_counts[qi * D.C + c] > 0 ? 1u : 0u;
+        for (int c = t; c < sort_n1; c += blockDim.x) {
+            uint64_t key = ~0ull;
+            if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
+                float lo = 0.f, hi = 0.f;
+                if (est) approx_band(D, w, qi, c, &lo, &hi);
+                key = ((uint64_t)float_key(hi) << 32) | (uint32_t)c;
+                s_lo[c] = lo;
+                nz++;
+            }
+            s_keys[c] = key;
+        }
         nz = __reduce_add_sync(0xffffffffu, nz);  // one shared atomic per warp
         if ((t & 31) == 0 && nz) atomicAdd(&s_nvalid, (int)nz);
     }
@@ -557,35 +571,18 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     const bool all_c = s_nvalid <= Pc;
     // With the tensor-core estimates, only clusters whose lower bound is below the n_list-th
     // smallest upper bound can be in the exact top n_list; only those get exact distances.
-    const bool prune_c = !all_c && w.S != nullptr;
+    const bool prune_c = !all_c && est;
     if (prune_c) {
-        for (int c = t; c < sort_n1; c += blockDim.x) {
-            uint64_t key = ~0ull;
-            if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
-                float lo, hi;
-                approx_band(D, w, qi, c, &lo, &hi);
-                key = ((uint64_t)float_key(hi) << 32) | (uint32_t)c;
-            }
-            s_keys[c] = key;
-        }
-        __syncthreads();
-        const uint64_t kth = block_select_smallest(s_keys, sort_n1, Pc, s_hist, s_wc, s_sel);
+        const uint64_t kth = block_select_smallest(s_keys, sort_n1, Pc, s_hist, s_wc, s_sel, false);
         if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
         __syncthreads();
     }
     for (int c = t; c < sort_n1; c += blockDim.x) {
-        uint64_t key = ~0ull;
-        if (c < (int)D.C && w.cluster_counts[qi * D.C + c] > 0) {
-            bool cand = true;
-            if (prune_c) {
-                float lo, hi;
-                approx_band(D, w, qi, c, &lo, &hi);
-                cand = lo <= s_bound;
-            }
-            if (cand) {
-                const uint32_t dk = all_c ? 0u : float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d));
-                key = ((uint64_t)dk << 32) | (uint32_t)c;
-            }
+        uint64_t key = s_keys[c];
+        if (key != ~0ull) {
+            if (all_c) key = (uint32_t)key;
+            else if (prune_c && s_lo[c] > s_bound) key = ~0ull;
+            else key = ((uint64_t)float_key(seq_l2_v4(s_q, D.centers + (uint64_t)c * d, d)) << 32) | (uint32_t)c;
         }
         s_keys[c] = key;
     }
@@ -603,65 +600,48 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     __syncthreads();
     if (t == 0) s_nvalid = 0;
     __syncthreads();
-    // the non-empty lists of the chosen clusters (again no distances when all are taken)
+    // the same for the non-empty lists of the chosen clusters
     const uint32_t Smax = D.S_max;
     // list slot e = chosen cluster e / Smax, its list e % Smax (shifts when Smax is a power of two)
     const bool sm_pow2 = (Smax & (Smax - 1)) == 0;
     const int sm_shift = __ffs((int)Smax) - 1;
     {
         uint32_t nzl = 0;
-        for (int e = t; e < npc * (int)Smax; e += blockDim.x) {
+        for (int e = t; e < sort_n2; e += blockDim.x) {
+            uint64_t key = ~0ull;
             const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
-            const uint32_t c = s_chosen[i], j = D.cluster_off[c] + jj;
-            if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) nzl++;
+            if (i < npc) {
+                const uint32_t c = s_chosen[i], j = D.cluster_off[c] + jj;
+                if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
+                    float lo = 0.f, hi = 0.f;
+                    if (est) approx_band(D, w, qi, D.C + j, &lo, &hi);
+                    key = ((uint64_t)float_key(hi) << 32) | j;
+                    s_lo[e] = lo;
+                    nzl++;
+                }
+            }
+            s_keys[e] = key;
         }
-        nzl = __reduce_add_sync(0xffffffffu, nzl);  // one shared atomic per warp
+        nzl = __reduce_add_sync(0xffffffffu, nzl);
         if ((t & 31) == 0 && nzl) atomicAdd(&s_nvalid, (int)nzl);
     }
     __syncthreads();
     // lists probed by this query: sub_lists, or the query's own n_probe when given
     const int Psq = w.qps ? max(1, min(Ps, (int)w.qps[qi])) : Ps;
     const bool all_l = s_nvalid <= Psq;
-    const bool prune_l = !all_l && w.S != nullptr;
+    const bool prune_l = !all_l && est;
     if (prune_l) {
-        for (int e = t; e < sort_n2; e += blockDim.x) {
-            uint64_t key = ~0ull;
-            const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
-            if (i < npc) {
-                const uint32_t c = s_chosen[i];
-                const uint32_t j = D.cluster_off[c] + jj;
-                if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
-                    float lo, hi;
-                    approx_band(D, w, qi, D.C + j, &lo, &hi);
-                    key = ((uint64_t)float_key(hi) << 32) | j;
-                }
-            }
-            s_keys[e] = key;
-        }
-        __syncthreads();
-        const uint64_t kth = block_select_smallest(s_keys, sort_n2, Psq, s_hist, s_wc, s_sel);
+        const uint64_t kth = block_select_smallest(s_keys, sort_n2, Psq, s_hist, s_wc, s_sel, false);
         if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
         __syncthreads();
     }
     for (int e = t; e < sort_n2; e += blockDim.x) {
-        uint64_t key = ~0ull;
-        const int i = sm_pow2 ? (e >> sm_shift) : e / (int)Smax, jj = sm_pow2 ? (e & (int)(Smax - 1)) : e % (int)Smax;
-        if (i < npc) {
-            const uint32_t c = s_chosen[i];
-            const uint32_t j = D.cluster_off[c] + jj;
-            if (j < D.cluster_off[c + 1] && w.list_counts[qi * D.n_lists + j] > 0) {
-                bool cand = true;
-                if (prune_l) {
-                    float lo, hi;
-                    approx_band(D, w, qi, D.C + j, &lo, &hi);
-                    cand = lo <= s_bound;
-                }
-                if (cand) {
-                    const uint32_t dk =
-                        all_l ? 0u : float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d));
-                    key = ((uint64_t)dk << 32) | j;
-                }
-            }
+        uint64_t key = s_keys[e];
+        if (key != ~0ull) {
+            const uint32_t j = (uint32_t)key;
+            if (all_l) key = j;
+            else if (prune_l && s_lo[e] > s_bound) key = ~0ull;
+            else key = ((uint64_t)float_key(seq_l2_v4(s_q, D.sub_centers + (uint64_t)j * d, d)) << 32) | j;
         }
         s_keys[e] = key;
     }
@@ -741,20 +721,21 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     // the exclusive prefix of the ranges' lengths (its last entry the candidate total): the
     // predicate pass, the scan and the select find a position's range by searching it
     {
-        const int Rq = Ps * ns;
+        // (the ranges past the probed lists' are empty: their prefix is the total)
+        const int Rq = Ps * ns, Rn = nps * ns;
         const uint32_t* len = w.range_len + qi * Rq;
         uint32_t* pre = w.range_pre + qi * (Rq + 1);
         unsigned long long run = 0;
-        for (int b0 = 0; b0 < Rq; b0 += blockDim.x) {
+        for (int b0 = 0; b0 < Rn; b0 += blockDim.x) {
             const int i = b0 + t;
-            const unsigned long long x = i < Rq ? len[i] : 0;
+            const unsigned long long x = i < Rn ? len[i] : 0;
             unsigned long long tot = 0;
             const unsigned long long inc = block_inclusive_sum(x, s_scan, &tot);
-            if (i < Rq) pre[i] = (uint32_t)(run + inc - x);
+            if (i < Rn) pre[i] = (uint32_t)(run + inc - x);
             run += tot;
             __syncthreads();  // s_scan is reused by the next chunk
         }
-        if (t == 0) pre[Rq] = (uint32_t)run;
+        for (int i = Rn + t; i <= Rq; i += blockDim.x) pre[i] = (uint32_t)run;
     }
     if (t == 0) {
         w.qstat[qi * 4 + 0] = s_red[0];
@@ -2692,7 +2673,7 @@ static void enqueue_query(hdg_index* idx, QueryCtx& cx, const QueryCall& c, cuda
     tm.mark("prologue");
     const int sort_n1 = (int)next_pow2(std::max<uint32_t>(D.C, 2));
     const int sort_n2 = (int)next_pow2(std::max<uint32_t>((uint32_t)Pc * D.S_max, 2));
-    const size_t sm_co = sizeof(uint64_t) * std::max(sort_n1, sort_n2) + sizeof(float) * D.d;
+    const size_t sm_co = (sizeof(uint64_t) + sizeof(float)) * std::max(sort_n1, sort_n2) + sizeof(float) * D.d;
     HDG_REQUIRE(sm_co <= 200 * 1024, HDG_ERR_UNSUPPORTED, "coarse selection does not fit shared memory");
     if (sm_co > 48 * 1024)
         CK(cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_co));
