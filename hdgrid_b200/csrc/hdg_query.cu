@@ -651,13 +651,36 @@ __global__ void __launch_bounds__(kCoarseThreads) k_coarse(IndexDev D, GridMeta 
     if (all_l) block_compact_keys(s_keys, sort_n2, s_wc);
     else block_select_smallest(s_keys, sort_n2, Psq, s_hist, s_wc, s_sel);
     const int nps = min(Psq, s_nvalid);
-    // the probed lists in list-id (= pool) order, so candidate positions follow pool order
+    // the probed lists in list-id (= pool) order, so candidate positions follow pool order:
+    // marked in a bitmap over the lists (s_chosen is free again), then emitted word by word
     if (!(all_l && all_c)) {
-        const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
-        for (int i = t; i < sort_n3; i += blockDim.x)
-            s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
-        __syncthreads();
-        block_bitonic_sort(s_keys, sort_n3);
+        if (D.n_lists <= 32u * 1024u) {
+            const int W = (int)((D.n_lists + 31) / 32);
+            for (int i = t; i < W; i += blockDim.x) s_chosen[i] = 0;
+            __syncthreads();
+            for (int i = t; i < nps; i += blockDim.x) {
+                const uint32_t j = (uint32_t)s_keys[i];
+                atomicOr(&s_chosen[j >> 5], 1u << (j & 31));
+            }
+            __syncthreads();
+            unsigned long long run = 0;
+            for (int b0 = 0; b0 < W; b0 += blockDim.x) {
+                const int i = b0 + t;
+                const uint32_t word = i < W ? s_chosen[i] : 0u;
+                const unsigned long long x = (unsigned long long)__popc(word);
+                unsigned long long tot = 0;
+                uint32_t at = (uint32_t)(run + block_inclusive_sum(x, s_scan, &tot) - x);
+                for (uint32_t m = word; m; m &= m - 1) s_keys[at++] = (uint32_t)(32 * i + __ffs((int)m) - 1);
+                run += tot;
+                __syncthreads();  // s_scan is reused by the next chunk
+            }
+        } else {
+            const int sort_n3 = (int)next_pow2_dev((uint32_t)max(nps, 2));
+            for (int i = t; i < sort_n3; i += blockDim.x)
+                s_keys[i] = i < nps ? (uint64_t)(uint32_t)s_keys[i] : ~0ull;
+            __syncthreads();
+            block_bitonic_sort(s_keys, sort_n3);
+        }
     }
     const uint64_t zlo = w.zrange[qi * 2], zhi = w.zrange[qi * 2 + 1];
     uint32_t my_cand = 0, my_exact = 0;
