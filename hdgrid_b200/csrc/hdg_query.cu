@@ -2146,7 +2146,28 @@ __global__ void __launch_bounds__(kThreads, 5) k_refine(IndexDev D, const float*
         // 1. the predicate survivors, compacted in place as original ids (each chunk is read
         //    before the barrier and written at or below its own start)
         uint32_t n_lab = 0;
-        for (int base = 0; base < nc; base += kThreads) {
+        // a row taken whole holds valid pool rows only (the predicate pass listed them): no
+        // compaction, just the ids, four lookups in flight per thread and no barrier
+        const bool whole = takes_row(w, qi);
+        if (whole) {
+            for (int e0 = t; e0 < nc; e0 += 4 * kThreads) {
+                uint32_t p[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * kThreads;
+                    p[u] = e < nc ? list[e] : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) p[u] = __ldg(D.ids + p[u]);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * kThreads;
+                    if (e < nc) list[e] = p[u];
+                }
+            }
+            if (t == 0) s_ns = nc;
+        }
+        for (int base = 0; !whole && base < nc; base += kThreads) {
             const int e = base + t;
             bool keep = false;
             uint32_t pool = kInvalid;
