@@ -56,6 +56,7 @@ __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const 
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);         // [sort_n]
     uint32_t* s_cand = reinterpret_cast<uint32_t*>(s_keys + sort_n);  // [sort_n]
     float* s_q = reinterpret_cast<float*>(s_cand + sort_n);        // [d]
+    float* s_lo = s_q + D.d;                                         // [sort_n] the bands' lows
     __shared__ int s_ncand;
     __shared__ float s_bound;
     __shared__ float s_f[kMlpFeatures];
@@ -100,20 +101,18 @@ __global__ void __launch_bounds__(128) k_features(IndexDev D, GridMeta g, const 
                 float lo, hi;
                 coarse_band(qnorm[qi], D.cnorm[c], S[qi * ldS + c], &lo, &hi);
                 key = ((uint64_t)float_key(hi) << 32) | (uint32_t)c;
+                s_lo[c] = lo;
             }
             s_keys[c] = key;
         }
         if (t == 0) s_ncand = 0;
         __syncthreads();
-        const uint64_t kth = block_select_smallest(s_keys, sort_n, kn, s_hist, s_wc, s_sel);
+        // (only the k-th is needed: the keys stay in place)
+        const uint64_t kth = block_select_smallest(s_keys, sort_n, kn, s_hist, s_wc, s_sel, false);
         if (t == 0) s_bound = key_float((uint32_t)(kth >> 32));
         __syncthreads();
         for (int c = t; c < sort_n; c += blockDim.x) {
-            if (c < C) {
-                float lo, hi;
-                coarse_band(qnorm[qi], D.cnorm[c], S[qi * ldS + c], &lo, &hi);
-                if (lo <= s_bound) s_cand[atomicAdd(&s_ncand, 1)] = (uint32_t)c;
-            }
+            if (c < C && s_lo[c] <= s_bound) s_cand[atomicAdd(&s_ncand, 1)] = (uint32_t)c;
             s_keys[c] = ~0ull;
         }
         __syncthreads();
@@ -430,7 +429,7 @@ void learned_features(hdg_index* idx, const float* d_queries, uint64_t q, const 
                       const float* qnorm) {
     const IndexDev& D = idx->dev;
     const int sort_n = (int)next_pow2(std::max<uint32_t>(D.C, 16));
-    const size_t sm = (sizeof(uint64_t) + sizeof(uint32_t)) * sort_n + sizeof(float) * D.d;
+    const size_t sm = (sizeof(uint64_t) + sizeof(uint32_t) + sizeof(float)) * sort_n + sizeof(float) * D.d;
     HDG_REQUIRE(sm <= 200 * 1024, HDG_ERR_UNSUPPORTED, "feature kernel does not fit shared memory");
     CK(cudaFuncSetAttribute(k_features, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_features<<<(unsigned)q, 128, sm, st>>>(D, idx->grid, d_queries, box, cc, qk, k_max, sort_n, S, ldS, qnorm,
