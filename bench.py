@@ -318,6 +318,16 @@ def algorithmic_scan_bytes(cand_q, pass_q, pre_q, M: int, l: int, read_q=None, c
     return float((chk_q * cbytes + read_q * (4 * l))[pre].sum()), adc
 
 
+def refine_algorithmic_bytes(sel_q, pre_q, rows_q, lab_q, l: int, d: int, rank_bytes: int) -> float:
+    """Bytes the re-rank of one batch must read: a 4-byte id lookup per selected entry; for a
+    post-filter query, rank_bytes of packed label ranks per entry and 4*l label bytes per entry
+    whose ranks left the predicate open (lab_q); 4*d bytes per row re-ranked exactly (rows_q)."""
+    sel_q = np.asarray(sel_q, np.float64)
+    pre = np.asarray(pre_q, bool)
+    return float((sel_q * 4).sum() + (sel_q[~pre] * rank_bytes).sum()
+                 + (np.asarray(lab_q, np.float64) * 4 * l).sum() + (np.asarray(rows_q, np.float64) * 4 * d).sum())
+
+
 def scan_traffic(ws, candidates, kernel="k_scan_fast"):
     """DRAM bytes of one launch of the kernel: the per-candidate figure of the committed ncu
     summary for this workload (dram__bytes_read.sum + dram__bytes_write.sum over the
@@ -461,8 +471,8 @@ def run_hdgrid(args):
         sel_q = np.frombuffer(idx.debug_fetch("cand_count").tobytes(), np.uint32)[:nq].astype(np.float64)
         rows_q = np.frombuffer(idx.debug_fetch("refine_rows").tobytes(), np.uint32)[:nq].astype(np.float64)
         lab_q = np.frombuffer(idx.debug_fetch("refine_labels_read").tobytes(), np.uint32)[:nq].astype(np.float64)
-        refine_bytes = float((sel_q * 4).sum() + (sel_q[~pre_q] * info["rank_pack_bytes"]).sum()
-                             + (lab_q * 4 * info["l"]).sum() + (rows_q * 4 * info["d"]).sum())
+        refine_bytes = refine_algorithmic_bytes(sel_q, pre_q, rows_q, lab_q, info["l"], info["d"],
+                                                info["rank_pack_bytes"])
         refine_entries = {"selected": int(sel_q.sum()), "selected_post_filter": int(sel_q[~pre_q].sum()),
                           "labels_read": int(lab_q.sum()), "rows": int(rows_q.sum())}
 

@@ -63,12 +63,24 @@ def test_algorithmic_scan_bytes():
 
 def test_algorithmic_scan_bytes_of_the_predicate_pass():
     import bench
-    # the predicate pass reads the 2-byte packed cells of the 2000 checked candidates and the
-    # labels of the 300 inside the cell box; the ADC scan reads the codes of the 10 survivors
-    # and of every candidate of the post-filter query
+    # the predicate pass reads the 4-byte packed label ranks of the 2000 checked candidates and
+    # the labels of the 300 inside the rank box; the ADC scan reads the codes of the 10
+    # survivors and of every candidate of the post-filter query
     got = bench.algorithmic_scan_bytes([1000, 2000], [900, 10], [False, True], M=32, l=4, read_q=[0, 300],
-                                       chk_q=[0, 2000], cbytes=2)
-    assert got == (2000 * 2 + 300 * 16, 1000 * 32 + 10 * 32)
-    # no cell check (most candidates in the box): labels for all, no cells
+                                       chk_q=[0, 2000], cbytes=4)
+    assert got == (2000 * 4 + 300 * 16, 1000 * 32 + 10 * 32)
+    # no rank check (most candidates in the box): labels for all, no ranks
     got = bench.algorithmic_scan_bytes([2000], [10], [True], M=32, l=4, read_q=[2000], chk_q=[0], cbytes=4)
     assert got == (2000 * 16, 10 * 32)
+
+
+def test_refine_algorithmic_bytes():
+    import bench
+    # query 0 post-filter: 5000 selected entries, each a 4-byte id lookup and 4 bytes of ranks,
+    # labels (4*l) for the 40 whose ranks sat on the box's edge, 100 exact rows of 4*d; query 1
+    # predicate-first: 300 entries, every one an exact row
+    got = bench.refine_algorithmic_bytes([5000, 300], [False, True], [100, 300], [40, 0], l=4, d=128, rank_bytes=4)
+    assert got == 5300 * 4 + 5000 * 4 + 40 * 16 + 400 * 512
+    # without packed ranks the post-filter entries read no rank bytes
+    got = bench.refine_algorithmic_bytes([5000], [False], [100], [5000], l=4, d=128, rank_bytes=0)
+    assert got == 5000 * 4 + 5000 * 16 + 100 * 512
