@@ -794,7 +794,6 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_cn = reserve((H.C + H.n_lists) * 4);
     const size_t o_co = reserve(H.cluster_off.size() * 4), o_lo = reserve(H.list_off.size() * 4);
     GridMeta gp = H.grid;
-    morton_dim_masks(gp);
     // label-rank thresholds: per dim, the distinct values of a strided sample when they fit,
     // else its quantiles (equal counts per rank), so a rank box is about as tight as the labels
     const int rbits = H.n && !H.labels.empty() ? rank_bits_for((int)H.l) : 0;

@@ -52,35 +52,14 @@ struct GridMeta {
     uint64_t tot_cells = 0;
     int morton_dims = 0, morton_max_bits = 0, morton_valid_map = 0;
     int diff_dim = 0;
-    // bits of each (shuffled) dim inside a Morton code (0 for a masked dim); derived from the
-    // Morton configuration by morton_dim_masks, not stored in the index file
-    uint64_t zmask[kMaxDims] = {0};
 };
 
-// The Morton-code bit positions of every dim (zorder.cu:3-15 interleaves MSB first over the
-// valid dims): masking a code with zmask[i] keeps dim i's bits in their order, so comparing
-// two masked codes compares the two cells' coordinates of dim i.
 // Bits per label-rank field: l fields of b bits, each with its guard bit, in 32 bits; at most
 // 12 (4095 thresholds per dim); 0 when l fields do not fit.
 inline int rank_bits_for(int l) {
     if (l <= 0) return 0;
     const int b = (32 - l) / l;
     return b < 1 ? 0 : (b > 12 ? 12 : b);
-}
-
-inline void morton_dim_masks(GridMeta& g) {
-    int active = 0;
-    for (int i = 0; i < g.morton_dims; i++) active += (g.morton_valid_map >> i) & 1;
-    for (int i = 0; i < kMaxDims; i++) g.zmask[i] = 0;
-    int j = 0;
-    for (int i = 0; i < g.morton_dims; i++) {
-        if (!((g.morton_valid_map >> i) & 1)) continue;
-        for (int b = 0; b < g.morton_max_bits; b++) {
-            const int shift = (g.morton_max_bits - 1 - b) * active + (active - 1 - j);
-            if (shift >= 0 && shift < 64) g.zmask[i] |= 1ull << shift;
-        }
-        j++;
-    }
 }
 
 // filter.conf on the device (passed by value; the map table lives in the arena).
