@@ -102,6 +102,7 @@ def _load() -> C.CDLL:
         "hdg_bruteforce_knn": [vp, u64, u32, vp, u32, vp, u64, vp, u32, vp, vp, vp],
         "hdg_bf16_gemm": [vp, u64, vp, u64, u32, vp, u64, vp],
         "hdg_merge_topk": [vp, vp, u64, u32, u32, vp, vp, vp, vp],
+        "hdg_label_ranks": [vp, u64, u32, C.POINTER(u32), vp, vp, vp, vp],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -470,9 +471,30 @@ def version() -> str:
     return LIB.hdg_version().decode()
 
 
+def label_ranks(labels) -> dict:
+    """The label-rank thresholds the build derives from a base set's labels (hdg_label_ranks):
+    labels a host [n x l] float32 array.  Returns {"bits", "thresholds" (one ascending array per
+    dim), "min", "max"}; a label's rank in dim i is np.searchsorted(thresholds[i], x, "right")."""
+    import numpy as np
+    lab = np.ascontiguousarray(labels, dtype=np.float32)
+    if lab.ndim != 2:
+        raise ValueError("labels must be [n x l]")
+    n, l = lab.shape
+    bits = C.c_uint32(0)
+    _check(LIB.hdg_label_ranks(None, 0, l, C.byref(bits), None, None, None, None))
+    stride = (1 << bits.value) - 1
+    thr = np.zeros((l, stride), np.float32)
+    n_thr = np.zeros(l, np.uint32)
+    mn = np.zeros(l, np.float32)
+    mx = np.zeros(l, np.float32)
+    _check(LIB.hdg_label_ranks(lab.ctypes.data, n, l, C.byref(bits), thr.ctypes.data, n_thr.ctypes.data,
+                               mn.ctypes.data, mx.ctypes.data))
+    return {"bits": bits.value, "thresholds": [thr[i, :n_thr[i]].copy() for i in range(l)], "min": mn, "max": mx}
+
+
 __all__ = ["Config", "config_factory", "index_factory", "SuperGridIndex", "build_input_t", "query_input_t",
            "query_output_t", "HDGError", "parse_config", "parse_filter", "pq_lut", "pq_adc", "label_mask",
-           "recover_filters", "bruteforce_knn", "version", "EXPORTED", "LIB"]
+           "recover_filters", "bruteforce_knn", "version", "label_ranks", "EXPORTED", "LIB"]
 
 
 def merge_topk(dist, ids, k: int, offsets, out_dist, out_ids, stream=None) -> None:

@@ -115,6 +115,17 @@ hdg_status hdg_destroy(hdg_index* index) {
     return guarded([&] { delete index; });
 }
 
+hdg_status hdg_label_ranks(const float* labels, uint64_t n, uint32_t l, uint32_t* bits, float* thr,
+                           uint32_t* n_thr, float* lab_min, float* lab_max) {
+    return guarded([&] {
+        HDG_REQUIRE(bits && l >= 1 && l <= (uint32_t)kMaxDims, HDG_ERR_INVALID_ARG, "bits missing or l outside 1..8");
+        *bits = (uint32_t)rank_bits_for((int)l);
+        if (!thr) return;
+        HDG_REQUIRE(labels && n > 0 && n_thr && lab_min && lab_max, HDG_ERR_INVALID_ARG, "null argument or no rows");
+        label_rank_thresholds(labels, n, (int)l, (int)*bits, thr, n_thr, lab_min, lab_max);
+    });
+}
+
 hdg_status hdg_parse_config(const char* text, hdg_params* out) {
     return guarded([&] {
         HDG_REQUIRE(text && out, HDG_ERR_INVALID_ARG, "null argument");

@@ -769,6 +769,48 @@ void build_index(hdg_index* idx, const float* d_data, uint64_t n, uint32_t d, co
     upload_index(idx, st);
 }
 
+// Label-rank thresholds of n rows of l label dims (host memory, row-major [n][l]): per dim,
+// the distinct values of a strided sample of at most 262,144 rows when they fit in 2^bits - 1
+// thresholds (one rank per value), else the sample's quantiles (equal counts per rank); thr
+// [l][2^bits - 1], n_thr [l], and each dim's smallest and largest label over every row.  NaN
+// labels are left out of all of them.
+void label_rank_thresholds(const float* labels, uint64_t n, int l, int bits, float* thr, uint32_t* n_thr, float* mn,
+                           float* mx) {
+    const uint32_t stride = (1u << bits) - 1u;
+    const uint64_t step = std::max<uint64_t>(1, n / 262144);
+#pragma omp parallel for
+    for (int i = 0; i < l; i++) {
+        std::vector<float> v;
+        v.reserve(n / step + 1);
+        for (uint64_t r = 0; r < n; r += step) {
+            const float x = labels[r * l + i];
+            if (!std::isnan(x)) v.push_back(x);
+        }
+        std::sort(v.begin(), v.end());
+        float lo = INFINITY, hi = -INFINITY;  // over every label, not the sample
+        for (uint64_t r = 0; r < n; r++) {
+            const float x = labels[r * l + i];
+            lo = std::min(lo, x);
+            hi = std::max(hi, x);
+        }
+        mn[i] = lo;
+        mx[i] = hi;
+        std::vector<float> u(v);
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        float* t = thr + (size_t)i * stride;
+        uint32_t m = 0;
+        if (u.size() <= stride + 1) {
+            for (size_t k = 1; k < u.size(); k++) t[m++] = u[k];
+        } else {
+            for (uint32_t k = 1; k <= stride; k++) {
+                const float x = v[(size_t)((uint64_t)k * v.size() / (stride + 1))];
+                if (m == 0 || x > t[m - 1]) t[m++] = x;
+            }
+        }
+        n_thr[i] = m;
+    }
+}
+
 // Copy the host index into one device arena and fill idx->dev.
 void upload_index(hdg_index* idx, cudaStream_t st) {
     HostIndex& H = idx->host;
@@ -794,47 +836,13 @@ void upload_index(hdg_index* idx, cudaStream_t st) {
     const size_t o_cn = reserve((H.C + H.n_lists) * 4);
     const size_t o_co = reserve(H.cluster_off.size() * 4), o_lo = reserve(H.list_off.size() * 4);
     GridMeta gp = H.grid;
-    // label-rank thresholds: per dim, the distinct values of a strided sample when they fit,
-    // else its quantiles (equal counts per rank), so a rank box is about as tight as the labels
+    // label-rank thresholds, so that a rank box is about as tight as the labels
     const int rbits = H.n && !H.labels.empty() ? rank_bits_for((int)H.l) : 0;
     const uint32_t rstride = rbits ? (1u << rbits) - 1u : 0u;
     std::vector<float> rthr((size_t)H.l * rstride);
     uint32_t rn[kMaxDims] = {0};
     float rmin[kMaxDims] = {0.f}, rmax[kMaxDims] = {0.f};
-    if (rbits) {
-        const uint64_t step = std::max<uint64_t>(1, H.n / 262144);
-#pragma omp parallel for
-        for (int i = 0; i < (int)H.l; i++) {
-            std::vector<float> v;
-            v.reserve(H.n / step + 1);
-            for (uint64_t r = 0; r < H.n; r += step) {
-                const float x = H.labels[r * H.l + i];
-                if (!std::isnan(x)) v.push_back(x);
-            }
-            std::sort(v.begin(), v.end());
-            float mn = INFINITY, mx = -INFINITY;  // over every label, not the sample
-            for (uint64_t r = 0; r < H.n; r++) {
-                const float x = H.labels[r * H.l + i];
-                mn = std::min(mn, x);
-                mx = std::max(mx, x);
-            }
-            rmin[i] = mn;
-            rmax[i] = mx;
-            std::vector<float> u(v);
-            u.erase(std::unique(u.begin(), u.end()), u.end());
-            float* t = rthr.data() + (size_t)i * rstride;
-            uint32_t m = 0;
-            if (u.size() <= rstride + 1) {
-                for (size_t k = 1; k < u.size(); k++) t[m++] = u[k];  // one rank per distinct value
-            } else {
-                for (uint32_t k = 1; k <= rstride; k++) {
-                    const float x = v[(size_t)((uint64_t)k * v.size() / (rstride + 1))];
-                    if (m == 0 || x > t[m - 1]) t[m++] = x;
-                }
-            }
-            rn[i] = m;
-        }
-    }
+    if (rbits) label_rank_thresholds(H.labels.data(), H.n, (int)H.l, rbits, rthr.data(), rn, rmin, rmax);
     const size_t o_z = reserve(H.zcodes.size() * 8), o_id = reserve(H.ids.size() * 4);
     const size_t o_pk = reserve(rbits ? H.n * 4 : 0), o_rt = reserve(rthr.size() * 4);
     const size_t o_code = reserve(H.codes.size() + 64), o_lab = reserve(H.labels.size() * 4);

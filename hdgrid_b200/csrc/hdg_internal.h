@@ -45,6 +45,9 @@ void run_query(hdg_index* idx, const float* d_queries, uint64_t q, const float* 
                cudaStream_t st, const uint32_t* d_k = nullptr, const uint32_t* d_nprobe = nullptr,
                const uint8_t* d_sched = nullptr);
 int sm_count();  // SMs of the current device
+// per-dim label-rank thresholds and label ranges of a base set (hdg_build.cu)
+void label_rank_thresholds(const float* labels, uint64_t n, int l, int bits, float* thr, uint32_t* n_thr, float* mn,
+                           float* mx);
 // learned per-query schedule (hdg_learned.cu): 48 features -> 128 -> 128 -> 2 BF16 MLP,
 // parameters W1 [128 x 48], b1, W2 [128 x 128], b2, W3 [2 x 128], b3 in one f32 vector
 constexpr int kMlpFeatures = 48, kMlpHidden = 128, kMlpOut = 2;

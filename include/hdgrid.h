@@ -320,6 +320,18 @@ hdg_status hdg_merge_topk(const float* d_dist, const uint64_t* d_ids, uint64_t q
                           uint32_t n_batches, const uint64_t* d_offsets, float* d_out_dist,
                           uint64_t* d_out_ids, void* stream);
 
+/* ---- label ranks (no reference counterpart) -----------------------------------------------
+ * The predicate pass and the re-rank test a point's packed label ranks before its labels: per
+ * label dim, up to 2^bits - 1 ascending thresholds, a label's rank being the number of them at
+ * or below it (bits = min(12, (32 - l) / l)).  The build derives them from the base set's
+ * labels with this function.  labels: host [n x l] f32, row-major.  *bits receives the bits
+ * per dim; with thr non-NULL, thr receives [l x (2^bits - 1)] thresholds (row i: the first
+ * n_thr[i] entries, strictly ascending) -- the distinct values of a strided sample of at most
+ * 262,144 rows when they fit, else the sample's quantiles -- and lab_min / lab_max each dim's
+ * smallest and largest label over every row.  NaN labels are left out.  1 <= l <= 8. */
+hdg_status hdg_label_ranks(const float* labels, uint64_t n, uint32_t l, uint32_t* bits, float* thr,
+                           uint32_t* n_thr, float* lab_min, float* lab_max);
+
 /* Thread-local message of the last failing call. */
 const char* hdg_last_error(void);
 const char* hdg_version(void);
