@@ -1305,7 +1305,7 @@ __device__ __forceinline__ void pre_span(const IndexDev& D, int lbl, const float
         }
     }
     if (CHECK) {
-        n_read += qt;  // every cell-passed candidate had its labels read
+        n_read += qt;  // every rank-passed candidate had its labels read
         n_chk += e1 - e0;
         for (;;) {
             if (qi != qh) consume();
