@@ -98,3 +98,28 @@ def test_rank_boxes_are_exact():
 def test_invalid_arguments():
     with pytest.raises(hg.HDGError):
         hg.label_ranks(np.zeros((4, 9), np.float32))
+
+
+@pytest.mark.parametrize("l", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_guarded_field_range_test(l):
+    # The kernels test every dim of a packed rank word at once: with G the guard bits, lo and hi
+    # the box's bounds in their fields, ((c | G) - lo) & ((hi | G) - c) & G == G exactly when
+    # every field of c lies in [lo, hi] -- including the empty field [1, 0] of an inner box
+    # with no rank sure to pass.  Checked here on the 32-bit words of every field width.
+    bits = hg.label_ranks(np.zeros((2, l), np.float32))["bits"]
+    rng = np.random.default_rng(l)
+    top = (1 << bits) - 1
+    off = [i * (bits + 1) for i in range(l)]
+    G = sum(1 << (o + bits) for o in off)
+    mask32 = (1 << 32) - 1
+    for _ in range(2000):
+        c = rng.integers(0, top + 1, l)
+        lo = rng.integers(0, top + 1, l)
+        hi = rng.integers(0, top + 1, l)
+        empty = rng.random(l) < 0.1
+        lo[empty], hi[empty] = 1, 0
+        cw = sum(int(v) << o for v, o in zip(c, off))
+        low = sum(int(v) << o for v, o in zip(lo, off))
+        high = sum(int(v) << o for v, o in zip(hi, off)) | G
+        t = (((cw | G) - low) & mask32) & ((high - cw) & mask32)
+        assert ((t & G) == G) == bool(np.all((c >= lo) & (c <= hi))), (c, lo, hi)
